@@ -1,0 +1,369 @@
+"""Oracle: a NumPy FP64 restatement of the reference's molecular DF-RHF.
+
+TEST INFRASTRUCTURE ONLY (the checker for ``tests/``, ``smoke()`` and the CPU
+baseline of ``bench.py``); the product never imports it.
+
+Each function restates one piece of the reference, cited by file:line. Integrals
+come from ``oracle.kernels`` (the C++ restatement of the Rust kernels). The
+restatement is pinned against the reference itself: ``tests/golden/make_golden.py``
+runs the reference's own ``solve_scf`` on the same inputs in a container where
+the reference tree is mounted and stores energies, densities and iteration
+counts as fixtures, which ``tests/test_oracle.py`` compares against.
+
+Shell tables are passed as objects with the SoA attributes of
+``hafnium/integrals/shell_table.py:14-82`` (``angular_momenta``, ``centers``,
+``primitive_offsets``, ``exponents``, ``coefficients``, ``n_contractions``).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from oracle import kernels
+
+DEFAULT_METRIC_THRESHOLD = 1e-10  # density_fitting.py:32
+DEFAULT_OVERLAP_THRESHOLD = 1e-10  # orthogonalization.py:12
+NULL_SPACE_TOLERANCE = 1e-14  # diis.py:17
+DEFAULT_SCHWARZ_THRESHOLD = 1e-14  # integrals/two_electron.py:17
+FILL_TOLERANCE = 1e-12  # occupation.py:285
+ZERO = np.zeros((1, 3))
+
+
+def kernel_table(table) -> kernels.ShellTable:
+    """native.py:16-24: marshal the SoA arrays into the kernel module's table."""
+    counts = getattr(table, "n_contractions", None)
+    if counts is None:
+        counts = table.contraction_counts
+    return kernels.ShellTable(
+        table.angular_momenta, table.centers, table.primitive_offsets, table.exponents, table.coefficients, counts
+    )
+
+
+# ------------------------------------------------------------------ integrals
+def overlap(table) -> np.ndarray:
+    t = kernel_table(table)
+    return kernels.overlap(t, t, ZERO)[0]
+
+
+def core_hamiltonian(table, charges, positions) -> np.ndarray:
+    """one_electron.py:65-75: kinetic plus attraction to the nuclei."""
+    t = kernel_table(table)
+    return kernels.kinetic(t, t, ZERO)[0] + kernels.nuclear_attraction(t, t, ZERO, charges, positions)[0]
+
+
+def metric(aux) -> np.ndarray:
+    """density_fitting.py:77: (P|Q) with the full kernel."""
+    a = kernel_table(aux)
+    return kernels.coulomb_two_center(a, a, ZERO)[0]
+
+
+def three_center(aux, orb) -> np.ndarray:
+    """density_fitting.py:78-84: (P|uv) as [aux, ao, ao], both triangles."""
+    a, o = kernel_table(aux), kernel_table(orb)
+    return kernels.coulomb_three_center(a, o, o, np.zeros((1, 2, 3)))[0]
+
+
+def inverse_square_root(m: np.ndarray, threshold: float = DEFAULT_METRIC_THRESHOLD) -> tuple[np.ndarray, int]:
+    """density_fitting.py:181-197: M^{-1/2}, eigenvalues below threshold*max dropped."""
+    w, v = np.linalg.eigh(m)
+    keep = w > threshold * np.max(w)
+    safe = np.where(keep, w, 1.0)
+    inv = np.where(keep, 1.0 / np.sqrt(safe), 0.0)
+    return (v * inv) @ v.T, int(m.shape[0] - keep.sum())
+
+
+def df_tensor(m: np.ndarray, t3: np.ndarray, threshold: float = DEFAULT_METRIC_THRESHOLD) -> np.ndarray:
+    """density_fitting.py:97-107: B = M^{-1/2} (P|uv)."""
+    half, _ = inverse_square_root(m, threshold)
+    return (half @ t3.reshape(t3.shape[0], -1)).reshape(t3.shape)
+
+
+def coulomb(b: np.ndarray, d: np.ndarray) -> np.ndarray:
+    """coulomb_exchange.py:176-182: charges = B.vec(D); J = charges.B."""
+    naux, n = b.shape[0], b.shape[1]
+    flat = b.reshape(naux, n * n)
+    return (((flat @ d.reshape(n * n)) @ flat)).reshape(n, n)
+
+
+def exchange(b: np.ndarray, d: np.ndarray) -> np.ndarray:
+    """coulomb_exchange.py:184-190: K = sum_P B_P D B_P."""
+    naux, n = b.shape[0], b.shape[1]
+    half = b @ d
+    left = np.transpose(half, (1, 0, 2)).reshape(n, naux * n)
+    return left @ b.reshape(naux * n, n)
+
+
+def eri_exact(table) -> np.ndarray:
+    """two_electron.py (hafnium/integrals): (uv|wx) with Schwarz threshold 1e-14."""
+    t = kernel_table(table)
+    return kernels.coulomb_four_center((t, t), (t, t), np.zeros((1, 3, 3)), threshold=DEFAULT_SCHWARZ_THRESHOLD)[0]
+
+
+# ---------------------------------------------------------------- SCF pieces
+def canonical_orthogonalizer(s: np.ndarray, threshold: float = DEFAULT_OVERLAP_THRESHOLD) -> np.ndarray:
+    """orthogonalization.py:16-42: X = V s^{-1/2} over eigenvalues above threshold."""
+    w, v = np.linalg.eigh(s)
+    n = s.shape[-1]
+    kept = int(np.sum(w > threshold))
+    if kept == 0:
+        raise ValueError("no eigenvalue of the overlap exceeds the threshold")
+    return v[:, n - kept:] / np.sqrt(w[n - kept:])[None, :]
+
+
+def solve_diis(overlaps: np.ndarray) -> np.ndarray:
+    """diis.py:82-106: bordered system solved by eigh, null space dropped."""
+    m = overlaps.shape[0]
+    scale = np.max(np.diagonal(overlaps))
+    b = overlaps / (scale if scale > 0.0 else 1.0)
+    system = np.zeros((m + 1, m + 1))
+    system[:m, :m] = b
+    system[:m, m] = -1.0
+    system[m, :m] = -1.0
+    right = np.zeros(m + 1)
+    right[m] = -1.0
+    w, v = np.linalg.eigh(system)
+    keep = np.abs(w) > NULL_SPACE_TOLERANCE * np.max(np.abs(w))
+    inv = np.where(keep, 1.0 / np.where(keep, w, 1.0), 0.0)
+    return (v @ (inv * (v.T @ right)))[:m]
+
+
+def fill_aufbau(energies: np.ndarray, count: int) -> np.ndarray:
+    """occupation.py:321-339 for a molecule: the lowest ``count`` levels get one."""
+    occ = np.zeros(energies.shape[0])
+    occ[np.argsort(energies, kind="stable")[:count]] = 1.0
+    return occ
+
+
+def fill_averaged(energies: np.ndarray, count: float, tolerance: float = 1e-6) -> np.ndarray:
+    """occupation.py:342-370: degenerate groups share electrons equally."""
+    order = sorted(range(len(energies)), key=lambda i: float(energies[i]))
+    values = [float(energies[i]) for i in order]
+    spread = max(1.0, values[-1] - values[0]) if values else 1.0
+    occ = np.zeros(len(energies))
+    remaining = count
+    start = 0
+    while start < len(order):
+        end = start + 1
+        while end < len(order) and values[end] - values[end - 1] <= tolerance * spread:
+            end += 1
+        group = order[start:end]
+        capacity = float(len(group))
+        share = min(remaining, capacity) / capacity
+        occ[group] = share
+        remaining = max(remaining - share * capacity, 0.0)
+        start = end
+    if not math.isclose(remaining, 0.0, abs_tol=FILL_TOLERANCE):
+        raise ValueError(f"cannot place {count} electrons in {len(energies)} levels")
+    return occ
+
+
+@dataclass
+class Iteration:
+    index: int
+    energy: float
+    energy_change: float
+    gradient_norm: float
+
+
+@dataclass
+class RhfResult:
+    energy: float
+    density: np.ndarray  # per-spin D_alpha
+    fock: np.ndarray
+    mo_energies: np.ndarray
+    mo_coefficients: np.ndarray
+    converged: bool
+    history: list = field(default_factory=list)
+    energy_terms: tuple = ()
+
+    @property
+    def n_iterations(self) -> int:
+        return len(self.history)
+
+
+class ExactJK:
+    """coulomb_exchange.py:75-121 restricted to what the SAD atoms need."""
+
+    def __init__(self, eri: np.ndarray) -> None:
+        self.eri = eri
+
+    def coulomb(self, d):
+        return np.einsum("uvwx,wx->uv", self.eri, d)
+
+    def exchange(self, d):
+        return np.einsum("uwxv,wx->uv", self.eri, d)
+
+
+class FittedJK:
+    """coulomb_exchange.py:125-190: J and K from the fitted tensor B[aux, ao, ao]."""
+
+    def __init__(self, b: np.ndarray) -> None:
+        self.b = b
+
+    def coulomb(self, d):
+        return coulomb(self.b, d)
+
+    def exchange(self, d):
+        return exchange(self.b, d)
+
+
+def fock_rhf(h, jk, d_alpha, e_nuc):
+    """hamiltonian.py:331-370 for the restricted class: J from 2 D_a, K from D_a.
+
+    The structured trace of a restricted matrix counts both spins, so
+    E = E_nuc + 2 tr(D h) + tr(D J) - tr(D K) with J = J(2 D).
+    """
+    j = jk.coulomb(2.0 * d_alpha)
+    k = jk.exchange(d_alpha)
+    f = h + j - k
+    e1 = 2.0 * float(np.sum(d_alpha * h))
+    ej = 2.0 * float(np.sum(d_alpha * j)) / 2.0
+    ek = -2.0 * float(np.sum(d_alpha * k)) / 2.0
+    return f, (e_nuc, e1, ej, ek), e_nuc + e1 + ej + ek
+
+
+def solve_rhf(
+    s,
+    h,
+    jk,
+    e_nuc: float,
+    n_alpha: float,
+    *,
+    guess=None,
+    averaged: bool = False,
+    max_iterations: int = 100,
+    energy_tolerance: float = 1e-10,
+    gradient_tolerance: float = 1e-6,
+    diis_size: int = 8,
+) -> RhfResult:
+    """driver.py:154-213 + 331-366 for one restricted block.
+
+    ``averaged`` selects AveragedOccupation (the SAD atoms) over aufbau.
+    Raises RuntimeError with ``.last`` when the iteration does not converge.
+    """
+    x = canonical_orthogonalizer(s)
+
+    def solve(f):
+        w, v = np.linalg.eigh(x.T @ f @ x)
+        return w, x @ v
+
+    def occupy(w):
+        return fill_averaged(w, n_alpha) if averaged else fill_aufbau(w, int(n_alpha))
+
+    if guess is None:  # driver.py:230-236 _averaged_core_density
+        w, c = solve(h)
+        d = (c * fill_averaged(w, n_alpha)[None, :]) @ c.T
+    else:
+        d = guess
+    focks: list[np.ndarray] = []
+    errors: list[np.ndarray] = []
+    history: list[Iteration] = []
+    f = None
+    for index in range(max_iterations):
+        f, _, energy = fock_rhf(h, jk, d, e_nuc)
+        g = x.T @ (f @ d @ s - s @ d @ f) @ x
+        gnorm = math.sqrt(2.0 * float(np.sum(g * g)))
+        change = energy - history[-1].energy if history else math.inf
+        history.append(Iteration(index, energy, change, gnorm))
+        if abs(change) < energy_tolerance and gnorm < gradient_tolerance:
+            return _finish(f, solve, occupy, h, jk, e_nuc, history, True)
+        focks = (focks + [f])[-diis_size:]
+        errors = (errors + [g])[-diis_size:]
+        if len(focks) == 1:
+            extrapolated = focks[0]
+        else:
+            ov = np.array([[2.0 * float(np.sum(a * b)) for b in errors] for a in errors])
+            coef = solve_diis(ov)
+            extrapolated = sum(c * fk for c, fk in zip(coef, focks))
+        w, c = solve(extrapolated)
+        d = (c * occupy(w)[None, :]) @ c.T
+    result = _finish(focks[-1], solve, occupy, h, jk, e_nuc, history, False)
+    error = RuntimeError(f"the SCF did not converge in {max_iterations} iterations")
+    error.last = result  # type: ignore[attr-defined]
+    raise error
+
+
+def _finish(f, solve, occupy, h, jk, e_nuc, history, converged) -> RhfResult:
+    w, c = solve(f)
+    d = (c * occupy(w)[None, :]) @ c.T
+    final_f, terms, energy = fock_rhf(h, jk, d, e_nuc)
+    return RhfResult(energy, d, final_f, w, c, converged, history, terms)
+
+
+# --------------------------------------------------------------- SAD guess
+def atomic_density_guess(orb, symbols, charges_by_symbol) -> np.ndarray:
+    """atoms.py:76-120: converge each distinct element once, place on the diagonal.
+
+    ``orb`` is the molecular orbital shell table with ``shell_atoms``; every atom
+    of one element carries the same shells, so the element is the cache key.
+    """
+    cache: dict[str, np.ndarray] = {}
+    blocks = []
+    for atom, symbol in enumerate(symbols):
+        if symbol not in cache:
+            cache[symbol] = spherical_atom(_atom_table(orb, atom), charges_by_symbol[symbol])
+        blocks.append(cache[symbol])
+    n = sum(b.shape[0] for b in blocks)
+    d = np.zeros((n, n))
+    start = 0
+    for b in blocks:
+        w = b.shape[0]
+        d[start:start + w, start:start + w] = b
+        start += w
+    return d
+
+
+class _Table:
+    pass
+
+
+def _atom_table(orb, atom: int):
+    """The shells of one atom, centred at the origin (atoms.py:42-50, 55-64)."""
+    sel = np.nonzero(np.asarray(orb.shell_atoms) == atom)[0]
+    off = np.asarray(orb.primitive_offsets)
+    k = np.asarray(orb.n_contractions)
+    coef_off = np.concatenate([[0], np.cumsum(k * np.diff(off))])
+    t = _Table()
+    t.angular_momenta = np.asarray(orb.angular_momenta)[sel]
+    t.centers = np.zeros((len(sel), 3))
+    t.primitive_offsets = np.concatenate([[0], np.cumsum(np.diff(off)[sel])]).astype(np.int64)
+    t.exponents = np.concatenate([np.asarray(orb.exponents)[off[i]:off[i + 1]] for i in sel])
+    t.coefficients = np.concatenate([np.asarray(orb.coefficients)[coef_off[i]:coef_off[i + 1]] for i in sel])
+    t.n_contractions = k[sel]
+    return t
+
+
+def spherical_atom(table, z: float) -> np.ndarray:
+    """atoms.py:55-73: neutral atom, exact J/K, electrons averaged over both spins."""
+    s = overlap(table)
+    h = core_hamiltonian(table, np.array([z]), np.zeros((1, 3)))
+    jk = ExactJK(eri_exact(table))
+    result = solve_rhf(s, h, jk, 0.0, z / 2.0, averaged=True)
+    return result.density
+
+
+# ----------------------------------------------------------------- pipeline
+@dataclass
+class DfRhfProblem:
+    s: np.ndarray
+    h: np.ndarray
+    b: np.ndarray
+    e_nuc: float
+    n_alpha: int
+    metric: np.ndarray
+    three_center: np.ndarray
+    dropped: int
+
+
+def build_problem(orb, aux, charges, positions, e_nuc: float, n_alpha: int) -> DfRhfProblem:
+    """hartree_fock.py:88-191 molecular Hamiltonian with a fitted two-body term."""
+    s = overlap(orb)
+    h = core_hamiltonian(orb, charges, positions)
+    m = metric(aux)
+    t3 = three_center(aux, orb)
+    half, dropped = inverse_square_root(m)
+    b = (half @ t3.reshape(t3.shape[0], -1)).reshape(t3.shape)
+    return DfRhfProblem(s, h, b, e_nuc, n_alpha, m, t3, dropped)

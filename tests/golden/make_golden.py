@@ -1,0 +1,114 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Run where the reference tree is mounted (it does not exist on the GPU hosts):
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+Two kinds of fixture are written:
+
+* ``pyscf_*.npz``: the PySCF/libcint values the reference stores in
+  tests/reference/data/*.json (metric and three-centre integrals of water in
+  STO-3G / def2-universal-jkfit; S, T, V of water in cc-pVDZ), converted to
+  NumPy arrays unchanged, with the reference's stored DF-RHF and exact RHF
+  energies of water/STO-3G.
+* ``reference_dfrhf_*.npz``: the reference's own DF-RHF (``hartree_fock`` with
+  its SAD guess, DIIS 8, default tolerances; hafnium/scf/hartree_fock.py:24)
+  run unchanged on seeded water clusters in cc-pVDZ / def2-universal-jkfit,
+  its integrals supplied by the oracle's C++ restatement of the Rust kernels:
+  geometry, total energy, alpha density, iteration energies. The same script
+  checks the oracle's NumPy restatement (oracle/dfrhf.py) against each run.
+"""
+
+from __future__ import annotations
+
+import json
+import pathlib
+import sys
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+
+CLUSTERS = [(1, None), (2, 0), (4, 1), (8, 2)]  # (waters, seed); one water = the reference's water()
+
+
+def molecule_for(n, seed):
+    from hafnium_b200.molecule import water, water_cluster
+
+    return water() if seed is None else water_cluster(n, seed)
+
+
+def stored_pyscf(reference: pathlib.Path) -> None:
+    data = reference / "tests" / "reference" / "data"
+    df = json.loads((data / "density_fitting_water_sto-3g.json").read_text())
+    one = json.loads((data / "one_electron_water_cc-pvdz.json").read_text())
+    mp2 = json.loads((data / "mp2_water_sto-3g.json").read_text())
+    scf = json.loads((data / "scf_water_sto-3g.json").read_text())
+    np.savez_compressed(
+        HERE / "pyscf_water.npz",
+        df_positions_bohr=np.asarray(df["provenance"]["positions_bohr"]),
+        df_metric=np.asarray(df["metric"]),
+        df_three_center=np.asarray(df["three_center"]),
+        one_positions_bohr=np.asarray(one["provenance"].get("positions_bohr", df["provenance"]["positions_bohr"])),
+        one_overlap=np.asarray(one["overlap"]),
+        one_kinetic=np.asarray(one["kinetic"]),
+        one_nuclear=np.asarray(one["nuclear_attraction"]),
+        dfrhf_energy_sto3g=np.asarray(mp2["reference_energy"]),
+        rhf_energy_sto3g=np.asarray(scf["energy"] if "energy" in scf else scf["total_energy"]),
+    )
+
+
+def reference_runs(reference: pathlib.Path) -> None:
+    from oracle import reference_env
+
+    reference_env.install(reference)
+    from hafnium.basis import BasisLibrary, BasisSet
+    from hafnium.integrals import RustEngine
+    from hafnium.molecule import Molecule as RefMolecule
+    from hafnium.scf import hartree_fock
+
+    from hafnium_b200.basis import ShellTable
+    from oracle import dfrhf
+
+    library = BasisLibrary(offline=True)
+    engine = RustEngine()
+    for n, seed in CLUSTERS:
+        mol = molecule_for(n, seed)
+        ref_mol = RefMolecule.from_atoms(list(zip(mol.symbols, map(tuple, mol.positions))), unit="bohr")
+        basis = BasisSet.for_atoms(ref_mol, "cc-pvdz", library=library)
+        aux = BasisSet.for_atoms(ref_mol, "def2-universal-jkfit", library=library)
+        result = hartree_fock(engine, basis, ref_mol, auxiliary=aux)
+        d_ref = np.asarray(result.density.blocks[0])
+        hist = np.asarray([row.energy for row in result.history])
+        # The oracle restatement on the same input.
+        orb = ShellTable.build("cc-pvdz", mol.symbols, mol.positions)
+        auxt = ShellTable.build("def2-universal-jkfit", mol.symbols, mol.positions)
+        prob = dfrhf.build_problem(orb, auxt, mol.nuclear_charges, mol.positions, mol.nuclear_repulsion_energy(),
+                                   mol.n_alpha)
+        guess = dfrhf.atomic_density_guess(orb, mol.symbols, {"O": 8.0, "H": 1.0})
+        ours = dfrhf.solve_rhf(prob.s, prob.h, dfrhf.FittedJK(prob.b), prob.e_nuc, prob.n_alpha, guess=guess)
+        de = abs(ours.energy - result.energy)
+        dd = float(np.max(np.abs(ours.density - d_ref)))
+        print(f"(H2O){n} seed {seed}: reference E = {result.energy:.12f} in {result.n_iterations} iterations; "
+              f"oracle |dE| = {de:.2e}, max|dD| = {dd:.2e}, iterations {ours.n_iterations}; "
+              f"metric eigenvalues dropped: {prob.dropped}")
+        assert de < 1e-10 and dd < 1e-7 and ours.n_iterations == result.n_iterations
+        tag = "water" if seed is None else f"h2o{n}_s{seed}"
+        np.savez_compressed(
+            HERE / f"reference_dfrhf_{tag}.npz",
+            n_waters=np.asarray(n),
+            seed=np.asarray(-1 if seed is None else seed),
+            positions_bohr=mol.positions,
+            energy=np.asarray(result.energy),
+            density=d_ref,
+            history=hist,
+            n_iterations=np.asarray(result.n_iterations),
+        )
+
+
+if __name__ == "__main__":
+    ref = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    stored_pyscf(ref)
+    reference_runs(ref)
