@@ -1,0 +1,251 @@
+"""ctypes binding of ``libhfjk.so`` (include/hfjk.h).
+
+The library is built in-tree (``python -m hafnium_b200.build``) and loaded by
+path. There is no fallback: if the library or a CUDA device is missing, the
+calls raise ``BackendError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+import numpy as np
+
+from hafnium_b200.errors import BackendError, InputError
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIBRARY = HERE / "_build" / "libhfjk.so"
+
+HF_OK, HF_ERR_ARG, HF_ERR_OOM, HF_ERR_CUDA, HF_ERR_TIMEOUT, HF_ERR_NUMERIC, HF_ERR_STATE = range(7)
+PREC_FP64, PREC_BF16X3 = 0, 1
+
+EXPORTS = (
+    "hf_ctx_create", "hf_ctx_destroy", "hf_last_error", "hf_set_stream", "hf_shells_upload",
+    "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
+    "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_get_stats",
+)
+
+
+class ShellTableC(ctypes.Structure):
+    _fields_ = [
+        ("n_shells", ctypes.c_int64),
+        ("angular_momenta", ctypes.c_void_p),
+        ("centers", ctypes.c_void_p),
+        ("primitive_offsets", ctypes.c_void_p),
+        ("exponents", ctypes.c_void_p),
+        ("coefficients", ctypes.c_void_p),
+        ("n_contractions", ctypes.c_void_p),
+    ]
+
+
+class StatsC(ctypes.Structure):
+    _fields_ = [
+        ("ms_metric", ctypes.c_double),
+        ("ms_factor", ctypes.c_double),
+        ("ms_three_center", ctypes.c_double),
+        ("ms_fit", ctypes.c_double),
+        ("ms_coulomb", ctypes.c_double),
+        ("ms_exchange", ctypes.c_double),
+        ("ms_factorize_density", ctypes.c_double),
+        ("min_pivot_ratio", ctypes.c_double),
+        ("n_ao", ctypes.c_int64),
+        ("n_aux", ctypes.c_int64),
+        ("n_tiles", ctypes.c_int64),
+        ("b_bytes", ctypes.c_int64),
+        ("exchange_rank", ctypes.c_int64),
+        ("kernel_launches", ctypes.c_int64),
+    ]
+
+
+_lib: ctypes.CDLL | None = None
+
+
+def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
+    """Load the library (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    target = pathlib.Path(path) if path else LIBRARY
+    if path is None:
+        from hafnium_b200 import build
+
+        if build.needs_build():
+            try:
+                build.build()
+            except Exception as error:  # noqa: BLE001
+                if not target.exists():
+                    raise BackendError(f"libhfjk.so is missing and could not be built: {error}") from error
+    if not target.exists():
+        raise BackendError(f"libhfjk.so not found at {target}; run python -m hafnium_b200.build")
+    lib = ctypes.CDLL(str(target))
+    v, p, i64, i = ctypes.c_void_p, ctypes.POINTER, ctypes.c_int64, ctypes.c_int
+    lib.hf_ctx_create.argtypes = [i, p(v)]
+    lib.hf_ctx_destroy.argtypes = [v]
+    lib.hf_last_error.argtypes = [v]
+    lib.hf_last_error.restype = ctypes.c_char_p
+    lib.hf_set_stream.argtypes = [v, v]
+    lib.hf_shells_upload.argtypes = [v, p(ShellTableC), p(ShellTableC)]
+    lib.hf_build_fitted_tensor.argtypes = [v]
+    lib.hf_dims.argtypes = [v, p(i64), p(i64)]
+    lib.hf_coulomb.argtypes = [v, v, v, i]
+    lib.hf_exchange.argtypes = [v, v, v, i, i]
+    lib.hf_exchange_factored.argtypes = [v, v, i64, v, v, i, i]
+    lib.hf_metric.argtypes = [v, v]
+    lib.hf_three_center.argtypes = [v, v]
+    lib.hf_fitted_eri.argtypes = [v, v]
+    lib.hf_one_electron.argtypes = [v, i, v, v, i64, v, i]
+    lib.hf_get_stats.argtypes = [v, p(StatsC)]
+    for name in EXPORTS:
+        getattr(lib, name).restype = ctypes.c_int if name != "hf_last_error" else ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def shell_struct(table) -> tuple[ShellTableC, tuple]:
+    """A C view of a ShellTable-like object; the tuple keeps the arrays alive."""
+    counts = getattr(table, "n_contractions", None)
+    if counts is None:
+        counts = table.contraction_counts
+    arrays = (
+        np.ascontiguousarray(table.angular_momenta, dtype=np.int64),
+        np.ascontiguousarray(table.centers, dtype=np.float64),
+        np.ascontiguousarray(table.primitive_offsets, dtype=np.int64),
+        np.ascontiguousarray(table.exponents, dtype=np.float64),
+        np.ascontiguousarray(table.coefficients, dtype=np.float64),
+        np.ascontiguousarray(counts, dtype=np.int64),
+    )
+    s = ShellTableC(arrays[0].shape[0], *(a.ctypes.data for a in arrays))
+    return s, arrays
+
+
+class Context:
+    """One ``hf_ctx``: the device-resident fitted tensor and its J/K builds."""
+
+    def __init__(self, device: int = 0) -> None:
+        self.lib = load()
+        handle = ctypes.c_void_p()
+        status = self.lib.hf_ctx_create(int(device), ctypes.byref(handle))
+        if status != HF_OK:
+            raise BackendError(f"hf_ctx_create failed with status {status} (no usable CUDA device {device}?)")
+        self.handle = handle
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.hf_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter shutdown order varies
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def check(self, status: int, what: str) -> None:
+        if status == HF_OK:
+            return
+        message = (self.lib.hf_last_error(self.handle) or b"").decode()
+        text = f"{what}: {message}" if message else f"{what} failed with status {status}"
+        if status in (HF_ERR_ARG, HF_ERR_NUMERIC, HF_ERR_STATE):
+            raise InputError(text)
+        raise BackendError(text)
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        self.check(self.lib.hf_set_stream(self.handle, stream_handle or None), "hf_set_stream")
+
+    def upload(self, orbital, auxiliary) -> None:
+        o, keep_o = shell_struct(orbital)
+        a, keep_a = shell_struct(auxiliary)
+        self.check(self.lib.hf_shells_upload(self.handle, ctypes.byref(o), ctypes.byref(a)), "hf_shells_upload")
+        del keep_o, keep_a
+
+    def build(self) -> None:
+        self.check(self.lib.hf_build_fitted_tensor(self.handle), "hf_build_fitted_tensor")
+
+    def dims(self) -> tuple[int, int]:
+        n, naux = ctypes.c_int64(), ctypes.c_int64()
+        self.check(self.lib.hf_dims(self.handle, ctypes.byref(n), ctypes.byref(naux)), "hf_dims")
+        return int(n.value), int(naux.value)
+
+    def stats(self) -> dict:
+        s = StatsC()
+        self.check(self.lib.hf_get_stats(self.handle, ctypes.byref(s)), "hf_get_stats")
+        return {name: getattr(s, name) for name, _ in StatsC._fields_}
+
+    # -- host-array entry points (numpy in, numpy out) ---------------------
+    def coulomb_host(self, d: np.ndarray) -> np.ndarray:
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        out = np.empty_like(d)
+        self.check(self.lib.hf_coulomb(self.handle, d.ctypes.data, out.ctypes.data, 0), "hf_coulomb")
+        return out
+
+    def exchange_host(self, d: np.ndarray, precision: int = PREC_FP64) -> np.ndarray:
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        out = np.empty_like(d)
+        self.check(self.lib.hf_exchange(self.handle, d.ctypes.data, out.ctypes.data, precision, 0), "hf_exchange")
+        return out
+
+    def exchange_factored_host(self, c: np.ndarray, weights=None, precision: int = PREC_FP64) -> np.ndarray:
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        n = c.shape[0]
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        out = np.empty((n, n))
+        self.check(
+            self.lib.hf_exchange_factored(
+                self.handle, c.ctypes.data, c.shape[1], None if w is None else w.ctypes.data, out.ctypes.data,
+                precision, 0,
+            ),
+            "hf_exchange_factored",
+        )
+        return out
+
+    # -- device entry points (torch CUDA tensors) ---------------------------
+    def coulomb_device(self, d, out) -> None:
+        self.check(self.lib.hf_coulomb(self.handle, d.data_ptr(), out.data_ptr(), 1), "hf_coulomb")
+
+    def exchange_device(self, d, out, precision: int = PREC_FP64) -> None:
+        self.check(self.lib.hf_exchange(self.handle, d.data_ptr(), out.data_ptr(), precision, 1), "hf_exchange")
+
+    def exchange_factored_device(self, c, out, weights=None, precision: int = PREC_FP64) -> None:
+        self.check(
+            self.lib.hf_exchange_factored(
+                self.handle, c.data_ptr(), c.shape[1], None if weights is None else weights.data_ptr(),
+                out.data_ptr(), precision, 1,
+            ),
+            "hf_exchange_factored",
+        )
+
+    # -- inspection ----------------------------------------------------------
+    def metric(self) -> np.ndarray:
+        _, naux = self.dims()
+        out = np.empty((naux, naux))
+        self.check(self.lib.hf_metric(self.handle, out.ctypes.data), "hf_metric")
+        return out
+
+    def three_center(self) -> np.ndarray:
+        n, naux = self.dims()
+        out = np.empty((naux, n, n))
+        self.check(self.lib.hf_three_center(self.handle, out.ctypes.data), "hf_three_center")
+        return out
+
+    def fitted_eri(self) -> np.ndarray:
+        n, _ = self.dims()
+        out = np.empty((n, n, n, n))
+        self.check(self.lib.hf_fitted_eri(self.handle, out.ctypes.data), "hf_fitted_eri")
+        return out
+
+    def one_electron(self, kind: int, charges=None, positions=None) -> np.ndarray:
+        n, _ = self.dims()
+        out = np.empty((n, n))
+        q = None if charges is None else np.ascontiguousarray(charges, dtype=np.float64)
+        r = None if positions is None else np.ascontiguousarray(positions, dtype=np.float64)
+        natoms = 0 if q is None else q.shape[0]
+        self.check(
+            self.lib.hf_one_electron(
+                self.handle, int(kind), None if q is None else q.ctypes.data, None if r is None else r.ctypes.data,
+                natoms, out.ctypes.data, 0,
+            ),
+            "hf_one_electron",
+        )
+        return out

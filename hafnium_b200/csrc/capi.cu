@@ -1,0 +1,941 @@
+// The C ABI (include/hfjk.h): context, shell upload, fitted-tensor build, J, K.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hfjk.h"
+#include "dgemm.cuh"
+#include "integrals.cuh"
+#include "jk.cuh"
+#include "linalg.cuh"
+#include "md.cuh"
+
+using namespace hf;
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct hf_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    hf_stats stats{};
+    bool uploaded = false, built = false;
+    // shells
+    int n = 0, nt = 0, naux = 0;
+    int64_t ntiles = 0;
+    std::vector<DevShell> orb, aux;  // aux in internal order (sorted by l)
+    std::vector<int> aux_ref_fn;     // internal aux function -> reference index
+    int aux_count[kMaxAuxL + 1] = {};
+    DevShell* d_orb = nullptr;
+    DevShell* d_aux = nullptr;
+    double* d_exps = nullptr;
+    double* d_coefs = nullptr;
+    int* d_aux_by_l[kMaxAuxL + 1] = {};
+    double* d_btable = nullptr;
+    // tensors
+    double* d_metric = nullptr;  // N x N internal order
+    double* d_B = nullptr;       // N x ntiles*4096
+    // scratch
+    double* d_work = nullptr;
+    size_t work_bytes = 0;
+    double* d_io = nullptr;  // host-transfer staging: 2 n x n
+    size_t io_bytes = 0;
+    double* d_kscratch = nullptr;  // K build: Kp | X | Xs
+    size_t kscratch_bytes = 0;
+    double* d_stage = nullptr;  // exchange staging: C, w, Ct, sign, D, Lc, K
+    size_t stage_bytes = 0;
+    int* d_info = nullptr;
+    double* d_scalar = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int fail(hf_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define HF_CU(call)                                                                           \
+    do {                                                                                      \
+        cudaError_t _e = (call);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            return fail(ctx, _e == cudaErrorMemoryAllocation ? HF_ERR_OOM : HF_ERR_CUDA,      \
+                        std::string(#call) + ": " + cudaGetErrorString(_e));                  \
+    } while (0)
+
+int alloc(hf_ctx* ctx, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 8);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(ctx, HF_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+                                         cudaGetErrorString(e));
+    }
+    return HF_OK;
+}
+
+template <class T>
+void release(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+int ensure_work(hf_ctx* ctx, size_t bytes) {
+    if (ctx->work_bytes >= bytes) return HF_OK;
+    release(ctx->d_work);
+    ctx->work_bytes = 0;
+    int s = alloc(ctx, (void**)&ctx->d_work, bytes);
+    if (s == HF_OK) ctx->work_bytes = bytes;
+    return s;
+}
+
+int ensure_io(hf_ctx* ctx, size_t bytes) {
+    if (ctx->io_bytes >= bytes) return HF_OK;
+    release(ctx->d_io);
+    ctx->io_bytes = 0;
+    int s = alloc(ctx, (void**)&ctx->d_io, bytes);
+    if (s == HF_OK) ctx->io_bytes = bytes;
+    return s;
+}
+
+// Validation of integrals/mod.rs:111-173 plus the device kernels' limits.
+int check_table(hf_ctx* ctx, const hf_shell_table* t, const char* name, int max_l, bool aux) {
+    if (!t || t->n_shells < 0) return fail(ctx, HF_ERR_ARG, std::string(name) + ": missing shell table");
+    if (t->n_shells == 0) return fail(ctx, HF_ERR_ARG, std::string(name) + ": the shell table is empty");
+    if (!t->angular_momenta || !t->centers || !t->primitive_offsets || !t->exponents || !t->coefficients ||
+        !t->n_contractions)
+        return fail(ctx, HF_ERR_ARG, std::string(name) + ": null array in the shell table");
+    if (t->primitive_offsets[0] != 0)
+        return fail(ctx, HF_ERR_ARG, std::string(name) + ": primitive offsets start at zero");
+    for (int64_t s = 0; s < t->n_shells; ++s) {
+        const int64_t l = t->angular_momenta[s];
+        const int64_t np = t->primitive_offsets[s + 1] - t->primitive_offsets[s];
+        const int64_t k = t->n_contractions[s];
+        if (np < 1) return fail(ctx, HF_ERR_ARG, std::string(name) + ": every shell needs at least one primitive");
+        if (k < 1) return fail(ctx, HF_ERR_ARG, std::string(name) + ": every shell needs at least one contraction");
+        if (l < 0 || l > max_l)
+            return fail(ctx, HF_ERR_ARG, std::string(name) + ": angular momentum " + std::to_string(l) +
+                                             " exceeds the device kernels' maximum " + std::to_string(max_l));
+        if (aux ? (k != 1) : (k > kMaxOrbContr[l]))
+            return fail(ctx, HF_ERR_ARG, std::string(name) + ": too many general contractions (" + std::to_string(k) +
+                                             ") for l = " + std::to_string(l));
+        for (int x = 0; x < 3; ++x)
+            if (!std::isfinite(t->centers[3 * s + x]))
+                return fail(ctx, HF_ERR_ARG, std::string(name) + ": centres are finite");
+    }
+    int64_t ncoef = 0;
+    for (int64_t s = 0; s < t->n_shells; ++s)
+        ncoef += t->n_contractions[s] * (t->primitive_offsets[s + 1] - t->primitive_offsets[s]);
+    for (int64_t i = 0; i < t->primitive_offsets[t->n_shells]; ++i)
+        if (!(t->exponents[i] > 0.0) || !std::isfinite(t->exponents[i]))
+            return fail(ctx, HF_ERR_ARG, std::string(name) + ": exponents are positive");
+    for (int64_t i = 0; i < ncoef; ++i)
+        if (!std::isfinite(t->coefficients[i]))
+            return fail(ctx, HF_ERR_ARG, std::string(name) + ": coefficients are finite");
+    return HF_OK;
+}
+
+void time_begin(hf_ctx* ctx) { cudaEventRecord(ctx->ev0, ctx->stream); }
+double time_end(hf_ctx* ctx) {
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    cudaEventSynchronize(ctx->ev1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    return ms;
+}
+
+// Ct[i][mu] = C[mu][i] * sqrt|w_i| (zero padded), sign[i] = sign(w_i).
+__global__ void k_factor_transpose(const double* __restrict__ C, int64_t n, int64_t ncols,
+                                   const double* __restrict__ w, double* __restrict__ Ct, int64_t npad, int64_t opad,
+                                   double* __restrict__ sign) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= opad * npad) return;
+    const int64_t i = e / npad, mu = e % npad;
+    double v = 0.0, s = 1.0;
+    if (i < ncols) {
+        const double wi = w ? w[i] : 1.0;
+        s = wi < 0.0 ? -1.0 : 1.0;
+        if (mu < n) v = C[mu * ncols + i] * sqrt(fabs(wi));
+    }
+    Ct[e] = v;
+    if (mu == 0) sign[i] = s;
+}
+
+// Pivoted Cholesky of a symmetric PSD n x n matrix D in one CTA: rows of Lc
+// ([rank][n]) with D ~= Lc^T Lc, stopping when the largest remaining diagonal
+// entry falls to tol times the largest initial one. status: 0 ok, 1 indefinite.
+__global__ void __launch_bounds__(1024) k_pivoted_cholesky(const double* __restrict__ D, int n, double tol, int maxr,
+                                                           double* __restrict__ Lc, int* __restrict__ out) {
+    extern __shared__ double sm[];
+    double* d = sm;                                      // n
+    unsigned char* used = (unsigned char*)(sm + n);      // n
+    __shared__ double rv[32];
+    __shared__ int ri[32];
+    __shared__ double s_dmax0, s_piv;
+    __shared__ int s_p, s_stop;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n; i += blockDim.x) {
+        d[i] = D[(int64_t)i * n + i];
+        used[i] = 0;
+    }
+    __syncthreads();
+    // largest |diagonal|
+    double m = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) m = fmax(m, fabs(d[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((tid & 31) == 0) rv[tid >> 5] = m;
+    __syncthreads();
+    if (tid == 0) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) v = fmax(v, rv[w]);
+        s_dmax0 = v;
+    }
+    __syncthreads();
+    int k = 0;
+    for (; k < maxr; ++k) {
+        double best = -1.0;
+        int bi = -1;
+        for (int i = tid; i < n; i += blockDim.x)
+            if (!used[i] && d[i] > best) {
+                best = d[i];
+                bi = i;
+            }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) {
+                best = ob;
+                bi = oi;
+            }
+        }
+        if ((tid & 31) == 0) {
+            rv[tid >> 5] = best;
+            ri[tid >> 5] = bi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double b = -1.0;
+            int p = -1;
+            for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w)
+                if (rv[w] > b || (rv[w] == b && ri[w] >= 0 && (p < 0 || ri[w] < p))) {
+                    b = rv[w];
+                    p = ri[w];
+                }
+            s_stop = (p < 0 || !(b > tol * s_dmax0)) ? 1 : 0;
+            s_p = p;
+            s_piv = s_stop ? 0.0 : sqrt(b);
+        }
+        __syncthreads();
+        if (s_stop) break;
+        const int p = s_p;
+        const double piv = s_piv;
+        for (int i = tid; i < n; i += blockDim.x) {
+            double l = 0.0;
+            if (i == p) l = piv;
+            else if (!used[i]) {
+                double s = D[(int64_t)p * n + i];
+                for (int j = 0; j < k; ++j) s -= Lc[(int64_t)j * n + i] * Lc[(int64_t)j * n + p];
+                l = s / piv;
+            }
+            Lc[(int64_t)k * n + i] = l;
+        }
+        __syncthreads();
+        for (int i = tid; i < n; i += blockDim.x) {
+            if (i == p) used[i] = 1;
+            else if (!used[i]) {
+                const double l = Lc[(int64_t)k * n + i];
+                d[i] -= l * l;
+            }
+        }
+        __syncthreads();
+    }
+    // indefinite if a remaining diagonal entry is clearly negative
+    int bad = 0;
+    for (int i = tid; i < n; i += blockDim.x)
+        if (!used[i] && d[i] < -1e3 * tol * s_dmax0) bad = 1;
+    bad = __syncthreads_or(bad);
+    if (tid == 0) {
+        out[0] = k;
+        out[1] = bad;
+    }
+}
+
+__global__ void k_factor_pad(const double* __restrict__ Lc, int64_t n, int64_t rank, double* __restrict__ Ct,
+                             int64_t npad, int64_t opad, double* __restrict__ sign) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= opad * npad) return;
+    const int64_t i = e / npad, mu = e % npad;
+    Ct[e] = (i < rank && mu < n) ? Lc[i * n + mu] : 0.0;
+    if (mu == 0) sign[i] = 1.0;
+}
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// Carves 256-byte aligned sub-buffers out of one allocation.
+struct Carver {
+    size_t used = 0;
+    size_t take(size_t doubles) {
+        const size_t at = used;
+        used += (size_t)round_up((int64_t)doubles, 32);
+        return at;
+    }
+};
+
+// Grow-only scratch owned by the context: the K build's Kp/X chunks.
+int ensure_scratch(hf_ctx* ctx, double** p, size_t* have, size_t bytes) {
+    if (*have >= bytes) return HF_OK;
+    release(*p);
+    *have = 0;
+    int s = alloc(ctx, (void**)p, bytes);
+    if (s == HF_OK) *have = bytes;
+    return s;
+}
+
+int check_async(hf_ctx* ctx, const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return HF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hf_ctx_create(int device, hf_ctx** out) {
+    if (!out) return HF_ERR_ARG;
+    *out = nullptr;
+    hf_ctx* ctx = new (std::nothrow) hf_ctx();
+    if (!ctx) return HF_ERR_OOM;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        delete ctx;
+        return HF_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) {
+        delete ctx;
+        return HF_ERR_ARG;
+    }
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return HF_ERR_CUDA;
+    }
+    ctx->stream = ctx->own;
+    cudaEventCreate(&ctx->ev0);
+    cudaEventCreate(&ctx->ev1);
+    upload_c2s(ctx->stream);
+    auto grid = boys_grid_host();
+    if (alloc(ctx, (void**)&ctx->d_btable, sizeof(double) * grid.size()) != HF_OK ||
+        alloc(ctx, (void**)&ctx->d_info, 4 * sizeof(int)) != HF_OK ||
+        alloc(ctx, (void**)&ctx->d_scalar, 4 * sizeof(double)) != HF_OK) {
+        hf_ctx_destroy(ctx);
+        return HF_ERR_OOM;
+    }
+    cudaMemcpy(ctx->d_btable, grid.data(), sizeof(double) * grid.size(), cudaMemcpyHostToDevice);
+    if (cudaGetLastError() != cudaSuccess) {
+        hf_ctx_destroy(ctx);
+        return HF_ERR_CUDA;
+    }
+    *out = ctx;
+    return HF_OK;
+}
+
+static void free_shells(hf_ctx* ctx) {
+    release(ctx->d_orb);
+    release(ctx->d_aux);
+    release(ctx->d_exps);
+    release(ctx->d_coefs);
+    for (auto& p : ctx->d_aux_by_l) release(p);
+}
+
+int hf_ctx_destroy(hf_ctx* ctx) {
+    if (!ctx) return HF_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_shells(ctx);
+    release(ctx->d_btable);
+    release(ctx->d_metric);
+    release(ctx->d_B);
+    release(ctx->d_work);
+    release(ctx->d_io);
+    release(ctx->d_kscratch);
+    release(ctx->d_stage);
+    release(ctx->d_info);
+    release(ctx->d_scalar);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return HF_OK;
+}
+
+const char* hf_last_error(const hf_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int hf_set_stream(hf_ctx* ctx, void* stream) {
+    if (!ctx) return HF_ERR_ARG;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+    return HF_OK;
+}
+
+int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_table* auxt) {
+    if (!ctx) return HF_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int s;
+    if ((s = check_table(ctx, orbt, "orbital", kMaxOrbL, false)) != HF_OK) return s;
+    if ((s = check_table(ctx, auxt, "auxiliary", kMaxAuxL, true)) != HF_OK) return s;
+    free_shells(ctx);
+    release(ctx->d_B);
+    release(ctx->d_metric);
+    ctx->built = false;
+    std::vector<double> exps, coefs;
+    auto add = [&](const hf_shell_table* t, int64_t sh, int fn) {
+        DevShell d{};
+        d.x = t->centers[3 * sh];
+        d.y = t->centers[3 * sh + 1];
+        d.z = t->centers[3 * sh + 2];
+        d.l = (int)t->angular_momenta[sh];
+        const int64_t p0 = t->primitive_offsets[sh], p1 = t->primitive_offsets[sh + 1];
+        d.nprim = (int)(p1 - p0);
+        d.ncontr = (int)t->n_contractions[sh];
+        d.prim = (int)exps.size();
+        d.coef = (int)coefs.size();
+        d.fn = fn;
+        int64_t coff = 0;
+        for (int64_t q = 0; q < sh; ++q)
+            coff += t->n_contractions[q] * (t->primitive_offsets[q + 1] - t->primitive_offsets[q]);
+        for (int64_t i = p0; i < p1; ++i) exps.push_back(t->exponents[i]);
+        for (int64_t i = 0; i < d.ncontr * d.nprim; ++i) coefs.push_back(t->coefficients[coff + i]);
+        return d;
+    };
+    ctx->orb.clear();
+    int fn = 0;
+    for (int64_t sh = 0; sh < orbt->n_shells; ++sh) {
+        ctx->orb.push_back(add(orbt, sh, fn));
+        fn += ctx->orb.back().ncontr * nsph(ctx->orb.back().l);
+    }
+    ctx->n = fn;
+    // auxiliary: reference function offsets, then internal order sorted by l
+    std::vector<int> ref_off(auxt->n_shells);
+    int rf = 0;
+    for (int64_t sh = 0; sh < auxt->n_shells; ++sh) {
+        ref_off[sh] = rf;
+        rf += (int)auxt->n_contractions[sh] * nsph((int)auxt->angular_momenta[sh]);
+    }
+    ctx->aux.clear();
+    ctx->aux_ref_fn.clear();
+    std::vector<std::vector<int>> by_l(kMaxAuxL + 1);
+    int q = 0;
+    for (int l = 0; l <= kMaxAuxL; ++l)
+        for (int64_t sh = 0; sh < auxt->n_shells; ++sh) {
+            if (auxt->angular_momenta[sh] != l) continue;
+            by_l[l].push_back((int)ctx->aux.size());
+            ctx->aux.push_back(add(auxt, sh, q));
+            for (int m = 0; m < nsph(l); ++m) ctx->aux_ref_fn.push_back(ref_off[sh] + m);
+            q += nsph(l);
+        }
+    ctx->naux = q;
+    ctx->nt = (ctx->n + 63) / 64;
+    ctx->ntiles = (int64_t)ctx->nt * (ctx->nt + 1) / 2;
+    if (alloc(ctx, (void**)&ctx->d_orb, sizeof(DevShell) * ctx->orb.size()) ||
+        alloc(ctx, (void**)&ctx->d_aux, sizeof(DevShell) * ctx->aux.size()) ||
+        alloc(ctx, (void**)&ctx->d_exps, sizeof(double) * exps.size()) ||
+        alloc(ctx, (void**)&ctx->d_coefs, sizeof(double) * coefs.size()))
+        return HF_ERR_OOM;
+    HF_CU(cudaMemcpy(ctx->d_orb, ctx->orb.data(), sizeof(DevShell) * ctx->orb.size(), cudaMemcpyHostToDevice));
+    HF_CU(cudaMemcpy(ctx->d_aux, ctx->aux.data(), sizeof(DevShell) * ctx->aux.size(), cudaMemcpyHostToDevice));
+    HF_CU(cudaMemcpy(ctx->d_exps, exps.data(), sizeof(double) * exps.size(), cudaMemcpyHostToDevice));
+    HF_CU(cudaMemcpy(ctx->d_coefs, coefs.data(), sizeof(double) * coefs.size(), cudaMemcpyHostToDevice));
+    for (int l = 0; l <= kMaxAuxL; ++l) {
+        ctx->aux_count[l] = (int)by_l[l].size();
+        if (alloc(ctx, (void**)&ctx->d_aux_by_l[l], sizeof(int) * std::max<size_t>(1, by_l[l].size()))) return HF_ERR_OOM;
+        if (!by_l[l].empty())
+            HF_CU(cudaMemcpy(ctx->d_aux_by_l[l], by_l[l].data(), sizeof(int) * by_l[l].size(), cudaMemcpyHostToDevice));
+    }
+    ctx->stats.n_ao = ctx->n;
+    ctx->stats.n_aux = ctx->naux;
+    ctx->stats.n_tiles = ctx->ntiles;
+    ctx->uploaded = true;
+    return HF_OK;
+}
+
+int hf_dims(const hf_ctx* ctx, int64_t* n_ao, int64_t* n_aux) {
+    if (!ctx || !ctx->uploaded) return HF_ERR_STATE;
+    if (n_ao) *n_ao = ctx->n;
+    if (n_aux) *n_aux = ctx->naux;
+    return HF_OK;
+}
+
+// (P|Q) into d_metric (internal order).
+static int build_metric(hf_ctx* ctx) {
+    const size_t bytes = sizeof(double) * (size_t)ctx->naux * ctx->naux;
+    if (!ctx->d_metric && alloc(ctx, (void**)&ctx->d_metric, bytes)) return HF_ERR_OOM;
+    HF_CU(launch_metric(ctx->d_aux, ctx->d_exps, ctx->d_coefs, ctx->d_aux_by_l, ctx->aux_count, ctx->d_btable,
+                        ctx->d_metric, ctx->naux, ctx->stream));
+    ctx->stats.kernel_launches += 25;
+    return check_async(ctx, "metric");
+}
+
+// Pair tasks for tile rows [row0, row1): pairs (a <= b) with a touching those rows.
+static void chunk_tasks(const hf_ctx* ctx, int row0, int row1, std::vector<PairTask> (&tasks)[3][3],
+                        int (&max_npp)[3][3]) {
+    for (auto& r : tasks)
+        for (auto& v : r) v.clear();
+    for (auto& r : max_npp)
+        for (auto& v : r) v = 0;
+    const int ns = (int)ctx->orb.size();
+    for (int a = 0; a < ns; ++a) {
+        const DevShell& A = ctx->orb[a];
+        const int f0 = A.fn, f1 = A.fn + A.ncontr * nsph(A.l) - 1;
+        if ((f1 >> 6) < row0 || (f0 >> 6) >= row1) continue;
+        for (int b = a; b < ns; ++b) {
+            const DevShell& B = ctx->orb[b];
+            int la = A.l, lb = B.l, swap = 0;
+            if (la > lb) {
+                std::swap(la, lb);
+                swap = 1;
+            }
+            tasks[la][lb].push_back(PairTask{a, b, swap, 0});
+            max_npp[la][lb] = std::max(max_npp[la][lb], A.nprim * B.nprim);
+        }
+    }
+}
+
+// Three-centre integrals of tile rows [row0, row1) into T ([cols][naux]).
+static int three_center_chunk(hf_ctx* ctx, int row0, int row1, double* T, PairTask* d_tasks, size_t task_cap) {
+    std::vector<PairTask> tasks[3][3];
+    int max_npp[3][3];
+    chunk_tasks(ctx, row0, row1, tasks, max_npp);
+    ChunkDesc cd{row0, row1, ctx->nt, tile_index(row0, row0, ctx->nt), ctx->naux};
+    size_t off = 0;
+    for (int la = 0; la <= 2; ++la)
+        for (int lb = la; lb <= 2; ++lb) {
+            auto& v = tasks[la][lb];
+            if (v.empty()) continue;
+            if (off + v.size() > task_cap) return fail(ctx, HF_ERR_STATE, "task buffer too small");
+            HF_CU(cudaMemcpyAsync(d_tasks + off, v.data(), sizeof(PairTask) * v.size(), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+            HF_CU(launch_three_center(la, lb, d_tasks + off, (int)v.size(), max_npp[la][lb], ctx->d_orb, ctx->d_aux,
+                                      ctx->d_exps, ctx->d_coefs, ctx->d_aux_by_l, ctx->aux_count, ctx->d_btable, cd,
+                                      T, ctx->stream));
+            ctx->stats.kernel_launches += 5;
+            off += v.size();
+        }
+    // the host task vectors must outlive the async copies
+    HF_CU(cudaStreamSynchronize(ctx->stream));
+    return HF_OK;
+}
+
+int hf_build_fitted_tensor(hf_ctx* ctx) {
+    if (!ctx) return HF_ERR_ARG;
+    if (!ctx->uploaded) return fail(ctx, HF_ERR_STATE, "upload shells first");
+    cudaSetDevice(ctx->device);
+    const int N = ctx->naux;
+    int s;
+    time_begin(ctx);
+    if ((s = build_metric(ctx)) != HF_OK) return s;
+    ctx->stats.ms_metric = time_end(ctx);
+
+    // Cholesky + inverse of the factor.
+    time_begin(ctx);
+    double *L = nullptr, *Linv = nullptr, *LinvT = nullptr, *wk = nullptr;
+    const size_t nn = (size_t)N * N;
+    if (alloc(ctx, (void**)&L, nn * 8) || alloc(ctx, (void**)&Linv, nn * 8) || alloc(ctx, (void**)&LinvT, nn * 8) ||
+        alloc(ctx, (void**)&wk, (size_t)N * 64 * 8)) {
+        release(L);
+        release(Linv);
+        release(LinvT);
+        release(wk);
+        return HF_ERR_OOM;
+    }
+    HF_CU(cudaMemcpyAsync(L, ctx->d_metric, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    HF_CU(cudaMemsetAsync(ctx->d_info, 0, sizeof(int), ctx->stream));
+    const double big = 1e300;
+    HF_CU(cudaMemcpyAsync(ctx->d_scalar, &big, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    HF_CU(cholesky_lower(L, N, N, ctx->d_info, ctx->d_scalar, ctx->stream));
+    int info = 0;
+    double pivmin = 0.0;
+    HF_CU(cudaMemcpyAsync(&info, ctx->d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    HF_CU(cudaMemcpyAsync(&pivmin, ctx->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    HF_CU(cudaStreamSynchronize(ctx->stream));
+    if (info != 0) {
+        release(L);
+        release(Linv);
+        release(LinvT);
+        release(wk);
+        return fail(ctx, HF_ERR_NUMERIC, "the Coulomb metric is not positive definite (pivot " + std::to_string(info - 1) +
+                                             ")");
+    }
+    {
+        std::vector<double> diag(N);
+        for (int i = 0; i < N; ++i) HF_CU(cudaMemcpy(&diag[i], ctx->d_metric + (size_t)i * N + i, 8, cudaMemcpyDeviceToHost));
+        const double dmax = *std::max_element(diag.begin(), diag.end());
+        ctx->stats.min_pivot_ratio = pivmin * pivmin / dmax;
+    }
+    HF_CU(triangular_inverse(L, N, N, Linv, LinvT, wk, ctx->stream));
+    if ((s = check_async(ctx, "inverse factor")) != HF_OK) return s;
+    ctx->stats.ms_factor = time_end(ctx);
+    release(L);
+    release(LinvT);
+    release(wk);
+
+    // B = L^-1 (P|mu nu), chunked over tile rows.
+    release(ctx->d_B);
+    const int64_t ldb = ctx->ntiles * 4096;
+    if (alloc(ctx, (void**)&ctx->d_B, sizeof(double) * (size_t)N * ldb)) {
+        release(Linv);
+        return HF_ERR_OOM;
+    }
+    ctx->stats.b_bytes = (int64_t)sizeof(double) * N * ldb;
+    const size_t row_bytes = sizeof(double) * 4096 * (size_t)N * ctx->nt;  // the widest row
+    size_t budget = std::max<size_t>(row_bytes, (size_t)4 << 30);
+    size_t freeb = 0, totalb = 0;
+    cudaMemGetInfo(&freeb, &totalb);
+    if (budget > freeb / 2) budget = std::max(row_bytes, freeb / 2);
+    double* T = nullptr;
+    const size_t ns = ctx->orb.size();
+    PairTask* d_tasks = nullptr;
+    const size_t task_cap = ns * (ns + 1) / 2 + 16;
+    if (alloc(ctx, (void**)&T, budget) || alloc(ctx, (void**)&d_tasks, sizeof(PairTask) * task_cap)) {
+        release(T);
+        release(Linv);
+        return HF_ERR_OOM;
+    }
+    double ms3c = 0.0, msfit = 0.0;
+    for (int row0 = 0; row0 < ctx->nt;) {
+        int row1 = row0 + 1;
+        while (row1 < ctx->nt &&
+               sizeof(double) * 4096 * (size_t)N * (tile_index(row1 + 1, row1 + 1, ctx->nt) - tile_index(row0, row0, ctx->nt)) <= budget)
+            ++row1;
+        const int64_t t0 = tile_index(row0, row0, ctx->nt), t1 = tile_index(row1, row1, ctx->nt);
+        const int64_t ncols = (t1 - t0) * 4096;
+        time_begin(ctx);
+        HF_CU(cudaMemsetAsync(T, 0, sizeof(double) * (size_t)ncols * N, ctx->stream));
+        if ((s = three_center_chunk(ctx, row0, row1, T, d_tasks, task_cap)) != HF_OK) {
+            release(T);
+            release(d_tasks);
+            release(Linv);
+            return s;
+        }
+        ms3c += time_end(ctx);
+        time_begin(ctx);
+        HF_CU(apply_inverse_factor(Linv, N, N, T, N, ncols, ctx->d_B + t0 * 4096, ldb, ctx->stream));
+        ++ctx->stats.kernel_launches;
+        if ((s = check_async(ctx, "fitted tensor chunk")) != HF_OK) {
+            release(T);
+            release(d_tasks);
+            release(Linv);
+            return s;
+        }
+        msfit += time_end(ctx);
+        row0 = row1;
+    }
+    release(T);
+    release(d_tasks);
+    release(Linv);
+    HF_CU(cudaStreamSynchronize(ctx->stream));
+    HF_CU(cudaGetLastError());
+    ctx->stats.ms_three_center = ms3c;
+    ctx->stats.ms_fit = msfit;
+    ctx->built = true;
+    return HF_OK;
+}
+
+static JkPlan plan_of(const hf_ctx* ctx) {
+    JkPlan p{};
+    p.B = ctx->d_B;
+    p.ldb = ctx->ntiles * 4096;
+    p.n = ctx->n;
+    p.nt = ctx->nt;
+    p.ntiles = ctx->ntiles;
+    p.naux = ctx->naux;
+    return p;
+}
+
+int hf_coulomb(hf_ctx* ctx, const double* D, double* J, int on_device) {
+    if (!ctx || !D || !J) return HF_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    cudaSetDevice(ctx->device);
+    const JkPlan p = plan_of(ctx);
+    const size_t nn = (size_t)ctx->n * ctx->n;
+    int s;
+    if ((s = ensure_work(ctx, sizeof(double) * coulomb_work_doubles(p))) != HF_OK) return s;
+    const double* dD = D;
+    double* dJ = J;
+    if (!on_device) {
+        if ((s = ensure_io(ctx, 2 * nn * sizeof(double))) != HF_OK) return s;
+        HF_CU(cudaMemcpyAsync(ctx->d_io, D, nn * 8, cudaMemcpyHostToDevice, ctx->stream));
+        dD = ctx->d_io;
+        dJ = ctx->d_io + nn;
+    }
+    time_begin(ctx);
+    HF_CU(coulomb_build(p, dD, dJ, ctx->d_work, ctx->stream));
+    ctx->stats.kernel_launches += 4;
+    if (!on_device) HF_CU(cudaMemcpyAsync(J, dJ, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->stats.ms_coulomb = time_end(ctx);
+    return check_async(ctx, "hf_coulomb");
+}
+
+// K from Ct ([opad][npad], device) and sign ([opad]).
+static int exchange_from_ct(hf_ctx* ctx, const double* Ct, int opad, const double* sign, bool any_negative,
+                            double* dK, int precision) {
+    if (precision != HF_PREC_FP64) return fail(ctx, HF_ERR_ARG, "this precision is not available in this build");
+    const JkPlan p = plan_of(ctx);
+    const int64_t npad = (int64_t)ctx->nt * 64;
+    // X chunk: npad x qchunk x opad doubles, within a budget
+    size_t freeb = 0, totalb = 0;
+    cudaMemGetInfo(&freeb, &totalb);
+    const size_t per_q = sizeof(double) * npad * opad * (any_negative ? 2 : 1);
+    size_t budget = std::min<size_t>((size_t)4 << 30, freeb / 3);
+    int qchunk = (int)std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)ctx->naux));
+    qchunk = std::min(qchunk, 65535);
+    const size_t kp_doubles = (size_t)round_up(npad * npad, 32);
+    int st = ensure_scratch(ctx, &ctx->d_kscratch, &ctx->kscratch_bytes, sizeof(double) * kp_doubles + per_q * qchunk);
+    if (st != HF_OK) return st;
+    double* Kp = ctx->d_kscratch;
+    double* X = Kp + kp_doubles;
+    double* Xs = any_negative ? X + npad * (int64_t)qchunk * opad : nullptr;
+    cudaError_t e = exchange_build_fp64(p, Ct, opad, any_negative ? sign : nullptr, dK, Kp, X, Xs, qchunk, ctx->stream);
+    ctx->stats.kernel_launches += 3 * ((ctx->naux + qchunk - 1) / qchunk) + 2;
+    if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("exchange: ") + cudaGetErrorString(e));
+    return check_async(ctx, "exchange");
+}
+
+int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const double* w, double* K, int precision,
+                         int on_device) {
+    if (!ctx || !C || !K || ncols < 0) return HF_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    cudaSetDevice(ctx->device);
+    const int64_t n = ctx->n, npad = (int64_t)ctx->nt * 64;
+    const int64_t opad = std::max<int64_t>(64, round_up(ncols, 64));
+    bool neg = false;
+    std::vector<double> wh;
+    const double* dC = C;
+    const double* dw = w;
+    Carver cv;
+    const size_t oC = cv.take(n * ncols), ow = cv.take(ncols), oCt = cv.take(opad * npad), osg = cv.take(opad),
+                 oK = cv.take(n * n);
+    int st = ensure_scratch(ctx, &ctx->d_stage, &ctx->stage_bytes, sizeof(double) * cv.used);
+    if (st != HF_OK) return st;
+    double* buf = ctx->d_stage;
+    double* sC = buf + oC;
+    double* sw = buf + ow;
+    double* Ct = buf + oCt;
+    double* sign = buf + osg;
+    double* sK = buf + oK;
+    if (w) {
+        wh.resize(ncols);
+        if (on_device) cudaMemcpy(wh.data(), w, sizeof(double) * ncols, cudaMemcpyDeviceToHost);
+        else std::memcpy(wh.data(), w, sizeof(double) * ncols);
+        for (double v : wh) neg = neg || v < 0.0;
+    }
+    if (!on_device) {
+        cudaMemcpyAsync(sC, C, sizeof(double) * n * ncols, cudaMemcpyHostToDevice, ctx->stream);
+        if (w) cudaMemcpyAsync(sw, w, sizeof(double) * ncols, cudaMemcpyHostToDevice, ctx->stream);
+        dC = sC;
+        dw = w ? sw : nullptr;
+    }
+    time_begin(ctx);
+    k_factor_transpose<<<(unsigned)((opad * npad + 255) / 256), 256, 0, ctx->stream>>>(dC, n, ncols, dw, Ct, npad, opad,
+                                                                                        sign);
+    double* dK = on_device ? K : sK;
+    int s = exchange_from_ct(ctx, Ct, (int)opad, sign, neg, dK, precision);
+    if (s == HF_OK && !on_device) cudaMemcpyAsync(K, sK, sizeof(double) * n * n, cudaMemcpyDeviceToHost, ctx->stream);
+    ctx->stats.ms_exchange = time_end(ctx);
+    ctx->stats.exchange_rank = ncols;
+    if (s == HF_OK) s = check_async(ctx, "hf_exchange_factored");
+    return s;
+}
+
+int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_device) {
+    if (!ctx || !D || !K) return HF_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    cudaSetDevice(ctx->device);
+    const int64_t n = ctx->n, npad = (int64_t)ctx->nt * 64;
+    const size_t nn = (size_t)n * n;
+    const int64_t opad_max = std::max<int64_t>(64, round_up(n, 64));
+    Carver cv;
+    const size_t oD = cv.take(nn), oL = cv.take(nn), oK = cv.take(nn), oCt = cv.take(opad_max * npad),
+                 osg = cv.take(opad_max);
+    int st = ensure_scratch(ctx, &ctx->d_stage, &ctx->stage_bytes, sizeof(double) * cv.used);
+    if (st != HF_OK) return st;
+    double* buf = ctx->d_stage;
+    double* sD = buf + oD;
+    double* Lc = buf + oL;
+    double* sK = buf + oK;
+    const double* dD = D;
+    if (!on_device) {
+        cudaMemcpyAsync(sD, D, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream);
+        dD = sD;
+    }
+    time_begin(ctx);
+    const size_t smem = sizeof(double) * n + n + 16;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_pivoted_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaMemsetAsync(ctx->d_info, 0, 2 * sizeof(int), ctx->stream);
+    k_pivoted_cholesky<<<1, 1024, smem, ctx->stream>>>(dD, (int)n, 1e-14, (int)n, Lc, ctx->d_info);
+    int res[2] = {0, 0};
+    cudaMemcpyAsync(res, ctx->d_info, sizeof(res), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    ctx->stats.ms_factorize_density = time_end(ctx);
+    if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("pivoted Cholesky: ") + cudaGetErrorString(e));
+    if (res[1])
+        return fail(ctx, HF_ERR_NUMERIC, "the density is not positive semidefinite; pass a signed factor to "
+                                         "hf_exchange_factored");
+    const int64_t rank = res[0];
+    const int64_t opad = std::max<int64_t>(64, round_up(rank, 64));
+    double* Ct = buf + oCt;
+    double* sign = buf + osg;
+    time_begin(ctx);
+    k_factor_pad<<<(unsigned)((opad * npad + 255) / 256), 256, 0, ctx->stream>>>(Lc, n, rank, Ct, npad, opad, sign);
+    double* dK = on_device ? K : sK;
+    int s = exchange_from_ct(ctx, Ct, (int)opad, sign, false, dK, precision);
+    if (s == HF_OK && !on_device) cudaMemcpyAsync(K, sK, sizeof(double) * nn, cudaMemcpyDeviceToHost, ctx->stream);
+    ctx->stats.ms_exchange = time_end(ctx);
+    ctx->stats.exchange_rank = rank;
+    if (s == HF_OK) s = check_async(ctx, "hf_exchange");
+    return s;
+}
+
+int hf_metric(hf_ctx* ctx, double* out) {
+    if (!ctx || !out) return HF_ERR_ARG;
+    if (!ctx->uploaded) return fail(ctx, HF_ERR_STATE, "upload shells first");
+    cudaSetDevice(ctx->device);
+    int s;
+    if (!ctx->d_metric && (s = build_metric(ctx)) != HF_OK) return s;
+    const int N = ctx->naux;
+    std::vector<double> m((size_t)N * N);
+    HF_CU(cudaStreamSynchronize(ctx->stream));
+    HF_CU(cudaMemcpy(m.data(), ctx->d_metric, sizeof(double) * m.size(), cudaMemcpyDeviceToHost));
+    for (int a = 0; a < N; ++a)
+        for (int b = 0; b < N; ++b)
+            out[(size_t)ctx->aux_ref_fn[a] * N + ctx->aux_ref_fn[b]] = m[(size_t)a * N + b];
+    return HF_OK;
+}
+
+int hf_three_center(hf_ctx* ctx, double* out) {
+    if (!ctx || !out) return HF_ERR_ARG;
+    if (!ctx->uploaded) return fail(ctx, HF_ERR_STATE, "upload shells first");
+    cudaSetDevice(ctx->device);
+    const int N = ctx->naux, n = ctx->n, nt = ctx->nt;
+    const int64_t ncols = ctx->ntiles * 4096;
+    double* T = nullptr;
+    PairTask* d_tasks = nullptr;
+    const size_t ns = ctx->orb.size(), task_cap = ns * (ns + 1) / 2 + 16;
+    if (alloc(ctx, (void**)&T, sizeof(double) * (size_t)ncols * N) ||
+        alloc(ctx, (void**)&d_tasks, sizeof(PairTask) * task_cap)) {
+        release(T);
+        return HF_ERR_OOM;
+    }
+    HF_CU(cudaMemsetAsync(T, 0, sizeof(double) * (size_t)ncols * N, ctx->stream));
+    int s = three_center_chunk(ctx, 0, nt, T, d_tasks, task_cap);
+    std::vector<double> h;
+    if (s == HF_OK) {
+        h.resize((size_t)ncols * N);
+        cudaMemcpy(h.data(), T, sizeof(double) * h.size(), cudaMemcpyDeviceToHost);
+    }
+    release(T);
+    release(d_tasks);
+    if (s != HF_OK) return s;
+    for (int mu = 0; mu < n; ++mu)
+        for (int nu = 0; nu < n; ++nu) {
+            int a = mu, b = nu;
+            if ((a >> 6) > (b >> 6)) std::swap(a, b);
+            const int64_t col = tile_index(a >> 6, b >> 6, nt) * 4096 + (a & 63) * 64 + (b & 63);
+            for (int q = 0; q < N; ++q)
+                out[((size_t)ctx->aux_ref_fn[q] * n + mu) * n + nu] = h[(size_t)col * N + q];
+        }
+    return HF_OK;
+}
+
+int hf_fitted_eri(hf_ctx* ctx, double* out) {
+    if (!ctx || !out) return HF_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    cudaSetDevice(ctx->device);
+    const int N = ctx->naux, n = ctx->n, nt = ctx->nt;
+    const int64_t ldb = ctx->ntiles * 4096;
+    std::vector<double> b((size_t)N * ldb);
+    HF_CU(cudaStreamSynchronize(ctx->stream));
+    HF_CU(cudaMemcpy(b.data(), ctx->d_B, sizeof(double) * b.size(), cudaMemcpyDeviceToHost));
+    std::vector<double> full((size_t)N * n * n);
+    for (int q = 0; q < N; ++q)
+        for (int mu = 0; mu < n; ++mu)
+            for (int nu = 0; nu < n; ++nu) {
+                int a = mu, c = nu;
+                if ((a >> 6) > (c >> 6)) std::swap(a, c);
+                full[((size_t)q * n + mu) * n + nu] = b[(size_t)q * ldb + tile_index(a >> 6, c >> 6, nt) * 4096 + (a & 63) * 64 + (c & 63)];
+            }
+    const size_t n2 = (size_t)n * n;
+    for (size_t i = 0; i < n2; ++i)
+        for (size_t j = 0; j < n2; ++j) {
+            double s = 0.0;
+            for (int q = 0; q < N; ++q) s += full[q * n2 + i] * full[q * n2 + j];
+            out[i * n2 + j] = s;
+        }
+    return HF_OK;
+}
+
+int hf_one_electron(hf_ctx* ctx, int kind, const double* charges, const double* positions, int64_t natoms, double* out,
+                    int on_device) {
+    if (!ctx || !out || kind < 0 || kind > 2) return HF_ERR_ARG;
+    if (!ctx->uploaded) return fail(ctx, HF_ERR_STATE, "upload shells first");
+    if (kind == 2 && (natoms < 0 || (natoms > 0 && (!charges || !positions))))
+        return fail(ctx, HF_ERR_ARG, "attraction needs charges and positions");
+    cudaSetDevice(ctx->device);
+    const int64_t n = ctx->n;
+    const size_t nn = (size_t)n * n;
+    double* buf = nullptr;
+    const int ns = (int)ctx->orb.size();
+    std::vector<int2> tasks[3][3];
+    for (int a = 0; a < ns; ++a)
+        for (int b = 0; b < ns; ++b) tasks[ctx->orb[a].l][ctx->orb[b].l].push_back(make_int2(a, b));
+    const size_t need = sizeof(double) * (nn + 4 * (size_t)std::max<int64_t>(natoms, 1)) + sizeof(int2) * ns * ns + 64;
+    if (alloc(ctx, (void**)&buf, need)) return HF_ERR_OOM;
+    double* sOut = buf;
+    double* sq = sOut + nn;
+    double* spos = sq + std::max<int64_t>(natoms, 1);
+    int2* dt = (int2*)(spos + 3 * std::max<int64_t>(natoms, 1));
+    if (kind == 2 && natoms > 0) {
+        cudaMemcpy(sq, charges, sizeof(double) * natoms, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+        cudaMemcpy(spos, positions, sizeof(double) * 3 * natoms,
+                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+    }
+    double* dOut = on_device ? out : sOut;
+    size_t off = 0;
+    cudaError_t e = cudaSuccess;
+    for (int la = 0; la <= 2 && e == cudaSuccess; ++la)
+        for (int lb = 0; lb <= 2 && e == cudaSuccess; ++lb) {
+            auto& v = tasks[la][lb];
+            if (v.empty()) continue;
+            cudaMemcpy(dt + off, v.data(), sizeof(int2) * v.size(), cudaMemcpyHostToDevice);
+            e = launch_one_electron(kind, la, lb, dt + off, (int)v.size(), ctx->d_orb, ctx->d_exps, ctx->d_coefs, sq,
+                                    spos, (int)natoms, ctx->d_btable, dOut, n, ctx->stream);
+            ++ctx->stats.kernel_launches;
+            off += v.size();
+        }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess && !on_device) e = cudaMemcpy(out, sOut, sizeof(double) * nn, cudaMemcpyDeviceToHost);
+    release(buf);
+    if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("one-electron: ") + cudaGetErrorString(e));
+    return HF_OK;
+}
+
+int hf_get_stats(const hf_ctx* ctx, hf_stats* out) {
+    if (!ctx || !out) return HF_ERR_ARG;
+    *out = ctx->stats;
+    return HF_OK;
+}
+
+}  // extern "C"

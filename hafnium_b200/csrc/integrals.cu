@@ -1,0 +1,589 @@
+// McMurchie–Davidson integral kernels for sm_100a, FP64.
+//
+// Reference counterparts (crates/hafnium-core/src/integrals/):
+//   (P|Q)        two_electron.rs:74-130  coulomb_two_center, Full kernel, threshold 0
+//   (P|mu nu)    two_electron.rs:212-297 coulomb_three_center, mu<=nu symmetric path
+//   S, T, V      one_electron.rs:40-190
+// The primitive-quartet contraction follows two_electron.rs:1398-1580 with the
+// prefactor 2 pi^(5/2) / (p q sqrt(p+q)); the Cartesian-to-spherical transform is
+// applied to the bra pair's Hermite coefficients once per primitive pair instead
+// of to every output block (cartesian.rs:93-110, two_electron.rs:1028-1060).
+#include <cmath>
+#include <vector>
+
+#include "integrals.cuh"
+#include "md.cuh"
+
+namespace hf {
+
+__constant__ double c_c2s[kC2sSize];
+// (t, u, v) of each tetrahedral index up to order 8, and Cartesian exponents per l.
+__constant__ int c_tet_t[ntet(8)];
+__constant__ int c_tet_u[ntet(8)];
+__constant__ int c_tet_v[ntet(8)];
+__constant__ int c_cart[kMaxAuxL + 1][15][3];
+
+namespace {
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTwoPi52 = 34.98683665524972;  // 2 pi^(5/2)
+
+double fact(int n) {
+    double v = 1.0;
+    for (int k = 2; k <= n; ++k) v *= k;
+    return v;
+}
+double binom(int n, int k) {
+    if (k < 0 || k > n) return 0.0;
+    double v = 1.0;
+    for (int i = 0; i < k; ++i) v = v * (n - i) / (i + 1);
+    return std::round(v);
+}
+// Row-major [2l+1][ncart(l)] sphere-normalised solid harmonics (Helgaker 6.4.47).
+std::vector<double> c2s_host(int l) {
+    const int nc = ncart(l);
+    std::vector<double> m(nsph(l) * nc, 0.0);
+    const double sphere = std::sqrt((2.0 * l + 1.0) / (4.0 * kPi));
+    std::vector<int> ms;
+    if (l == 1) ms = {1, -1, 0};
+    else
+        for (int v = -l; v <= l; ++v) ms.push_back(v);
+    for (int row = 0; row < (int)ms.size(); ++row) {
+        const int mv = ms[row], am = std::abs(mv);
+        const bool neg = mv < 0;
+        const double norm = std::sqrt(2.0 * fact(l + am) * fact(l - am) / (mv == 0 ? 2.0 : 1.0)) /
+                            (std::pow(2.0, am) * fact(l));
+        for (int t = 0; t <= (l - am) / 2; ++t)
+            for (int u = 0; u <= t; ++u) {
+                const int vmax = neg ? (am - 1) / 2 : am / 2;
+                for (int vh = 0; vh <= vmax; ++vh) {
+                    const int two_v = neg ? 2 * vh + 1 : 2 * vh;
+                    if (two_v > am) continue;
+                    const double sign = ((t + vh) % 2 == 0) ? 1.0 : -1.0;
+                    const double coef = sign * std::pow(0.25, t) * binom(l, t) * binom(l - t, am + t) *
+                                        binom(t, u) * binom(am, two_v);
+                    const int py = 2 * u + two_v, px = 2 * t + am - py, pz = l - 2 * t - am;
+                    for (int c = 0; c < nc; ++c)
+                        if (cart_x(l, c) == px && cart_y(l, c) == py && cart_z(l, c) == pz)
+                            m[row * nc + c] += sphere * norm * coef;
+                }
+            }
+    }
+    return m;
+}
+}  // namespace
+
+void upload_c2s(cudaStream_t stream) {
+    std::vector<double> all;
+    for (int l = 0; l <= kMaxAuxL; ++l) {
+        auto m = c2s_host(l);
+        all.insert(all.end(), m.begin(), m.end());
+    }
+    cudaMemcpyToSymbolAsync(c_c2s, all.data(), sizeof(double) * all.size(), 0, cudaMemcpyHostToDevice, stream);
+    int tt[ntet(8)], tu[ntet(8)], tv[ntet(8)];
+    for (int s = 0; s <= 8; ++s)
+        for (int t = 0; t <= s; ++t)
+            for (int u = 0; u <= s - t; ++u) {
+                const int v = s - t - u;
+                tt[tet(t, u, v)] = t;
+                tu[tet(t, u, v)] = u;
+                tv[tet(t, u, v)] = v;
+            }
+    int cc[kMaxAuxL + 1][15][3] = {};
+    for (int l = 0; l <= kMaxAuxL; ++l)
+        for (int c = 0; c < ncart(l); ++c) {
+            cc[l][c][0] = cart_x(l, c);
+            cc[l][c][1] = cart_y(l, c);
+            cc[l][c][2] = cart_z(l, c);
+        }
+    cudaMemcpyToSymbolAsync(c_tet_t, tt, sizeof(tt), 0, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyToSymbolAsync(c_tet_u, tu, sizeof(tu), 0, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyToSymbolAsync(c_tet_v, tv, sizeof(tv), 0, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyToSymbolAsync(c_cart, cc, sizeof(cc), 0, cudaMemcpyHostToDevice, stream);
+    cudaStreamSynchronize(stream);
+}
+
+// F_m(T_j) for T_j = j * step, m < kBoysOrders, by the series of special.rs:67-81
+// for the highest order and the downward recursion for the rest.
+std::vector<double> boys_grid_host() {
+    std::vector<double> g(kBoysGrid * kBoysOrders);
+    const int nmax = kBoysOrders - 1;
+    for (int j = 0; j < kBoysGrid; ++j) {
+        const double t = j * kBoysStep;
+        const double et = std::exp(-t);
+        double term = 1.0 / (2 * nmax + 1), sum = term;
+        for (int i = 1;; ++i) {
+            term *= 2.0 * t / (2 * nmax + 2 * i + 1);
+            sum += term;
+            if (term < sum * 1e-17) break;
+        }
+        double* row = &g[j * kBoysOrders];
+        row[nmax] = et * sum;
+        for (int n = nmax; n >= 1; --n) row[n - 1] = (2.0 * t * row[n] + et) / (2 * n - 1);
+    }
+    return g;
+}
+
+// ------------------------------------------------------------- (P|Q) metric
+template <int LP, int LQ>
+__global__ void __launch_bounds__(128) k_metric(const DevShell* __restrict__ aux, const double* __restrict__ exps,
+                                                const double* __restrict__ coefs, const int* __restrict__ plist,
+                                                int np, const int* __restrict__ qlist, int nq,
+                                                const double* __restrict__ btable, double* __restrict__ M,
+                                                int64_t ldm) {
+    constexpr int L = LP + LQ;
+    constexpr int NCP = ncart(LP), NCQ = ncart(LQ), NSP = nsph(LP), NSQ = nsph(LQ);
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)np * NSP * nq) return;
+    const int iq = (int)(idx % nq);
+    const int64_t rest = idx / nq;
+    const int mp = (int)(rest % NSP);
+    const int ip = (int)(rest / NSP);
+    const DevShell P = aux[plist[ip]];
+    const DevShell Q = aux[qlist[iq]];
+    double crow[NCP];
+#pragma unroll
+    for (int c = 0; c < NCP; ++c) crow[c] = c_c2s[c2s_offset(LP) + mp * NCP + c];
+    double acc[NSQ];
+#pragma unroll
+    for (int m = 0; m < NSQ; ++m) acc[m] = 0.0;
+    const double X = P.x - Q.x, Y = P.y - Q.y, Z = P.z - Q.z;
+    for (int i = 0; i < P.nprim; ++i) {
+        const double p = exps[P.prim + i];
+        const double cp = coefs[P.coef + i] * pow(2.0 * p, -(double)LP);
+        for (int j = 0; j < Q.nprim; ++j) {
+            const double q = exps[Q.prim + j];
+            double cq = coefs[Q.coef + j] * pow(2.0 * q, -(double)LQ);
+            if (LQ & 1) cq = -cq;
+            const double alpha = p * q / (p + q);
+            double R[ntet(L)];
+            hermite_r<L>(alpha, X, Y, Z, btable, R);
+            const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * cp * cq;
+            double h[NCQ];
+#pragma unroll
+            for (int b = 0; b < NCQ; ++b) {
+                double s = 0.0;
+#pragma unroll
+                for (int a = 0; a < NCP; ++a)
+                    s += crow[a] * R[tet(cart_x(LP, a) + cart_x(LQ, b), cart_y(LP, a) + cart_y(LQ, b),
+                                         cart_z(LP, a) + cart_z(LQ, b))];
+                h[b] = s;
+            }
+#pragma unroll
+            for (int m = 0; m < NSQ; ++m) {
+                double s = 0.0;
+#pragma unroll
+                for (int b = 0; b < NCQ; ++b) s += c_c2s[c2s_offset(LQ) + m * NCQ + b] * h[b];
+                acc[m] += pref * s;
+            }
+        }
+    }
+    double* row = M + (int64_t)(P.fn + mp) * ldm + Q.fn;
+#pragma unroll
+    for (int m = 0; m < NSQ; ++m) row[m] = acc[m];
+}
+
+template <int LP, int LQ>
+static cudaError_t metric_one(const DevShell* aux, const double* exps, const double* coefs, const int* plist, int np,
+                              const int* qlist, int nq, const double* btable, double* M, int64_t ldm,
+                              cudaStream_t stream) {
+    const int64_t total = (int64_t)np * nsph(LP) * nq;
+    if (total == 0) return cudaSuccess;
+    const int64_t blocks = (total + 127) / 128;
+    k_metric<LP, LQ><<<(unsigned)blocks, 128, 0, stream>>>(aux, exps, coefs, plist, np, qlist, nq, btable, M, ldm);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_metric(const DevShell* aux, const double* exps, const double* coefs,
+                          const int* const* aux_by_l, const int* count, const double* btable, double* M,
+                          int64_t ldm, cudaStream_t stream) {
+    cudaError_t e = cudaSuccess;
+#define HF_METRIC(LP, LQ)                                                                                    \
+    if (e == cudaSuccess)                                                                                    \
+        e = metric_one<LP, LQ>(aux, exps, coefs, aux_by_l[LP], count[LP], aux_by_l[LQ], count[LQ], btable, M, \
+                               ldm, stream);
+#define HF_METRIC_ROW(LP) HF_METRIC(LP, 0) HF_METRIC(LP, 1) HF_METRIC(LP, 2) HF_METRIC(LP, 3) HF_METRIC(LP, 4)
+    HF_METRIC_ROW(0)
+    HF_METRIC_ROW(1)
+    HF_METRIC_ROW(2)
+    HF_METRIC_ROW(3)
+    HF_METRIC_ROW(4)
+#undef HF_METRIC_ROW
+#undef HF_METRIC
+    return e;
+}
+
+// ------------------------------------------------------------ (P|mu nu)
+// One CTA per orbital shell pair of class (LA <= LB); its threads run over the
+// auxiliary shells of class LP, one thread per (aux shell, m_P). The pair's
+// primitive data and spherical Hermite coefficients sit in shared memory and
+// are read by every thread at the same address (broadcast).
+template <int LA, int LB>
+struct PairLayout {
+    static constexpr int NSA = nsph(LA), NSB = nsph(LB), NSAB = NSA * NSB;
+    static constexpr int KA = kMaxOrbContr[LA], KB = kMaxOrbContr[LB], KK = KA * KB;
+    static constexpr int NH = ntet(LA + LB);
+    // per primitive pair: p, Px, Py, Pz, cc[KK], Etil[NSAB][NH]
+    static constexpr int STRIDE = 4 + KK + NSAB * NH;
+};
+
+template <int LA, int LB>
+__device__ void pair_prologue(const DevShell& A, const DevShell& B, const double* __restrict__ exps,
+                              const double* __restrict__ coefs, double* smem) {
+    using PL = PairLayout<LA, LB>;
+    constexpr int NCA = ncart(LA), NCB = ncart(LB);
+    const int npp = A.nprim * B.nprim;
+    const double abx = A.x - B.x, aby = A.y - B.y, abz = A.z - B.z;
+    const double rab2 = abx * abx + aby * aby + abz * abz;
+    for (int pp = threadIdx.x; pp < npp; pp += blockDim.x) {
+        const int i = pp / B.nprim, j = pp % B.nprim;
+        const double a = exps[A.prim + i], b = exps[B.prim + j];
+        const double p = a + b;
+        const double mu = a * b / p;
+        const double px = (a * A.x + b * B.x) / p, py = (a * A.y + b * B.y) / p, pz = (a * A.z + b * B.z) / p;
+        double* s = smem + pp * PL::STRIDE;
+        s[0] = p;
+        s[1] = px;
+        s[2] = py;
+        s[3] = pz;
+#pragma unroll
+        for (int ka = 0; ka < PL::KA; ++ka)
+#pragma unroll
+            for (int kb = 0; kb < PL::KB; ++kb)
+                s[4 + ka * PL::KB + kb] = (ka < A.ncontr && kb < B.ncontr)
+                                              ? coefs[A.coef + ka * A.nprim + i] * coefs[B.coef + kb * B.nprim + j]
+                                              : 0.0;
+        Hermite1D<LA, LB> ex, ey, ez;
+        const double e00 = exp(-mu * rab2);
+        ex.build(p, e00, px - A.x, px - B.x);
+        ey.build(p, 1.0, py - A.y, py - B.y);
+        ez.build(p, 1.0, pz - A.z, pz - B.z);
+        double* et = s + 4 + PL::KK;
+        for (int k = 0; k < PL::NSAB * PL::NH; ++k) et[k] = 0.0;
+#pragma unroll 1
+        for (int ca = 0; ca < NCA; ++ca)
+#pragma unroll 1
+            for (int cb = 0; cb < NCB; ++cb) {
+                const int ix = c_cart[LA][ca][0], iy = c_cart[LA][ca][1], iz = c_cart[LA][ca][2];
+                const int jx = c_cart[LB][cb][0], jy = c_cart[LB][cb][1], jz = c_cart[LB][cb][2];
+#pragma unroll 1
+                for (int t = 0; t <= ix + jx; ++t)
+#pragma unroll 1
+                    for (int u = 0; u <= iy + jy; ++u)
+#pragma unroll 1
+                        for (int v = 0; v <= iz + jz; ++v) {
+                            const double w = ex.e[ix][jx][t] * ey.e[iy][jy][u] * ez.e[iz][jz][v];
+#pragma unroll 1
+                            for (int ma = 0; ma < PL::NSA; ++ma) {
+                                const double wa = c_c2s[c2s_offset(LA) + ma * NCA + ca] * w;
+                                if (wa == 0.0) continue;
+#pragma unroll 1
+                                for (int mb = 0; mb < PL::NSB; ++mb)
+                                    et[(ma * PL::NSB + mb) * PL::NH + tet(t, u, v)] +=
+                                        c_c2s[c2s_offset(LB) + mb * NCB + cb] * wa;
+                            }
+                        }
+            }
+    }
+}
+
+template <int LA, int LB, int LP>
+__global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict__ tasks,
+                                                      const DevShell* __restrict__ orb,
+                                                      const DevShell* __restrict__ aux,
+                                                      const double* __restrict__ exps,
+                                                      const double* __restrict__ coefs,
+                                                      const int* __restrict__ alist, int nalist,
+                                                      const double* __restrict__ btable, ChunkDesc chunk,
+                                                      double* __restrict__ T) {
+    using PL = PairLayout<LA, LB>;
+    constexpr int L = LA + LB + LP;
+    constexpr int LAB = LA + LB;
+    constexpr int NCP = ncart(LP), NSP = nsph(LP);
+    constexpr int SPB = 128 / NSP;  // aux shells per CTA
+    extern __shared__ double smem[];
+    const PairTask task = tasks[blockIdx.x];
+    const DevShell A = orb[task.swap ? task.second : task.first];
+    const DevShell B = orb[task.swap ? task.first : task.second];
+    pair_prologue<LA, LB>(A, B, exps, coefs, smem);
+    __syncthreads();
+
+    const int slot = threadIdx.x / NSP, mp = threadIdx.x % NSP;
+    const int ia = blockIdx.y * SPB + slot;
+    if (slot >= SPB || ia >= nalist) return;
+    const DevShell P = aux[alist[ia]];
+    double crow[NCP];
+#pragma unroll
+    for (int c = 0; c < NCP; ++c) crow[c] = c_c2s[c2s_offset(LP) + mp * NCP + c];
+
+    double acc[PL::KK][PL::NSAB];
+#pragma unroll
+    for (int k = 0; k < PL::KK; ++k)
+#pragma unroll
+        for (int m = 0; m < PL::NSAB; ++m) acc[k][m] = 0.0;
+
+    const int npp = A.nprim * B.nprim;
+    for (int i = 0; i < P.nprim; ++i) {
+        const double q = exps[P.prim + i];
+        double cq = coefs[P.coef + i] * pow(2.0 * q, -(double)LP);
+        if (LP & 1) cq = -cq;
+        for (int pp = 0; pp < npp; ++pp) {
+            const double* s = smem + pp * PL::STRIDE;
+            const double p = s[0];
+            const double alpha = p * q / (p + q);
+            double R[ntet(L)];
+            hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, R);
+            double G[ntet(LAB)];
+#pragma unroll 1
+            for (int h = 0; h < ntet(LAB); ++h) {
+                const int tu = c_tet_t[h], uu = c_tet_u[h], vu = c_tet_v[h];
+                double g = 0.0;
+#pragma unroll 1
+                for (int c = 0; c < NCP; ++c)
+                    g += crow[c] * R[tet(tu + c_cart[LP][c][0], uu + c_cart[LP][c][1], vu + c_cart[LP][c][2])];
+                G[h] = g;
+            }
+            const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * cq;
+            const double* et = s + 4 + PL::KK;
+#pragma unroll
+            for (int m = 0; m < PL::NSAB; ++m) {
+                double val = 0.0;
+#pragma unroll 1
+                for (int h = 0; h < PL::NH; ++h) val += et[m * PL::NH + h] * G[h];
+                val *= pref;
+#pragma unroll
+                for (int k = 0; k < PL::KK; ++k) acc[k][m] += s[4 + k] * val;
+            }
+        }
+    }
+
+    // Scatter into the chunk: element (mu, nu) in AO order, both orders where the
+    // tile is on or above the diagonal and its row belongs to this chunk.
+    const int same = task.first == task.second;
+    const int q0 = P.fn + mp;
+#pragma unroll
+    for (int ka = 0; ka < PL::KA; ++ka)
+#pragma unroll
+        for (int kb = 0; kb < PL::KB; ++kb) {
+            if (ka >= A.ncontr || kb >= B.ncontr) continue;
+#pragma unroll
+            for (int ma = 0; ma < PL::NSA; ++ma)
+#pragma unroll
+                for (int mb = 0; mb < PL::NSB; ++mb) {
+                    const double v = acc[ka * PL::KB + kb][ma * PL::NSB + mb];
+                    int mu = A.fn + ka * PL::NSA + ma;
+                    int nu = B.fn + kb * PL::NSB + mb;
+                    if (task.swap) {
+                        const int tmp = mu;
+                        mu = nu;
+                        nu = tmp;
+                    }
+                    if (same && mu > nu) continue;
+#pragma unroll
+                    for (int o = 0; o < 2; ++o) {
+                        const int r = (o ? nu : mu), c = (o ? mu : nu);
+                        if (o && r == c) break;
+                        const int tr = r >> 6, tc = c >> 6;
+                        if (tr < chunk.row0 || tr >= chunk.row1 || tc < tr) continue;
+                        const int64_t col = (tile_index(tr, tc, chunk.nt) - chunk.tile_base) * 4096 +
+                                            (r & 63) * 64 + (c & 63);
+                        T[col * chunk.ld + q0] = v;
+                    }
+                }
+        }
+}
+
+template <int LA, int LB, int LP>
+static cudaError_t three_center_one(const PairTask* tasks, int ntasks, int max_npp, const DevShell* orb,
+                                    const DevShell* aux, const double* exps, const double* coefs,
+                                    const int* alist, int nalist, const double* btable, ChunkDesc chunk,
+                                    double* T, cudaStream_t stream) {
+    if (ntasks == 0 || nalist == 0) return cudaSuccess;
+    constexpr int SPB = 128 / nsph(LP);
+    const size_t smem = sizeof(double) * (size_t)max_npp * PairLayout<LA, LB>::STRIDE;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_three_center<LA, LB, LP>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid(ntasks, (nalist + SPB - 1) / SPB);
+    k_three_center<LA, LB, LP><<<grid, 128, smem, stream>>>(tasks, orb, aux, exps, coefs, alist, nalist, btable,
+                                                            chunk, T);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_three_center(int la, int lb, const PairTask* tasks, int ntasks, int max_npp, const DevShell* orb,
+                                const DevShell* aux, const double* exps, const double* coefs,
+                                const int* const* aux_by_l, const int* count, const double* btable,
+                                ChunkDesc chunk, double* T, cudaStream_t stream) {
+    cudaError_t e = cudaSuccess;
+#define HF_3C(LA, LB, LP)                                                                                     \
+    if (e == cudaSuccess && la == LA && lb == LB)                                                             \
+        e = three_center_one<LA, LB, LP>(tasks, ntasks, max_npp, orb, aux, exps, coefs, aux_by_l[LP], count[LP], \
+                                         btable, chunk, T, stream);
+#define HF_3C_P(LA, LB) HF_3C(LA, LB, 0) HF_3C(LA, LB, 1) HF_3C(LA, LB, 2) HF_3C(LA, LB, 3) HF_3C(LA, LB, 4)
+    HF_3C_P(0, 0)
+    HF_3C_P(0, 1)
+    HF_3C_P(0, 2)
+    HF_3C_P(1, 1)
+    HF_3C_P(1, 2)
+    HF_3C_P(2, 2)
+#undef HF_3C_P
+#undef HF_3C
+    return e;
+}
+
+// ---------------------------------------------------------- S, T and V
+template <int LA, int LB, int KIND>
+__global__ void __launch_bounds__(128) k_one_electron(const int2* __restrict__ tasks, int ntasks,
+                                                      const DevShell* __restrict__ orb,
+                                                      const double* __restrict__ exps,
+                                                      const double* __restrict__ coefs,
+                                                      const double* __restrict__ charges,
+                                                      const double* __restrict__ positions, int natoms,
+                                                      const double* __restrict__ btable, double* __restrict__ out,
+                                                      int64_t n) {
+    constexpr int NCA = ncart(LA), NCB = ncart(LB), NSA = nsph(LA), NSB = nsph(LB);
+    constexpr int KA = kMaxOrbContr[LA], KB = kMaxOrbContr[LB];
+    constexpr int XB = (KIND == 1) ? 2 : 0;
+    constexpr int LAB = LA + LB;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntasks) return;
+    const int2 task = tasks[t];
+    const DevShell A = orb[task.x];
+    const DevShell B = orb[task.y];
+    double acc[KA * KB][NSA * NSB];
+#pragma unroll
+    for (int k = 0; k < KA * KB; ++k)
+#pragma unroll
+        for (int m = 0; m < NSA * NSB; ++m) acc[k][m] = 0.0;
+    const double abx = A.x - B.x, aby = A.y - B.y, abz = A.z - B.z;
+    const double rab2 = abx * abx + aby * aby + abz * abz;
+    for (int i = 0; i < A.nprim; ++i)
+        for (int j = 0; j < B.nprim; ++j) {
+            const double a = exps[A.prim + i], b = exps[B.prim + j];
+            const double p = a + b, mu = a * b / p;
+            const double px = (a * A.x + b * B.x) / p, py = (a * A.y + b * B.y) / p, pz = (a * A.z + b * B.z) / p;
+            Hermite1D<LA, LB + XB> ex, ey, ez;
+            ex.build(p, exp(-mu * rab2), px - A.x, px - B.x);
+            ey.build(p, 1.0, py - A.y, py - B.y);
+            ez.build(p, 1.0, pz - A.z, pz - B.z);
+            double cart[NCA][NCB];
+            if (KIND == 2) {
+                double Rs[ntet(LAB)];
+#pragma unroll
+                for (int h = 0; h < ntet(LAB); ++h) Rs[h] = 0.0;
+                for (int c = 0; c < natoms; ++c) {
+                    double R[ntet(LAB)];
+                    hermite_r<LAB>(p, px - positions[3 * c], py - positions[3 * c + 1], pz - positions[3 * c + 2],
+                                   btable, R);
+                    const double z = charges[c];
+#pragma unroll
+                    for (int h = 0; h < ntet(LAB); ++h) Rs[h] -= z * R[h];
+                }
+                const double pref = 2.0 * kPi / p;
+#pragma unroll
+                for (int ca = 0; ca < NCA; ++ca)
+#pragma unroll
+                    for (int cb = 0; cb < NCB; ++cb) {
+                        const int ix = cart_x(LA, ca), iy = cart_y(LA, ca), iz = cart_z(LA, ca);
+                        const int jx = cart_x(LB, cb), jy = cart_y(LB, cb), jz = cart_z(LB, cb);
+                        double s = 0.0;
+#pragma unroll
+                        for (int tt = 0; tt <= ix + jx; ++tt)
+#pragma unroll
+                            for (int u = 0; u <= iy + jy; ++u)
+#pragma unroll
+                                for (int v = 0; v <= iz + jz; ++v)
+                                    s += ex.e[ix][jx][tt] * ey.e[iy][jy][u] * ez.e[iz][jz][v] * Rs[tet(tt, u, v)];
+                        cart[ca][cb] = pref * s;
+                    }
+            } else {
+                const double ov = pow(kPi / p, 1.5);
+#pragma unroll
+                for (int ca = 0; ca < NCA; ++ca)
+#pragma unroll
+                    for (int cb = 0; cb < NCB; ++cb) {
+                        const int ix = cart_x(LA, ca), iy = cart_y(LA, ca), iz = cart_z(LA, ca);
+                        const int jx = cart_x(LB, cb), jy = cart_y(LB, cb), jz = cart_z(LB, cb);
+                        const double sx = ex.e[ix][jx][0], sy = ey.e[iy][jy][0], sz = ez.e[iz][jz][0];
+                        if (KIND == 0) {
+                            cart[ca][cb] = ov * sx * sy * sz;
+                        } else {
+                            // <x^i | d^2/dx^2 | x^j> / sqrt(pi/p) (pairs.rs:41-52, Helgaker 9.3.33)
+                            auto d2 = [&](const Hermite1D<LA, LB + XB>& e, int ii, int jj) {
+                                double v = 4.0 * b * b * e.e[ii][jj + 2 < LB + XB + 1 ? jj + 2 : 0][0] -
+                                           2.0 * b * (2 * jj + 1) * e.e[ii][jj][0];
+                                if (jj >= 2) v += jj * (jj - 1) * e.e[ii][jj - 2][0];
+                                return v;
+                            };
+                            cart[ca][cb] = -0.5 * ov *
+                                           (d2(ex, ix, jx) * sy * sz + sx * d2(ey, iy, jy) * sz + sx * sy * d2(ez, iz, jz));
+                        }
+                    }
+            }
+#pragma unroll
+            for (int ma = 0; ma < NSA; ++ma)
+#pragma unroll
+                for (int mb = 0; mb < NSB; ++mb) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int ca = 0; ca < NCA; ++ca) {
+                        const double ta = c_c2s[c2s_offset(LA) + ma * NCA + ca];
+                        if (ta == 0.0) continue;
+#pragma unroll
+                        for (int cb = 0; cb < NCB; ++cb) s += ta * c_c2s[c2s_offset(LB) + mb * NCB + cb] * cart[ca][cb];
+                    }
+#pragma unroll
+                    for (int ka = 0; ka < KA; ++ka)
+#pragma unroll
+                        for (int kb = 0; kb < KB; ++kb) {
+                            if (ka >= A.ncontr || kb >= B.ncontr) continue;
+                            acc[ka * KB + kb][ma * NSB + mb] +=
+                                coefs[A.coef + ka * A.nprim + i] * coefs[B.coef + kb * B.nprim + j] * s;
+                        }
+                }
+        }
+#pragma unroll
+    for (int ka = 0; ka < KA; ++ka)
+#pragma unroll
+        for (int kb = 0; kb < KB; ++kb) {
+            if (ka >= A.ncontr || kb >= B.ncontr) continue;
+#pragma unroll
+            for (int ma = 0; ma < NSA; ++ma)
+#pragma unroll
+                for (int mb = 0; mb < NSB; ++mb)
+                    out[(int64_t)(A.fn + ka * NSA + ma) * n + B.fn + kb * NSB + mb] = acc[ka * KB + kb][ma * NSB + mb];
+        }
+}
+
+template <int LA, int LB, int KIND>
+static cudaError_t one_electron_one(const int2* tasks, int ntasks, const DevShell* orb, const double* exps,
+                                    const double* coefs, const double* charges, const double* positions, int natoms,
+                                    const double* btable, double* out, int64_t n, cudaStream_t stream) {
+    if (ntasks == 0) return cudaSuccess;
+    k_one_electron<LA, LB, KIND><<<(ntasks + 127) / 128, 128, 0, stream>>>(tasks, ntasks, orb, exps, coefs, charges,
+                                                                          positions, natoms, btable, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_one_electron(int kind, int la, int lb, const int2* tasks, int ntasks, const DevShell* orb,
+                                const double* exps, const double* coefs, const double* charges,
+                                const double* positions, int natoms, const double* btable, double* out, int64_t n,
+                                cudaStream_t stream) {
+    cudaError_t e = cudaSuccess;
+#define HF_1E(K, LA, LB)                                                                                        \
+    if (kind == K && la == LA && lb == LB)                                                                      \
+        e = one_electron_one<LA, LB, K>(tasks, ntasks, orb, exps, coefs, charges, positions, natoms, btable, out, \
+                                        n, stream);
+#define HF_1E_K(K)                                                                                  \
+    HF_1E(K, 0, 0) HF_1E(K, 0, 1) HF_1E(K, 0, 2) HF_1E(K, 1, 0) HF_1E(K, 1, 1) HF_1E(K, 1, 2) HF_1E(K, 2, 0) \
+    HF_1E(K, 2, 1) HF_1E(K, 2, 2)
+    HF_1E_K(0)
+    HF_1E_K(1)
+    HF_1E_K(2)
+#undef HF_1E_K
+#undef HF_1E
+    return e;
+}
+
+}  // namespace hf

@@ -1,0 +1,63 @@
+// Host-visible declarations of the integral kernels' launch helpers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+namespace hf {
+
+// One shell on the device. `fn` is the first orbital function (AO order) for
+// orbital shells and the first internal auxiliary index for auxiliary shells.
+struct DevShell {
+    double x, y, z;
+    int l, nprim, ncontr, prim, coef, fn;
+};
+
+// The part of the packed fitted tensor a three-centre launch fills: tile rows
+// [row0, row1) of the upper triangle of 64x64 (mu, nu) tiles, laid out as
+// T[col][q] with col = (tile - tile_base) * 4096 + (mu % 64) * 64 + nu % 64.
+struct ChunkDesc {
+    int row0, row1, nt;
+    int64_t tile_base;
+    int64_t ld;  // leading dimension (number of auxiliary functions, padded)
+};
+
+__host__ __device__ inline int64_t tile_index(int I, int J, int nt) {
+    return (int64_t)I * nt - (int64_t)I * (I - 1) / 2 + (J - I);
+}
+
+// A shell pair task: orbital shells a <= b in AO order. `swap` marks a pair
+// evaluated with the roles of a and b exchanged (so that l_first <= l_second).
+struct PairTask {
+    int first, second, swap, pad;
+};
+
+struct ShellClassLists {
+    // orbital pairs bucketed by (la, lb) with la <= lb: 3x3 buckets (only la<=lb used)
+    std::vector<PairTask> pairs[3][3];
+    int max_npp[3][3] = {};
+};
+
+void upload_c2s(cudaStream_t stream);
+std::vector<double> boys_grid_host();
+
+// (P|Q) for all aux shells into M[N][N] (internal order, row-major, ld = ldm).
+cudaError_t launch_metric(const DevShell* aux, const double* exps, const double* coefs,
+                          const int* const* aux_by_l_dev, const int* aux_count, const double* btable,
+                          double* M, int64_t ldm, cudaStream_t stream);
+
+// (P|ab) for the given pair tasks of class (la, lb) and all aux shells, into a chunk.
+cudaError_t launch_three_center(int la, int lb, const PairTask* tasks, int ntasks, int max_npp,
+                                const DevShell* orb, const DevShell* aux, const double* exps,
+                                const double* coefs, const int* const* aux_by_l_dev, const int* aux_count,
+                                const double* btable, ChunkDesc chunk, double* T, cudaStream_t stream);
+
+// S, T (kinetic) or V (attraction to point charges) over all ordered shell pairs
+// of class (la, lb) into out[n][n] (AO order). kind: 0 S, 1 T, 2 V.
+cudaError_t launch_one_electron(int kind, int la, int lb, const int2* tasks, int ntasks, const DevShell* orb,
+                                const double* exps, const double* coefs, const double* charges,
+                                const double* positions, int natoms, const double* btable, double* out,
+                                int64_t n, cudaStream_t stream);
+
+}  // namespace hf

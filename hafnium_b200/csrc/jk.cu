@@ -1,0 +1,294 @@
+// Coulomb and exchange builds over the packed fitted tensor.
+//
+// Reference: hafnium/scf/coulomb_exchange.py:176-190. The reference holds B as
+// [aux, ao, ao] and computes J = (B . vec D) . B and K = sum_P B_P D B_P. Here B
+// is stored once per auxiliary index as the upper-triangle 64x64 tiles of
+// B_P (layout: B[q][tile][64][64], tile (I, J >= I) at I*nt - I(I-1)/2 + J - I):
+//
+//   J:  c_q = sum_t w_t <B_q[t], D[t]>  (w = 1 on diagonal tiles, 2 above), then
+//       J[t] = sum_q c_q B_q[t]; both passes stream B once from HBM.
+//   K:  with D = C W C^T (W diagonal), X_q = B_q C and K = sum_q X_q W X_q^T.
+//       The half-transform runs per q on DMMA tensor cores reading the tiles of
+//       B_q (transposed for tiles below the diagonal); the second product is a
+//       GEMM over the q-chunk, only upper 64x64 output tiles computed.
+#include <cmath>
+
+#include "dgemm.cuh"
+#include "jk.cuh"
+
+namespace hf {
+
+namespace {
+
+// Dw[t][r][c] = w_t D[64I + r][64J + c], zero outside n.
+__global__ void k_pack_density(const double* __restrict__ D, int64_t n, int nt, double* __restrict__ Dw) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t ntiles = (int64_t)nt * (nt + 1) / 2;
+    if (e >= ntiles * 4096) return;
+    const int64_t t = e >> 12;
+    const int r = (int)((e >> 6) & 63), c = (int)(e & 63);
+    // tile index -> (I, J): rows of the upper triangle, row I holds nt - I tiles
+    int I = 0;
+    int64_t base = 0;
+    while (base + (nt - I) <= t) {
+        base += nt - I;
+        ++I;
+    }
+    const int J = I + (int)(t - base);
+    const int64_t mu = 64 * (int64_t)I + r, nu = 64 * (int64_t)J + c;
+    double v = 0.0;
+    if (mu < n && nu < n) v = (I == J ? 1.0 : 2.0) * D[mu * n + nu];
+    Dw[e] = v;
+}
+
+// c[q] = sum_e B[q][e] Dw[e]; one CTA per q, 128-bit loads.
+__global__ void __launch_bounds__(512) k_coulomb_charges(const double* __restrict__ B, int64_t ldb, int64_t nelem,
+                                                         const double* __restrict__ Dw, double* __restrict__ c) {
+    const int q = blockIdx.x;
+    const double2* row = reinterpret_cast<const double2*>(B + (int64_t)q * ldb);
+    const double2* d = reinterpret_cast<const double2*>(Dw);
+    const int64_t n2 = nelem / 2;
+    double s0 = 0.0, s1 = 0.0;
+    int64_t i = threadIdx.x;
+    for (; i + 3 * blockDim.x < n2; i += 4 * blockDim.x) {
+        double2 b0 = __ldcs(row + i), b1 = __ldcs(row + i + blockDim.x), b2 = __ldcs(row + i + 2 * blockDim.x),
+                b3 = __ldcs(row + i + 3 * blockDim.x);
+        double2 d0 = __ldg(d + i), d1 = __ldg(d + i + blockDim.x), d2 = __ldg(d + i + 2 * blockDim.x),
+                d3 = __ldg(d + i + 3 * blockDim.x);
+        s0 += b0.x * d0.x + b1.x * d1.x + b2.x * d2.x + b3.x * d3.x;
+        s1 += b0.y * d0.y + b1.y * d1.y + b2.y * d2.y + b3.y * d3.y;
+    }
+    for (; i < n2; i += blockDim.x) {
+        double2 b0 = __ldcs(row + i), d0 = __ldg(d + i);
+        s0 += b0.x * d0.x;
+        s1 += b0.y * d0.y;
+    }
+    double s = s0 + s1;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ double part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = (threadIdx.x < blockDim.x / 32) ? part[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) c[q] = v;
+    }
+}
+
+// Jt[e] += sum_{q in slab} c[q] B[q][e]; each thread owns two adjacent elements.
+constexpr int kJSlab = 256;
+__global__ void __launch_bounds__(256) k_coulomb_assemble(const double* __restrict__ B, int64_t ldb, int64_t nelem,
+                                                          int naux, const double* __restrict__ c,
+                                                          double* __restrict__ Jt) {
+    const int64_t e2 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (2 * e2 >= nelem) return;
+    const int q0 = blockIdx.y * kJSlab;
+    const int q1 = min(naux, q0 + kJSlab);
+    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+    int q = q0;
+    for (; q + 1 < q1; q += 2) {
+        const double2 x = __ldcs(reinterpret_cast<const double2*>(B + (int64_t)q * ldb) + e2);
+        const double2 y = __ldcs(reinterpret_cast<const double2*>(B + (int64_t)(q + 1) * ldb) + e2);
+        const double cq = __ldg(c + q), cr = __ldg(c + q + 1);
+        a0 += cq * x.x;
+        a1 += cq * x.y;
+        b0 += cr * y.x;
+        b1 += cr * y.y;
+    }
+    if (q < q1) {
+        const double2 x = __ldcs(reinterpret_cast<const double2*>(B + (int64_t)q * ldb) + e2);
+        const double cq = __ldg(c + q);
+        a0 += cq * x.x;
+        a1 += cq * x.y;
+    }
+    atomicAdd(Jt + 2 * e2, a0 + b0);
+    atomicAdd(Jt + 2 * e2 + 1, a1 + b1);
+}
+
+// Full symmetric matrix from upper 64x64 tiles: J[mu][nu] = tiles(min, max).
+__global__ void k_unpack_tiles(const double* __restrict__ Jt, int64_t n, int nt, double* __restrict__ J) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * n) return;
+    int64_t mu = e / n, nu = e % n;
+    int I = (int)(mu >> 6), Jc = (int)(nu >> 6);
+    if (I > Jc) {
+        const int64_t t = mu;
+        mu = nu;
+        nu = t;
+        const int ti = I;
+        I = Jc;
+        Jc = ti;
+    }
+    const int64_t tile = (int64_t)I * nt - (int64_t)I * (I - 1) / 2 + (Jc - I);
+    J[e] = Jt[tile * 4096 + (mu & 63) * 64 + (nu & 63)];
+}
+
+// K[mu][nu] from the upper-tile-valid padded matrix Kp (row stride ldk).
+__global__ void k_symmetrize_upper(const double* __restrict__ Kp, int64_t ldk, int64_t n, double* __restrict__ K) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * n) return;
+    const int64_t mu = e / n, nu = e % n;
+    const bool upper = (mu >> 6) <= (nu >> 6);
+    K[e] = upper ? Kp[mu * ldk + nu] : Kp[nu * ldk + mu];
+}
+
+// X[p][ql][i] = sum_r B_q[p][r] Ct[i][r] for q = q0 + ql, p in row tile I.
+constexpr int BM = 64, BN = 64, BK = 16, LDS = 72;
+__global__ void __launch_bounds__(128) k_exchange_half(const double* __restrict__ B, int64_t ldb, int q0, int nt,
+                                                       const double* __restrict__ Ct, int64_t ldc_t, int npad,
+                                                       double* __restrict__ X, int64_t ldx, int opad) {
+    const int I = blockIdx.y;
+    const int n0 = blockIdx.x * BN;
+    const int ql = blockIdx.z;
+    const double* Bq = B + (int64_t)(q0 + ql) * ldb;
+    __shared__ double As[2][BK][LDS];
+    __shared__ double Bs[2][BK][LDS];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g8 = lane >> 2, t4 = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    double ra[8], rb[8];
+    // k-contiguous loader (row = tid>>1, 8 k) and m-contiguous loader (k = tid>>3, 8 m)
+    auto load = [&](int k0) {
+        const int Jt = k0 >> 6, kl = k0 & 63;
+        if (Jt >= I) {
+            const double* tile = Bq + ((int64_t)I * nt - (int64_t)I * (I - 1) / 2 + (Jt - I)) * 4096;
+            const double2* src = reinterpret_cast<const double2*>(tile + (tid >> 1) * 64 + kl + (tid & 1) * 8);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double2 v = __ldcs(src + j);
+                ra[2 * j] = v.x;
+                ra[2 * j + 1] = v.y;
+            }
+        } else {
+            const double* tile = Bq + ((int64_t)Jt * nt - (int64_t)Jt * (Jt - 1) / 2 + (I - Jt)) * 4096;
+            const double2* src = reinterpret_cast<const double2*>(tile + (kl + (tid >> 3)) * 64 + (tid & 7) * 8);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double2 v = __ldcs(src + j);
+                ra[2 * j] = v.x;
+                ra[2 * j + 1] = v.y;
+            }
+        }
+        const double2* bsrc = reinterpret_cast<const double2*>(Ct + (int64_t)(n0 + (tid >> 1)) * ldc_t + k0 + (tid & 1) * 8);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double2 v = __ldg(bsrc + j);
+            rb[2 * j] = v.x;
+            rb[2 * j + 1] = v.y;
+        }
+    };
+    auto store = [&](int buf, int k0) {
+        const int Jt = k0 >> 6;
+        if (Jt >= I) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) As[buf][(tid & 1) * 8 + j][tid >> 1] = ra[j];
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) As[buf][tid >> 3][(tid & 7) * 8 + j] = ra[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) Bs[buf][(tid & 1) * 8 + j][tid >> 1] = rb[j];
+    };
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    int buf = 0;
+    load(0);
+    store(0, 0);
+    __syncthreads();
+    for (int k0 = 0; k0 < npad; k0 += BK) {
+        const bool more = k0 + BK < npad;
+        if (more) load(k0 + BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = As[buf][kk + t4][wm + i * 8 + g8];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) bf[j] = Bs[buf][kk + t4][wn + j * 8 + g8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+        if (more) store(buf ^ 1, k0 + BK);
+        __syncthreads();
+        buf ^= 1;
+    }
+    double* xo = X + (int64_t)ql * opad;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int m = I * 64 + wm + i * 8 + g8;
+            const int nn = n0 + wn + j * 8 + 2 * t4;
+            *reinterpret_cast<double2*>(xo + (int64_t)m * ldx + nn) = make_double2(acc[i][j][0], acc[i][j][1]);
+        }
+}
+
+__global__ void k_scale_columns(const double* __restrict__ X, double* __restrict__ Xs, int64_t rows, int64_t ld,
+                                int opad, const double* __restrict__ sign) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= rows * ld) return;
+    Xs[e] = X[e] * sign[(e % ld) % opad];
+}
+
+}  // namespace
+
+cudaError_t coulomb_build(const JkPlan& p, const double* D, double* J, double* work, cudaStream_t stream) {
+    // work: Dw (ntiles*4096) | c (naux) | Jt (ntiles*4096)
+    const int64_t nelem = p.ntiles * 4096;
+    double* Dw = work;
+    double* c = work + nelem;
+    double* Jt = c + ((p.naux + 1) / 2) * 2;
+    k_pack_density<<<(unsigned)((nelem + 255) / 256), 256, 0, stream>>>(D, p.n, p.nt, Dw);
+    k_coulomb_charges<<<p.naux, 512, 0, stream>>>(p.B, p.ldb, nelem, Dw, c);
+    cudaMemsetAsync(Jt, 0, sizeof(double) * nelem, stream);
+    dim3 grid((unsigned)((nelem / 2 + 255) / 256), (p.naux + kJSlab - 1) / kJSlab);
+    k_coulomb_assemble<<<grid, 256, 0, stream>>>(p.B, p.ldb, nelem, p.naux, c, Jt);
+    const int64_t nn = p.n * p.n;
+    k_unpack_tiles<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(Jt, p.n, p.nt, J);
+    return cudaGetLastError();
+}
+
+int64_t coulomb_work_doubles(const JkPlan& p) { return 2 * p.ntiles * 4096 + ((p.naux + 1) / 2) * 2; }
+
+cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int opad, const double* sign, double* K,
+                                double* Kp, double* X, double* Xs, int qchunk, cudaStream_t stream) {
+    const int64_t npad = (int64_t)p.nt * 64;
+    cudaMemsetAsync(Kp, 0, sizeof(double) * npad * npad, stream);
+    for (int q0 = 0; q0 < p.naux; q0 += qchunk) {
+        const int qc = (p.naux - q0 < qchunk) ? p.naux - q0 : qchunk;
+        const int64_t ldx = (int64_t)qc * opad;
+        dim3 grid(opad / 64, p.nt, qc);
+        k_exchange_half<<<grid, 128, 0, stream>>>(p.B, p.ldb, q0, p.nt, Ct, npad, (int)npad, X, ldx, opad);
+        const double* Xb = X;
+        if (sign != nullptr) {
+            const int64_t tot = npad * ldx;
+            k_scale_columns<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(X, Xs, npad, ldx, opad, sign);
+            Xb = Xs;
+        }
+        GemmArgs g{};
+        g.M = g.N = (int)npad;
+        g.K = (int)ldx;
+        g.A = X;
+        g.lda = ldx;
+        g.B = Xb;
+        g.ldb = ldx;
+        g.C = Kp;
+        g.ldc = npad;
+        g.alpha = 1.0;
+        g.beta = 1.0;
+        g.kmode = 0;
+        g.epi = 3;
+        cudaError_t e = dgemm_nt(g, 1, stream);
+        if (e != cudaSuccess) return e;
+    }
+    const int64_t nn = p.n * p.n;
+    k_symmetrize_upper<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(Kp, npad, p.n, K);
+    return cudaGetLastError();
+}
+
+}  // namespace hf

@@ -1,0 +1,348 @@
+"""A device-resident restatement of the reference's restricted SCF driver.
+
+Follows hafnium/scf/driver.py:154-213 (loop), 248-260 (orbital gradient),
+307-329 (canonically orthogonalised eigh, next density), 331-366 (finish),
+385-389 (convergence test); hafnium/scf/diis.py:55-106 (Pulay DIIS, bordered
+system by eigh with the null space dropped); hafnium/scf/orthogonalization.py:16-42;
+hafnium/scf/hamiltonian.py:331-370 (restricted Fock build and energy terms);
+hafnium/scf/occupation.py:321-370 (aufbau and averaged filling). Every matrix
+stays on the GPU in float64 (torch for the eigensolves); J and K come from
+``libhfjk.so``. The exchange is built from the occupied orbitals the driver
+already holds (D = C_occ C_occ^T), which is the same contraction as K(D).
+
+The reference driver itself is unchanged and can use the drop-in builder
+directly; this module exists so that a whole SCF runs on the device, which the
+benchmarks and the mixed-precision schedule need.
+"""
+
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from hafnium_b200 import _lib
+from hafnium_b200.basis import ShellTable
+from hafnium_b200.errors import ConvergenceError, InputError
+from hafnium_b200.jk import B200DensityFittedCoulombExchange
+
+NULL_SPACE_TOLERANCE = 1e-14  # diis.py:17
+DEFAULT_OVERLAP_THRESHOLD = 1e-10  # orthogonalization.py:12
+FILL_TOLERANCE = 1e-12  # occupation.py:285
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+@dataclass(frozen=True)
+class ScfOptions:
+    """driver.py:38-66 (no level shift or damping on the device path)."""
+
+    max_iterations: int = 100
+    energy_tolerance: float = 1e-10
+    gradient_tolerance: float = 1e-6
+    diis_size: int = 8
+    overlap_threshold: float = DEFAULT_OVERLAP_THRESHOLD
+
+    def __post_init__(self) -> None:
+        if self.max_iterations < 1:
+            raise InputError("at least one iteration is needed")
+        if self.energy_tolerance <= 0.0 or self.gradient_tolerance <= 0.0:
+            raise InputError("tolerances must be positive")
+        if self.diis_size < 1:
+            raise InputError("the DIIS subspace holds at least one matrix")
+
+
+@dataclass(frozen=True)
+class PrecisionSchedule:
+    """Which arithmetic the exchange build uses per iteration.
+
+    ``fp64``: every build in FP64. ``mixed``: split-BF16 builds of the
+    incremental exchange K(D_new) = K(D_old) + K(dD) while the orbital gradient
+    is above ``switch_gradient``, then FP64 full rebuilds to the end.
+    """
+
+    mode: str = "fp64"
+    switch_gradient: float = 1e-4
+
+    def __post_init__(self) -> None:
+        if self.mode not in ("fp64", "mixed"):
+            raise InputError("the precision schedule is 'fp64' or 'mixed'")
+
+
+@dataclass
+class Iteration:
+    index: int
+    energy: float
+    energy_change: float
+    gradient_norm: float
+    precision: str = "fp64"
+
+
+@dataclass
+class ScfResult:
+    energy: float
+    density: object  # torch [n, n], per spin
+    fock: object
+    mo_energies: object
+    mo_coefficients: object
+    converged: bool
+    history: list = field(default_factory=list)
+    energy_terms: tuple = ()
+    seconds: float = 0.0
+    timings: dict = field(default_factory=dict)
+
+    @property
+    def n_iterations(self) -> int:
+        return len(self.history)
+
+
+class DeviceHamiltonian:
+    """Overlap, core Hamiltonian, nuclear repulsion and the fitted two-body term."""
+
+    def __init__(self, s, h, two_body: B200DensityFittedCoulombExchange, e_nuc: float, n_alpha: int,
+                 timings: dict | None = None) -> None:
+        self.s, self.h, self.two_body, self.e_nuc, self.n_alpha = s, h, two_body, e_nuc, n_alpha
+        self.timings = timings or {}
+
+    @property
+    def n_ao(self) -> int:
+        return self.two_body.n_ao
+
+    @classmethod
+    def build(cls, molecule, basis: str, auxiliary: str, *, device: int = 0) -> "DeviceHamiltonian":
+        torch = _torch()
+        t0 = time.perf_counter()
+        orb = ShellTable.build(basis, molecule.symbols, molecule.positions)
+        aux = ShellTable.build(auxiliary, molecule.symbols, molecule.positions)
+        ctx = _lib.Context(device)
+        ctx.upload(orb, aux)
+        dev = torch.device("cuda", device)
+        n = orb.n_functions
+        s = torch.empty((n, n), dtype=torch.float64, device=dev)
+        t = torch.empty_like(s)
+        v = torch.empty_like(s)
+        for kind, out, args in ((0, s, ()), (1, t, ()), (2, v, (molecule.nuclear_charges, molecule.positions))):
+            q = torch.as_tensor(args[0], dtype=torch.float64, device=dev) if args else None
+            r = torch.as_tensor(np.ascontiguousarray(args[1]), dtype=torch.float64, device=dev) if args else None
+            ctx.check(
+                ctx.lib.hf_one_electron(ctx.handle, kind, None if q is None else q.data_ptr(),
+                                        None if r is None else r.data_ptr(), 0 if q is None else q.shape[0],
+                                        out.data_ptr(), 1),
+                "hf_one_electron",
+            )
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        ctx.build()
+        torch.cuda.synchronize(dev)
+        t2 = time.perf_counter()
+        two_body = B200DensityFittedCoulombExchange(ctx)
+        timings = {"one_electron_s": t1 - t0, "fitted_tensor_s": t2 - t1, **ctx.stats()}
+        return cls(s, t + v, two_body, molecule.nuclear_repulsion_energy(), molecule.n_alpha, timings)
+
+
+def canonical_orthogonalizer(s, threshold: float = DEFAULT_OVERLAP_THRESHOLD):
+    """orthogonalization.py:16-42."""
+    torch = _torch()
+    w, v = torch.linalg.eigh(s)
+    n = s.shape[-1]
+    kept = int((w > threshold).sum())
+    if kept == 0:
+        raise InputError("no eigenvalue of the overlap exceeds the threshold")
+    return v[:, n - kept:] / torch.sqrt(w[n - kept:])[None, :]
+
+
+def solve_diis(overlaps: np.ndarray) -> np.ndarray:
+    """diis.py:82-106 on the host (an m x m system, m <= diis_size)."""
+    m = overlaps.shape[0]
+    scale = np.max(np.diagonal(overlaps))
+    b = overlaps / (scale if scale > 0.0 else 1.0)
+    system = np.zeros((m + 1, m + 1))
+    system[:m, :m] = b
+    system[:m, m] = -1.0
+    system[m, :m] = -1.0
+    right = np.zeros(m + 1)
+    right[m] = -1.0
+    w, v = np.linalg.eigh(system)
+    keep = np.abs(w) > NULL_SPACE_TOLERANCE * np.max(np.abs(w))
+    inv = np.where(keep, 1.0 / np.where(keep, w, 1.0), 0.0)
+    return (v @ (inv * (v.T @ right)))[:m]
+
+
+def fill_averaged(energies: np.ndarray, count: float, tolerance: float = 1e-6) -> np.ndarray:
+    """occupation.py:342-370: degenerate groups share electrons equally."""
+    order = np.argsort(energies, kind="stable")
+    values = energies[order]
+    spread = max(1.0, float(values[-1] - values[0])) if len(values) else 1.0
+    occ = np.zeros(len(energies))
+    remaining = count
+    start = 0
+    while start < len(order):
+        end = start + 1
+        while end < len(order) and values[end] - values[end - 1] <= tolerance * spread:
+            end += 1
+        group = order[start:end]
+        share = min(remaining, float(len(group))) / len(group)
+        occ[group] = share
+        remaining = max(remaining - share * len(group), 0.0)
+        start = end
+    if not math.isclose(remaining, 0.0, abs_tol=FILL_TOLERANCE):
+        raise InputError(f"cannot place {count} electrons in {len(energies)} levels")
+    return occ
+
+
+class _Rhf:
+    def __init__(self, ham: DeviceHamiltonian, options: ScfOptions, schedule: PrecisionSchedule,
+                 host_io: bool = False) -> None:
+        torch = _torch()
+        self.torch = torch
+        self.host_io = host_io
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
+        self.ham = ham
+        self.options = options
+        self.schedule = schedule
+        self.x = canonical_orthogonalizer(ham.s, options.overlap_threshold)
+        self.n = ham.n_ao
+        self.k_prev = None  # (factor, K) of the last mixed-precision build
+        self.timings = {"coulomb_ms": 0.0, "exchange_ms": 0.0, "eigh_ms": 0.0, "fock_builds": 0}
+
+    def solve(self, f):
+        w, v = self.torch.linalg.eigh(self.x.T @ f @ self.x)
+        return w, self.x @ v
+
+    def density(self, w, c, averaged: bool):
+        if averaged:
+            occ = fill_averaged(w.cpu().numpy(), float(self.ham.n_alpha))
+        else:
+            occ = np.zeros(w.shape[0])
+            occ[np.argsort(w.cpu().numpy(), kind="stable")[: self.ham.n_alpha]] = 1.0
+        keep = np.nonzero(occ > 0.0)[0]
+        idx = self.torch.as_tensor(keep, device=c.device)
+        occ_t = self.torch.as_tensor(occ[keep], dtype=self.torch.float64, device=c.device)
+        factor = (c[:, idx] * self.torch.sqrt(occ_t)[None, :]).contiguous()
+        return factor @ factor.T, factor
+
+    def exchange(self, d, factor, precision: str):
+        two_body = self.ham.two_body
+        if factor is None:
+            return two_body.exchange(d)
+        if precision == "fp64":
+            self.k_prev = None
+            return two_body.exchange_factored(factor)
+        # mixed: K(D) = K(D_prev) + K(dD), dD = [C | C_prev] diag(+1, -1) [C | C_prev]^T
+        if self.k_prev is None:
+            k = two_body.exchange_factored(factor)
+        else:
+            f_prev, k_prev = self.k_prev
+            both = self.torch.cat([factor, f_prev], dim=1).contiguous()
+            sign = self.torch.cat([
+                self.torch.ones(factor.shape[1], dtype=self.torch.float64, device=factor.device),
+                -self.torch.ones(f_prev.shape[1], dtype=self.torch.float64, device=factor.device),
+            ])
+            out = self.torch.empty_like(k_prev)
+            two_body.context.exchange_factored_device(both, out, sign, _lib.PREC_BF16X3)
+            k = k_prev + out
+        self.k_prev = (factor, k)
+        return k
+
+    def fock(self, d, factor, precision: str = "fp64"):
+        """hamiltonian.py:331-370 for one restricted block."""
+        torch = self.torch
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        if self.host_io:
+            # the reference-facing call: host NumPy density in, host NumPy J/K out
+            d_host = d.cpu().numpy()
+            j = torch.as_tensor(self.ham.two_body.coulomb(2.0 * d_host), device=d.device)
+            ev[1].record()
+            k = torch.as_tensor(self.ham.two_body.exchange(d_host), device=d.device)
+            nb = d_host.nbytes
+            self.h2d_bytes += 2 * nb
+            self.d2h_bytes += 2 * nb
+        else:
+            j = self.ham.two_body.coulomb((2.0 * d).contiguous())
+            ev[1].record()
+            k = self.exchange(d, factor, precision)
+        ev[2].record()
+        f = self.ham.h + j - k
+        e1 = 2.0 * torch.sum(d * self.ham.h)
+        ej = torch.sum(d * j)
+        ek = -torch.sum(d * k)
+        terms = torch.stack([e1, ej, ek]).cpu().numpy()
+        self.timings["coulomb_ms"] += ev[0].elapsed_time(ev[1])
+        self.timings["exchange_ms"] += ev[1].elapsed_time(ev[2])
+        self.timings["fock_builds"] += 1
+        energy = self.ham.e_nuc + float(terms.sum())
+        return f, (self.ham.e_nuc, *map(float, terms)), energy
+
+    def run(self, guess) -> ScfResult:
+        torch = self.torch
+        opts = self.options
+        t_start = time.perf_counter()
+        if guess is None:  # driver.py:230-236 averaged core-Hamiltonian density
+            w, c = self.solve(self.ham.h)
+            d, factor = self.density(w, c, averaged=True)
+        else:
+            d = torch.as_tensor(guess, dtype=torch.float64, device=self.ham.s.device)
+            factor = None
+        s = self.ham.s
+        focks, errors, history = [], [], []
+        precision = "fp64" if self.schedule.mode == "fp64" else "bf16x3"
+        f = None
+        for index in range(opts.max_iterations):
+            f, _, energy = self.fock(d, factor, precision)
+            g = self.x.T @ (f @ d @ s - s @ d @ f) @ self.x
+            gnorm = math.sqrt(2.0 * float(torch.sum(g * g)))
+            change = energy - history[-1].energy if history else math.inf
+            history.append(Iteration(index, energy, change, gnorm, precision))
+            if precision != "fp64" and gnorm < self.schedule.switch_gradient:
+                precision = "fp64"
+                # the mixed energies are not final: restart the convergence test in FP64
+                continue_fp64 = True
+            else:
+                continue_fp64 = False
+            if not continue_fp64 and precision == "fp64" and history[-1].precision == "fp64" and (
+                abs(change) < opts.energy_tolerance and gnorm < opts.gradient_tolerance
+            ):
+                return self.finish(f, history, True, t_start)
+            focks = (focks + [f])[-opts.diis_size:]
+            errors = (errors + [g])[-opts.diis_size:]
+            if len(focks) == 1:
+                extrapolated = focks[0]
+            else:
+                ov = torch.stack([torch.stack([2.0 * torch.sum(a * b) for b in errors]) for a in errors]).cpu().numpy()
+                coef = solve_diis(ov)
+                extrapolated = sum(float(cf) * fk for cf, fk in zip(coef, focks))
+            w, c = self.solve(extrapolated)
+            d, factor = self.density(w, c, averaged=False)
+        result = self.finish(focks[-1], history, False, t_start)
+        raise ConvergenceError(f"the SCF did not converge in {opts.max_iterations} iterations", result)
+
+    def finish(self, f, history, converged: bool, t_start: float) -> ScfResult:
+        w, c = self.solve(f)
+        d, factor = self.density(w, c, averaged=False)
+        final_f, terms, energy = self.fock(d, factor, "fp64")
+        self.ham.two_body.context.lib  # keep the context alive until here
+        self.torch.cuda.synchronize()
+        return ScfResult(energy, d, final_f, w, c, converged, history, terms, time.perf_counter() - t_start,
+                         dict(self.timings))
+
+
+def solve_rhf(ham: DeviceHamiltonian, *, guess=None, options: ScfOptions | None = None,
+              schedule: PrecisionSchedule | None = None, host_io: bool = False) -> ScfResult:
+    """Converge the restricted state of ``ham`` on the device (driver.py:154-213).
+
+    ``host_io`` routes every J and K through the drop-in's host-array API (NumPy
+    density in, NumPy J/K out), as the unchanged reference driver would call it.
+    """
+    rhf = _Rhf(ham, options or ScfOptions(), schedule or PrecisionSchedule(), host_io)
+    result = rhf.run(guess)
+    result.timings["h2d_bytes"] = rhf.h2d_bytes
+    result.timings["d2h_bytes"] = rhf.d2h_bytes
+    return result

@@ -1,0 +1,119 @@
+/* hfjk.h: C ABI of the B200 density-fitted Coulomb/exchange (J/K) builder.
+ *
+ * A drop-in for the molecular DensityFittedCoulombExchange of maxnus/hafnium:
+ *   hafnium/scf/coulomb_exchange.py:53-71   CoulombExchange protocol (n_ao, coulomb, exchange)
+ *   hafnium/scf/coulomb_exchange.py:125-190 DensityFittedCoulombExchange (from_molecule, J, K)
+ *   hafnium/integrals/density_fitting.py:59-107 DensityFitting.build / df_tensor
+ *   hafnium/integrals/native.py:16-24, 104-177 RustEngine 2c/3c + ShellTable marshalling
+ *   crates/hafnium-py/src/lib.rs:66-108, 352-423 the PyO3 entry points the shell table crosses
+ *
+ * Conventions: plain pointers and sizes, no exceptions cross this boundary,
+ * every entry point returns an hf_status. Host arrays are caller-owned; device
+ * arrays passed with on_device = 1 are raw CUDA pointers on the context's device.
+ * Matrices are row-major float64. One context per host thread / stream.
+ */
+#ifndef HFJK_H
+#define HFJK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hf_status {
+    HF_OK = 0,
+    HF_ERR_ARG = 1,      /* invalid argument or shell table (reference: ValueError, lib.rs:1118) */
+    HF_ERR_OOM = 2,      /* device allocation failed */
+    HF_ERR_CUDA = 3,     /* CUDA runtime error; see hf_last_error */
+    HF_ERR_TIMEOUT = 4,  /* a bounded device wait ran out */
+    HF_ERR_NUMERIC = 5,  /* metric not positive definite, or density not factorisable */
+    HF_ERR_STATE = 6     /* call order: shells not uploaded / tensor not built */
+} hf_status;
+
+typedef struct hf_ctx hf_ctx;
+
+/* Shells in structure-of-arrays form, the layout of hafnium's ShellTable
+ * (hafnium/integrals/shell_table.py:14-82, crates/.../integrals/mod.rs:63-173):
+ * one entry per shell with all its contractions; coefficients of bare
+ * primitives stored shell by shell as [contraction][primitive]. */
+typedef struct hf_shell_table {
+    int64_t n_shells;
+    const int64_t* angular_momenta;   /* [n_shells] */
+    const double* centers;            /* [n_shells][3], Bohr */
+    const int64_t* primitive_offsets; /* [n_shells + 1] */
+    const double* exponents;          /* [primitive_offsets[n_shells]] */
+    const double* coefficients;       /* [sum_s n_contractions[s] * n_prim(s)] */
+    const int64_t* n_contractions;    /* [n_shells] */
+} hf_shell_table;
+
+typedef enum hf_precision {
+    HF_PREC_FP64 = 0,      /* FP64 DMMA tensor cores */
+    HF_PREC_BF16X3 = 1     /* 3 split-BF16 products, FP32 accumulation (tcgen05) */
+} hf_precision;
+
+typedef struct hf_stats {
+    double ms_metric;       /* (P|Q) */
+    double ms_factor;       /* Cholesky + inverse of the factor */
+    double ms_three_center; /* (P|mu nu), all chunks */
+    double ms_fit;          /* B = L^-1 (P|mu nu), all chunks */
+    double ms_coulomb;      /* last J build */
+    double ms_exchange;     /* last K build */
+    double ms_factorize_density; /* last pivoted Cholesky of D (hf_exchange) */
+    double min_pivot_ratio; /* min Cholesky pivot^2 / max metric diagonal */
+    int64_t n_ao, n_aux, n_tiles;
+    int64_t b_bytes;        /* bytes of the packed fitted tensor */
+    int64_t exchange_rank;  /* columns of the last exchange factor */
+    int64_t kernel_launches;/* launches issued by this context so far */
+} hf_stats;
+
+/* Context lifetime (no reference counterpart: the reference's kernels are
+ * stateless functions over host arrays). */
+int hf_ctx_create(int device, hf_ctx** out);
+int hf_ctx_destroy(hf_ctx* ctx);
+const char* hf_last_error(const hf_ctx* ctx);
+/* Launch on this stream (cudaStream_t) from now on; NULL = the context's own. */
+int hf_set_stream(hf_ctx* ctx, void* stream);
+
+/* Upload the orbital and auxiliary shells (replaces the _kernels.ShellTable
+ * marshalling of native.py:16-24; validation of integrals/mod.rs:111-173). */
+int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbital, const hf_shell_table* auxiliary);
+
+/* (P|Q), its Cholesky factor and (P|mu nu) -> packed B = L^-1 (P|mu nu) on the
+ * device (replaces DensityFitting.build + df_tensor, density_fitting.py:59-107,
+ * and the Rust coulomb_two_center / coulomb_three_center, two_electron.rs:74-297). */
+int hf_build_fitted_tensor(hf_ctx* ctx);
+
+int hf_dims(const hf_ctx* ctx, int64_t* n_ao, int64_t* n_aux);
+
+/* J[u][v] = sum_wx (uv|wx) D[w][x] (coulomb_exchange.py:176-182). */
+int hf_coulomb(hf_ctx* ctx, const double* density, double* coulomb, int on_device);
+
+/* K[u][v] = sum_wx (uw|xv) D[w][x] (coulomb_exchange.py:184-190) for a symmetric
+ * positive semidefinite D, factorised on the device by a pivoted Cholesky;
+ * HF_ERR_NUMERIC when D is indefinite (use hf_exchange_factored then). */
+int hf_exchange(hf_ctx* ctx, const double* density, double* exchange, int precision, int on_device);
+
+/* K for D = C diag(w) C^T with C [n_ao][n_cols] row-major (w = NULL: all ones). */
+int hf_exchange_factored(hf_ctx* ctx, const double* factor, int64_t n_cols, const double* weights,
+                         double* exchange, int precision, int on_device);
+
+/* Parity / inspection entry points (small systems). Reference order of the
+ * auxiliary functions (the order of the auxiliary shell table). */
+int hf_metric(hf_ctx* ctx, double* out /* [n_aux][n_aux] host */);
+int hf_three_center(hf_ctx* ctx, double* out /* [n_aux][n_ao][n_ao] host */);
+/* B^T B contracted on the auxiliary index, (uv|wx) fitted, [n][n][n][n] host. */
+int hf_fitted_eri(hf_ctx* ctx, double* out);
+
+/* One-electron integrals over the orbital shells (one_electron.rs:40-190):
+ * kind 0 overlap, 1 kinetic, 2 attraction to point charges (charges [n_atoms],
+ * positions [n_atoms][3] Bohr). out: [n_ao][n_ao]. */
+int hf_one_electron(hf_ctx* ctx, int kind, const double* charges, const double* positions, int64_t n_atoms,
+                    double* out, int on_device);
+
+int hf_get_stats(const hf_ctx* ctx, hf_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HFJK_H */
