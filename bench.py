@@ -119,10 +119,11 @@ def measure_fp64_peak(torch, dev) -> float:
 
 
 def one_scf(torch, mol, dev, host_io=False):
-    from hafnium_b200.scf import DeviceHamiltonian, ScfOptions, solve_rhf
+    from hafnium_b200.scf import DeviceHamiltonian, ScfOptions, atomic_density_guess, solve_rhf
 
     ham = DeviceHamiltonian.build(mol, BASIS, AUX, device=dev.index or 0)
-    result = solve_rhf(ham, options=ScfOptions(), host_io=host_io)
+    guess = atomic_density_guess(mol, BASIS, device=dev.index or 0)
+    result = solve_rhf(ham, guess=guess, options=ScfOptions(), host_io=host_io)
     stats = ham.two_body.stats()
     out = {"energy": result.energy, "iterations": result.n_iterations, "converged": result.converged,
            "build": {k: ham.timings.get(k) for k in ("ms_metric", "ms_factor", "ms_three_center", "ms_fit",

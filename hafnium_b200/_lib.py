@@ -23,7 +23,7 @@ PREC_FP64, PREC_BF16X3 = 0, 1
 EXPORTS = (
     "hf_ctx_create", "hf_ctx_destroy", "hf_last_error", "hf_set_stream", "hf_shells_upload",
     "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
-    "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_get_stats",
+    "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_four_center", "hf_get_stats",
 )
 
 
@@ -95,6 +95,7 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_three_center.argtypes = [v, v]
     lib.hf_fitted_eri.argtypes = [v, v]
     lib.hf_one_electron.argtypes = [v, i, v, v, i64, v, i]
+    lib.hf_four_center.argtypes = [v, v, i]
     lib.hf_get_stats.argtypes = [v, p(StatsC)]
     for name in EXPORTS:
         getattr(lib, name).restype = ctypes.c_int if name != "hf_last_error" else ctypes.c_char_p
@@ -154,8 +155,11 @@ class Context:
     def set_stream(self, stream_handle: int | None) -> None:
         self.check(self.lib.hf_set_stream(self.handle, stream_handle or None), "hf_set_stream")
 
-    def upload(self, orbital, auxiliary) -> None:
+    def upload(self, orbital, auxiliary=None) -> None:
         o, keep_o = shell_struct(orbital)
+        if auxiliary is None:
+            self.check(self.lib.hf_shells_upload(self.handle, ctypes.byref(o), None), "hf_shells_upload")
+            return
         a, keep_a = shell_struct(auxiliary)
         self.check(self.lib.hf_shells_upload(self.handle, ctypes.byref(o), ctypes.byref(a)), "hf_shells_upload")
         del keep_o, keep_a
@@ -233,6 +237,12 @@ class Context:
         n, _ = self.dims()
         out = np.empty((n, n, n, n))
         self.check(self.lib.hf_fitted_eri(self.handle, out.ctypes.data), "hf_fitted_eri")
+        return out
+
+    def four_center(self) -> np.ndarray:
+        n, _ = self.dims()
+        out = np.empty((n, n, n, n))
+        self.check(self.lib.hf_four_center(self.handle, out.ctypes.data, 0), "hf_four_center")
         return out
 
     def one_electron(self, kind: int, charges=None, positions=None) -> np.ndarray:

@@ -395,7 +395,7 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
     cudaSetDevice(ctx->device);
     int s;
     if ((s = check_table(ctx, orbt, "orbital", kMaxOrbL, false)) != HF_OK) return s;
-    if ((s = check_table(ctx, auxt, "auxiliary", kMaxAuxL, true)) != HF_OK) return s;
+    if (auxt && (s = check_table(ctx, auxt, "auxiliary", kMaxAuxL, true)) != HF_OK) return s;
     free_shells(ctx);
     release(ctx->d_B);
     release(ctx->d_metric);
@@ -428,6 +428,8 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
     }
     ctx->n = fn;
     // auxiliary: reference function offsets, then internal order sorted by l
+    static const hf_shell_table kNoShells{};
+    if (!auxt) auxt = &kNoShells;
     std::vector<int> ref_off(auxt->n_shells);
     int rf = 0;
     for (int64_t sh = 0; sh < auxt->n_shells; ++sh) {
@@ -450,12 +452,13 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
     ctx->nt = (ctx->n + 63) / 64;
     ctx->ntiles = (int64_t)ctx->nt * (ctx->nt + 1) / 2;
     if (alloc(ctx, (void**)&ctx->d_orb, sizeof(DevShell) * ctx->orb.size()) ||
-        alloc(ctx, (void**)&ctx->d_aux, sizeof(DevShell) * ctx->aux.size()) ||
+        alloc(ctx, (void**)&ctx->d_aux, sizeof(DevShell) * std::max<size_t>(1, ctx->aux.size())) ||
         alloc(ctx, (void**)&ctx->d_exps, sizeof(double) * exps.size()) ||
         alloc(ctx, (void**)&ctx->d_coefs, sizeof(double) * coefs.size()))
         return HF_ERR_OOM;
     HF_CU(cudaMemcpy(ctx->d_orb, ctx->orb.data(), sizeof(DevShell) * ctx->orb.size(), cudaMemcpyHostToDevice));
-    HF_CU(cudaMemcpy(ctx->d_aux, ctx->aux.data(), sizeof(DevShell) * ctx->aux.size(), cudaMemcpyHostToDevice));
+    if (!ctx->aux.empty())
+        HF_CU(cudaMemcpy(ctx->d_aux, ctx->aux.data(), sizeof(DevShell) * ctx->aux.size(), cudaMemcpyHostToDevice));
     HF_CU(cudaMemcpy(ctx->d_exps, exps.data(), sizeof(double) * exps.size(), cudaMemcpyHostToDevice));
     HF_CU(cudaMemcpy(ctx->d_coefs, coefs.data(), sizeof(double) * coefs.size(), cudaMemcpyHostToDevice));
     for (int l = 0; l <= kMaxAuxL; ++l) {
@@ -541,6 +544,7 @@ static int three_center_chunk(hf_ctx* ctx, int row0, int row1, double* T, PairTa
 int hf_build_fitted_tensor(hf_ctx* ctx) {
     if (!ctx) return HF_ERR_ARG;
     if (!ctx->uploaded) return fail(ctx, HF_ERR_STATE, "upload shells first");
+    if (ctx->naux == 0) return fail(ctx, HF_ERR_STATE, "no auxiliary shells were uploaded");
     cudaSetDevice(ctx->device);
     const int N = ctx->naux;
     int s;
@@ -929,6 +933,29 @@ int hf_one_electron(hf_ctx* ctx, int kind, const double* charges, const double* 
     if (e == cudaSuccess && !on_device) e = cudaMemcpy(out, sOut, sizeof(double) * nn, cudaMemcpyDeviceToHost);
     release(buf);
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("one-electron: ") + cudaGetErrorString(e));
+    return HF_OK;
+}
+
+int hf_four_center(hf_ctx* ctx, double* out, int on_device) {
+    if (!ctx || !out) return HF_ERR_ARG;
+    if (!ctx->uploaded) return fail(ctx, HF_ERR_STATE, "upload shells first");
+    cudaSetDevice(ctx->device);
+    const int64_t n = ctx->n;
+    if (n > 128) return fail(ctx, HF_ERR_ARG, "the exact four-centre kernel serves atoms and small molecules (n <= 128)");
+    const size_t bytes = sizeof(double) * (size_t)n * n * n * n;
+    double* dst = out;
+    double* tmp = nullptr;
+    if (!on_device) {
+        if (alloc(ctx, (void**)&tmp, bytes)) return HF_ERR_OOM;
+        dst = tmp;
+    }
+    cudaError_t e = launch_four_center(ctx->d_orb, (int)ctx->orb.size(), ctx->d_exps, ctx->d_coefs, ctx->d_btable, dst,
+                                       (int)n, ctx->stream);
+    ++ctx->stats.kernel_launches;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess && !on_device) e = cudaMemcpy(out, tmp, bytes, cudaMemcpyDeviceToHost);
+    release(tmp);
+    if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("four-centre: ") + cudaGetErrorString(e));
     return HF_OK;
 }
 

@@ -587,3 +587,5 @@ cudaError_t launch_one_electron(int kind, int la, int lb, const int2* tasks, int
 }
 
 }  // namespace hf
+
+#include "four_center.cuh"

@@ -60,4 +60,8 @@ cudaError_t launch_one_electron(int kind, int la, int lb, const int2* tasks, int
                                 const double* positions, int natoms, const double* btable, double* out,
                                 int64_t n, cudaStream_t stream);
 
+// Exact (ab|cd) over all shell quartets of a small table into out[n][n][n][n].
+cudaError_t launch_four_center(const DevShell* shells, int ns, const double* exps, const double* coefs,
+                               const double* btable, double* out, int n, cudaStream_t stream);
+
 }  // namespace hf

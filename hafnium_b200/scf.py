@@ -196,12 +196,62 @@ def fill_averaged(energies: np.ndarray, count: float, tolerance: float = 1e-6) -
     return occ
 
 
+class _ExactTwoBody:
+    """Exact J/K from four-centre integrals held on the device (coulomb_exchange.py:75-121)."""
+
+    def __init__(self, eri) -> None:
+        self.eri = eri
+        self.n_ao = eri.shape[0]
+
+    def coulomb(self, d):
+        return _torch().einsum("uvwx,wx->uv", self.eri, d)
+
+    def exchange(self, d):
+        return _torch().einsum("uwxv,wx->uv", self.eri, d)
+
+    def exchange_factored(self, factor, weights=None):
+        return self.exchange(factor @ factor.T)
+
+
+def _spherical_atom(symbol: str, basis: str, device: int):
+    """atoms.py:55-73: the neutral atom with exact J/K and averaged occupations."""
+    torch = _torch()
+    from hafnium_b200.molecule import Molecule, atomic_number
+
+    z = atomic_number(symbol)
+    atom = Molecule((symbol,), np.zeros((1, 3)))
+    orb = ShellTable.build(basis, atom.symbols, atom.positions)
+    ctx = _lib.Context(device)
+    ctx.upload(orb)
+    dev = torch.device("cuda", device)
+    s = torch.as_tensor(ctx.one_electron(0), device=dev)
+    h = torch.as_tensor(ctx.one_electron(1) + ctx.one_electron(2, np.array([float(z)]), np.zeros((1, 3))), device=dev)
+    eri = torch.as_tensor(ctx.four_center(), device=dev)
+    ctx.close()
+    ham = DeviceHamiltonian(s, h, _ExactTwoBody(eri), 0.0, z / 2.0)
+    return _Rhf(ham, ScfOptions(), PrecisionSchedule(), averaged=True).run(None).density
+
+
+def atomic_density_guess(molecule, basis: str, *, device: int = 0):
+    """atoms.py:76-120: converge each distinct element once, place the per-spin
+    atomic densities on the diagonal in atom order (molecular case)."""
+    torch = _torch()
+    cache: dict[str, object] = {}
+    blocks = []
+    for symbol in molecule.symbols:
+        if symbol not in cache:
+            cache[symbol] = _spherical_atom(symbol, basis, device)
+        blocks.append(cache[symbol])
+    return torch.block_diag(*blocks).contiguous()
+
+
 class _Rhf:
     def __init__(self, ham: DeviceHamiltonian, options: ScfOptions, schedule: PrecisionSchedule,
-                 host_io: bool = False) -> None:
+                 host_io: bool = False, averaged: bool = False) -> None:
         torch = _torch()
         self.torch = torch
         self.host_io = host_io
+        self.averaged = averaged
         self.h2d_bytes = 0
         self.d2h_bytes = 0
         self.ham = ham
@@ -217,11 +267,11 @@ class _Rhf:
         return w, self.x @ v
 
     def density(self, w, c, averaged: bool):
-        if averaged:
+        if averaged or self.averaged:
             occ = fill_averaged(w.cpu().numpy(), float(self.ham.n_alpha))
         else:
             occ = np.zeros(w.shape[0])
-            occ[np.argsort(w.cpu().numpy(), kind="stable")[: self.ham.n_alpha]] = 1.0
+            occ[np.argsort(w.cpu().numpy(), kind="stable")[: int(self.ham.n_alpha)]] = 1.0
         keep = np.nonzero(occ > 0.0)[0]
         idx = self.torch.as_tensor(keep, device=c.device)
         occ_t = self.torch.as_tensor(occ[keep], dtype=self.torch.float64, device=c.device)
@@ -328,7 +378,6 @@ class _Rhf:
         w, c = self.solve(f)
         d, factor = self.density(w, c, averaged=False)
         final_f, terms, energy = self.fock(d, factor, "fp64")
-        self.ham.two_body.context.lib  # keep the context alive until here
         self.torch.cuda.synchronize()
         return ScfResult(energy, d, final_f, w, c, converged, history, terms, time.perf_counter() - t_start,
                          dict(self.timings))

@@ -76,7 +76,8 @@ const char* hf_last_error(const hf_ctx* ctx);
 int hf_set_stream(hf_ctx* ctx, void* stream);
 
 /* Upload the orbital and auxiliary shells (replaces the _kernels.ShellTable
- * marshalling of native.py:16-24; validation of integrals/mod.rs:111-173). */
+ * marshalling of native.py:16-24; validation of integrals/mod.rs:111-173).
+ * auxiliary may be NULL when only one-electron / four-centre integrals are wanted. */
 int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbital, const hf_shell_table* auxiliary);
 
 /* (P|Q), its Cholesky factor and (P|mu nu) -> packed B = L^-1 (P|mu nu) on the
@@ -110,6 +111,11 @@ int hf_fitted_eri(hf_ctx* ctx, double* out);
  * positions [n_atoms][3] Bohr). out: [n_ao][n_ao]. */
 int hf_one_electron(hf_ctx* ctx, int kind, const double* charges, const double* positions, int64_t n_atoms,
                     double* out, int on_device);
+
+/* Exact (uv|wx) over the uploaded orbital shells, [n][n][n][n], n <= 128: the
+ * atoms of the superposition-of-atomic-densities guess (hafnium/scf/atoms.py:55-73
+ * with the Rust coulomb_four_center, two_electron.rs:429-935). */
+int hf_four_center(hf_ctx* ctx, double* out, int on_device);
 
 int hf_get_stats(const hf_ctx* ctx, hf_stats* out);
 

@@ -81,3 +81,11 @@ def test_bad_shell_tables_raise_input_error():
         ctx.upload(bad, aux)
     with pytest.raises(InputError, match="upload shells first"):
         ctx.build()
+
+
+def test_four_center_matches_oracle():
+    mol = molecule("water")
+    orb, _ = tables(mol)
+    ctx = _lib.Context(0)
+    ctx.upload(orb)
+    np.testing.assert_allclose(ctx.four_center(), dfrhf.eri_exact(orb), atol=ORACLE_TOL, rtol=0)

@@ -25,3 +25,30 @@ def test_device_dfrhf_matches_reference(tag):
     assert result.converged
     assert abs(result.energy - float(ref["energy"])) <= 1e-8
     assert np.max(np.abs(result.density.cpu().numpy() - ref["density"])) <= 1e-6
+
+
+def test_sad_guess_matches_oracle():
+    """atoms.py:76-120 restated on the device against the oracle's restatement."""
+    from hafnium_b200.basis import ShellTable
+    from hafnium_b200.scf import atomic_density_guess
+    from oracle import dfrhf
+
+    mol = molecule("h2o2_s0")
+    orb = ShellTable.build("cc-pvdz", mol.symbols, mol.positions)
+    expected = dfrhf.atomic_density_guess(orb, mol.symbols, {"O": 8.0, "H": 1.0})
+    got = atomic_density_guess(mol, "cc-pvdz").cpu().numpy()
+    np.testing.assert_allclose(got, expected, atol=1e-8, rtol=0)
+
+
+@pytest.mark.parametrize("tag", ["h2o4_s1", "h2o8_s2"])
+def test_sad_started_scf_follows_the_reference_iterations(tag):
+    """With the reference's SAD guess the device SCF takes the reference's iterations."""
+    from hafnium_b200.scf import atomic_density_guess
+
+    ref = golden(f"reference_dfrhf_{tag}.npz")
+    mol = molecule(tag)
+    ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
+    result = solve_rhf(ham, guess=atomic_density_guess(mol, "cc-pvdz"))
+    assert result.n_iterations == int(ref["n_iterations"])
+    np.testing.assert_allclose([h.energy for h in result.history], ref["history"], atol=1e-8, rtol=0)
+    assert abs(result.energy - float(ref["energy"])) <= 1e-8

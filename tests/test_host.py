@@ -1,0 +1,61 @@
+"""Host-side logic: the cluster generator, shell tables and the driver's host pieces (CPU)."""
+
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+import pytest
+
+from hafnium_b200.basis import ShellTable, element_shells, primitive_norm
+from hafnium_b200.molecule import ANGSTROM_IN_BOHR, cube_side_angstrom, water_cluster
+from hafnium_b200.scf import fill_averaged, solve_diis
+from oracle import dfrhf
+
+
+@pytest.mark.parametrize("n,seed", [(8, 0), (32, 3), (64, 0)])
+def test_water_cluster_geometry(n, seed):
+    mol = water_cluster(n, seed)
+    assert mol.symbols == ("O", "H", "H") * n
+    pos = mol.positions / ANGSTROM_IN_BOHR
+    oxygens = pos[0::3]
+    for i, j in itertools.combinations(range(n), 2):
+        assert np.linalg.norm(oxygens[i] - oxygens[j]) >= 2.7 - 1e-12
+    side = cube_side_angstrom(n)
+    assert np.all(oxygens >= 0.0) and np.all(oxygens <= side)
+    for w in range(n):
+        o, h1, h2 = pos[3 * w: 3 * w + 3]
+        assert np.linalg.norm(h1 - o) == pytest.approx(0.9572, abs=1e-12)
+        cos = np.dot(h1 - o, h2 - o) / 0.9572 ** 2
+        assert np.degrees(np.arccos(cos)) == pytest.approx(104.52, abs=1e-9)
+    assert mol.n_alpha == 5 * n
+
+
+def test_cluster_sizes_match_the_configs():
+    for n, nbf, naux in ((8, 192, 904), (32, 768, 3616), (64, 1536, 7232)):
+        mol = water_cluster(n, 0)
+        orb = ShellTable.build("cc-pvdz", mol.symbols, mol.positions)
+        aux = ShellTable.build("def2-universal-jkfit", mol.symbols, mol.positions)
+        assert (orb.n_functions, aux.n_functions) == (nbf, naux)
+
+
+def test_contractions_have_unit_norm():
+    """<chi|chi> = 1 for every contracted spherical function (shell.py:87-104)."""
+    for shells in element_shells("cc-pvdz").values():
+        for shell in shells:
+            for row in shell.primitive_coefficients():
+                total = 0.0
+                for ci, ai in zip(row, shell.exponents):
+                    for cj, aj in zip(row, shell.exponents):
+                        ni, nj = primitive_norm(ai, shell.l), primitive_norm(aj, shell.l)
+                        total += ci * cj / (ni * nj) * (2 * np.sqrt(ai * aj) / (ai + aj)) ** (shell.l + 1.5)
+                assert total == pytest.approx(1.0, abs=1e-12)
+
+
+def test_diis_and_filling_match_the_oracle():
+    rng = np.random.default_rng(0)
+    a = rng.normal(size=(5, 5))
+    ov = a @ a.T
+    np.testing.assert_allclose(solve_diis(ov), dfrhf.solve_diis(ov), atol=1e-14)
+    e = np.array([-3.0, -1.0, 0.5, 0.5 + 1e-9, 0.5 - 1e-9, 2.0])
+    np.testing.assert_allclose(fill_averaged(e, 3.0), dfrhf.fill_averaged(e, 3.0), atol=0)
