@@ -24,6 +24,7 @@ EXPORTS = (
     "hf_ctx_create", "hf_ctx_destroy", "hf_last_error", "hf_set_stream", "hf_shells_upload",
     "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
     "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_four_center", "hf_get_stats",
+    "hf_coulomb_static",
 )
 
 
@@ -96,6 +97,7 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_fitted_eri.argtypes = [v, v]
     lib.hf_one_electron.argtypes = [v, i, v, v, i64, v, i]
     lib.hf_four_center.argtypes = [v, v, i]
+    lib.hf_coulomb_static.argtypes = [v, v, v]
     lib.hf_get_stats.argtypes = [v, p(StatsC)]
     for name in EXPORTS:
         getattr(lib, name).restype = ctypes.c_int if name != "hf_last_error" else ctypes.c_char_p

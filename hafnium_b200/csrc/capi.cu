@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -966,3 +967,71 @@ int hf_get_stats(const hf_ctx* ctx, hf_stats* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Coulomb build that allocates nothing.
+//
+// Some callers cannot call cudaMalloc: an application whose device memory is
+// already fully reserved by its own pool allocator (a cudaMalloc would fail or
+// fragment that pool), or a latency-critical loop in which a cudaMalloc /
+// cudaFree pair, which can synchronise the device, is not allowed. For them
+// hf_coulomb_static runs the same J build as hf_coulomb but takes its scratch
+// (the weighted packed density, the fitting charges and the packed J) from the
+// file-scope array below instead of from an allocation. The caller still passes
+// the density and J as device pointers.
+//
+// Limits: n_ao <= kStaticMaxAo (1536, 24 tiles of 64) and n_aux <= kStaticMaxAux
+// (8192). The array is 2 * 300 * 4096 + 8192 doubles, about 19.7 MB, and every
+// GPU that loads this library holds it until the process exits. All calls on a
+// device share it: calls whose work overlaps on the GPU (different streams or
+// contexts at the same time) race on it and must be serialised by the caller.
+// The first call on a device resolves the array's device address
+// (cudaGetSymbolAddress, with that device current); make that first call before
+// any stream capture.
+namespace {
+constexpr int64_t kStaticMaxAo = 1536;
+constexpr int64_t kStaticMaxAux = 8192;
+constexpr int64_t kStaticMaxTiles = (kStaticMaxAo / 64) * (kStaticMaxAo / 64 + 1) / 2;
+constexpr int64_t kStaticScratchDoubles = 2 * kStaticMaxTiles * 4096 + kStaticMaxAux;
+static __device__ __align__(256) double g_coulomb_scratch[kStaticScratchDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+double* g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_coulomb_scratch on `device` (current), resolved once.
+int static_scratch(hf_ctx* ctx, double** out) {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, HF_ERR_ARG, "device index out of range");
+    if (!g_scratch_ptr[ctx->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_coulomb_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            return fail(ctx, HF_ERR_CUDA, std::string("cudaGetSymbolAddress(g_coulomb_scratch): ") +
+                                              cudaGetErrorString(e));
+        g_scratch_ptr[ctx->device] = static_cast<double*>(p);
+    }
+    *out = g_scratch_ptr[ctx->device];
+    return HF_OK;
+}
+}  // namespace
+
+extern "C" int hf_coulomb_static(hf_ctx* ctx, const double* density, double* coulomb) {
+    if (!ctx || !density || !coulomb) return HF_ERR_ARG;
+    if (ctx->uploaded && (ctx->n > kStaticMaxAo || ctx->naux > kStaticMaxAux))
+        return fail(ctx, HF_ERR_ARG, "hf_coulomb_static supports n_ao <= " + std::to_string(kStaticMaxAo) +
+                                         " and n_aux <= " + std::to_string(kStaticMaxAux) + " (got " +
+                                         std::to_string(ctx->n) + " and " + std::to_string(ctx->naux) +
+                                         "); use hf_coulomb");
+    if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    cudaSetDevice(ctx->device);
+    double* scratch = nullptr;
+    int s = static_scratch(ctx, &scratch);
+    if (s != HF_OK) return s;
+    const JkPlan p = plan_of(ctx);
+    if (coulomb_work_doubles(p) > kStaticScratchDoubles) return fail(ctx, HF_ERR_ARG, "scratch size exceeded");
+    cudaError_t e = coulomb_build(p, density, coulomb, scratch, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("hf_coulomb_static: ") + cudaGetErrorString(e));
+    ctx->stats.kernel_launches += 4;
+    return check_async(ctx, "hf_coulomb_static");
+}

@@ -90,6 +90,17 @@ int hf_dims(const hf_ctx* ctx, int64_t* n_ao, int64_t* n_aux);
 /* J[u][v] = sum_wx (uv|wx) D[w][x] (coulomb_exchange.py:176-182). */
 int hf_coulomb(hf_ctx* ctx, const double* density, double* coulomb, int on_device);
 
+/* The J build of hf_coulomb without any device allocation, for callers that
+ * cannot call cudaMalloc (a device pool already reserved by their own
+ * allocator, or a loop where an allocation's device synchronisation is not
+ * allowed). No counterpart in the reference. Density and J are device pointers;
+ * scratch comes from a static device array of about 19.7 MB that every GPU
+ * loading this library holds until exit, so n_ao <= 1536 and n_aux <= 8192
+ * (HF_ERR_ARG beyond). Calls share that array: calls that overlap on the GPU
+ * race. The first call on a device resolves the array's address; make it
+ * before any stream capture. */
+int hf_coulomb_static(hf_ctx* ctx, const double* density, double* coulomb);
+
 /* K[u][v] = sum_wx (uw|xv) D[w][x] (coulomb_exchange.py:184-190) for a symmetric
  * positive semidefinite D, factorised on the device by a pivoted Cholesky;
  * HF_ERR_NUMERIC when D is indefinite (use hf_exchange_factored then). */
