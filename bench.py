@@ -118,18 +118,20 @@ def measure_fp64_peak(torch, dev) -> float:
     return 2 * 8192 ** 3 / best / 1e12
 
 
-def one_scf(torch, mol, dev, host_io=False):
-    from hafnium_b200.scf import DeviceHamiltonian, ScfOptions, atomic_density_guess, solve_rhf
+def one_scf(torch, mol, dev, host_io=False, mode="mixed"):
+    from hafnium_b200.scf import DeviceHamiltonian, PrecisionSchedule, ScfOptions, atomic_density_guess, solve_rhf
 
     ham = DeviceHamiltonian.build(mol, BASIS, AUX, device=dev.index or 0)
     guess = atomic_density_guess(mol, BASIS, device=dev.index or 0)
-    result = solve_rhf(ham, guess=guess, options=ScfOptions(), host_io=host_io)
+    result = solve_rhf(ham, guess=guess, options=ScfOptions(), host_io=host_io,
+                       schedule=PrecisionSchedule(mode=mode))
     stats = ham.two_body.stats()
     out = {"energy": result.energy, "iterations": result.n_iterations, "converged": result.converged,
            "build": {k: ham.timings.get(k) for k in ("ms_metric", "ms_factor", "ms_three_center", "ms_fit",
                                                      "one_electron_s", "fitted_tensor_s")},
            "scf": result.timings, "launches": stats["kernel_launches"], "n_ao": ham.n_ao,
-           "n_aux": ham.two_body.n_aux, "b_bytes": stats["b_bytes"]}
+           "n_aux": ham.two_body.n_aux, "b_bytes": stats["b_bytes"],
+           "precisions": [h.precision for h in result.history]}
     del ham, result
     torch.cuda.empty_cache()
     return out
@@ -148,55 +150,69 @@ def run_b200(args) -> None:
     from hafnium_b200.molecule import water_cluster
 
     mol = water_cluster(args.waters, args.seed + rank)
-    for _ in range(args.warmup):
-        one_scf(torch, mol, dev)
+    for i in range(args.warmup):
+        one_scf(torch, mol, dev, mode="mixed")
+        if i == 0:
+            one_scf(torch, mol, dev, mode="fp64")
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     sampler = ClockSampler(local)
     sampler.start()
-    times, details = [], []
-    for _ in range(args.steps):
+
+    def timed(mode):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(dev)
         e0.record()
-        info = one_scf(torch, mol, dev)
+        info = one_scf(torch, mol, dev, mode=mode)
         e1.record()
         e1.synchronize()
-        times.append(e0.elapsed_time(e1) / 1e3)
+        return e0.elapsed_time(e1) / 1e3, info
+
+    times, details, plain_times, plain_details = [], [], [], []
+    for _ in range(args.steps):
+        t, info = timed("mixed")
+        times.append(t)
         details.append(info)
+    for _ in range(args.steps):
+        t, info = timed("fp64")
+        plain_times.append(t)
+        plain_details.append(info)
     torch.cuda.synchronize(dev)
     clocks = sampler.stop()
-    step_s = statistics.median(times)
     if world > 1:
-        t = torch.tensor([max(times)], device=dev)
+        t = torch.tensor([max(times), max(plain_times)], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-        step_max = float(t.item())
+        step_max, plain_max = float(t[0].item()), float(t[1].item())
     else:
-        step_max = max(times)
+        step_max, plain_max = max(times), max(plain_times)
     e2e = None
     if not args.no_e2e:
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        info = one_scf(torch, mol, dev, host_io=True)
+        info = one_scf(torch, mol, dev, host_io=True, mode="fp64")
         torch.cuda.synchronize(dev)
         e2e_s = time.perf_counter() - t0
         e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": info["scf"]["h2d_bytes"],
-               "d2h_bytes_per_step": info["scf"]["d2h_bytes"], "energy": info["energy"]}
+               "d2h_bytes_per_step": info["scf"]["d2h_bytes"], "energy": info["energy"],
+               "path": "reference-facing host NumPy coulomb()/exchange() calls (FP64 exchange)"}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return
     last = details[-1]
+    plain = plain_details[-1]
     n, naux = last["n_ao"], last["n_aux"]
     o = mol.n_alpha
-    fock_builds = last["scf"]["fock_builds"]
-    k_ms = last["scf"]["exchange_ms"] / fock_builds
-    j_ms = last["scf"]["coulomb_ms"] / fock_builds
+    fock_builds = plain["scf"]["fock_builds"]
+    k64_ms = plain["scf"]["exchange_ms_fp64"] / plain["scf"]["exchange_builds_fp64"]
+    j_ms = plain["scf"]["coulomb_ms"] / fock_builds
     k_flops = 4.0 * naux * n * n * o
     j_bytes = 2.0 * last["b_bytes"]
+    k16_builds = last["scf"].get("exchange_builds_bf16", 0)
+    k16_ms = last["scf"]["exchange_ms_bf16"] / k16_builds if k16_builds else None
     fp64_peak = measure_fp64_peak(torch, dev)
     peaks = {}
     try:
@@ -205,8 +221,20 @@ def run_b200(args) -> None:
     except OSError:
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    k_tflops = k_flops / (k_ms / 1e3) / 1e12
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    k64_tflops = k_flops / (k64_ms / 1e3) / 1e12
     j_gbs = j_bytes / (j_ms / 1e3) / 1e9
+    if k16_ms:
+        executed = 3.0 * k_flops  # three BF16 products per FP64-equivalent product
+        k16_exec_tflops = executed / (k16_ms / 1e3) / 1e12
+        roofline = {"bound": "tensor", "kernel": "split-BF16 exchange on tcgen05 (k_tc_split3, both stages)",
+                    "achieved": k16_exec_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
+                    "frac": k16_exec_tflops / bf16_peak, "traffic": None,
+                    "algorithmic": "3 x 4 naux n^2 nocc BF16 flops per K build (the three split products)",
+                    "algorithmic_tflops": k_flops / (k16_ms / 1e3) / 1e12,
+                    "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, of measured)"}
+    else:
+        roofline = None
     line = {
         "metric": METRIC,
         "value": step_max,
@@ -221,21 +249,26 @@ def run_b200(args) -> None:
         "dtype": "f64",
         "data": "synthetic: seeded rigid-water clusters (no dataset)",
         "config": {"workload": f"DF-RHF (H2O){args.waters} seed {args.seed}, cc-pVDZ/def2-universal-jkfit "
-                               f"(n={n}, naux={naux}, nocc={o}), plain FP64 GPU path",
-                   "waters": args.waters, "basis": BASIS, "auxiliary": AUX, "precision_path": "fp64",
+                               f"(n={n}, naux={naux}, nocc={o}), SAD guess, mixed split-BF16/FP64 exchange",
+                   "waters": args.waters, "basis": BASIS, "auxiliary": AUX, "precision_path": "mixed",
+                   "guess": "SAD (the learned guess is not built yet)",
                    "l2": "inputs larger than L2 (B tensor %.1f GB)" % (last["b_bytes"] / 1e9),
                    "parallelism": f"replicas x{world}"},
         "energy": last["energy"],
         "iterations": last["iterations"],
         "converged": last["converged"],
+        "precisions": last["precisions"],
         "step_times_s": times,
-        "stages": {"build": last["build"], "per_iteration_ms": {"coulomb": j_ms, "exchange": k_ms},
-                   "fock_builds": fock_builds},
-        "roofline": {"bound": "tensor", "kernel": "exchange (K) FP64 DMMA half-transform + SYRK",
-                     "achieved": k_tflops, "peak": fp64_peak, "unit": "TFLOP/s", "frac": k_tflops / fp64_peak,
-                     "traffic": None,
-                     "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64)",
-                     "algorithmic": "4 naux n^2 nocc flops per K"},
+        "plain_fp64": {"value": plain_max, "step_times_s": plain_times, "energy": plain["energy"],
+                       "iterations": plain["iterations"], "speedup_of_mixed": plain_max / step_max,
+                       "dE_mixed_vs_fp64": last["energy"] - plain["energy"]},
+        "stages": {"build": last["build"], "per_build_ms": {"coulomb": j_ms, "exchange_fp64": k64_ms,
+                                                             "exchange_bf16": k16_ms},
+                   "mixed_scf": last["scf"], "plain_scf": plain["scf"]},
+        "roofline": roofline,
+        "roofline_exchange_fp64": {"bound": "tensor", "achieved": k64_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+                                   "frac": k64_tflops / fp64_peak, "algorithmic": "4 naux n^2 nocc flops per K",
+                                   "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run"},
         "roofline_coulomb": {"bound": "hbm", "achieved": j_gbs, "peak": hbm_peak, "unit": "GB/s",
                              "frac": j_gbs / hbm_peak, "algorithmic": "2 passes over packed B per J",
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},

@@ -192,7 +192,7 @@ class Context:
         self.check(self.lib.hf_exchange(self.handle, d.ctypes.data, out.ctypes.data, precision, 0), "hf_exchange")
         return out
 
-    def exchange_factored_host(self, c: np.ndarray, weights=None, precision: int = PREC_FP64) -> np.ndarray:
+    def exchange_factored_host(self, c: np.ndarray, weights=None, precision: int = PREC_FP64) -> np.ndarray:  # noqa: E501
         c = np.ascontiguousarray(c, dtype=np.float64)
         n = c.shape[0]
         w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)

@@ -15,6 +15,7 @@
 #include "jk.cuh"
 #include "linalg.cuh"
 #include "md.cuh"
+#include "tc_exchange.cuh"
 
 using namespace hf;
 
@@ -34,6 +35,7 @@ struct hf_ctx {
     int n = 0, nt = 0, naux = 0;
     int64_t ntiles = 0;
     std::vector<DevShell> orb, aux;  // aux in internal order (sorted by l)
+    std::vector<double> h_exps, h_coefs;  // host copies of the primitive data
     std::vector<int> aux_ref_fn;     // internal aux function -> reference index
     int aux_count[kMaxAuxL + 1] = {};
     DevShell* d_orb = nullptr;
@@ -54,6 +56,9 @@ struct hf_ctx {
     size_t kscratch_bytes = 0;
     double* d_stage = nullptr;  // exchange staging: C, w, Ct, sign, D, Lc, K
     size_t stage_bytes = 0;
+    void* d_bf16_b = nullptr;  // full BF16 hi/lo copies of B (split-BF16 exchange)
+    double* d_tcwork = nullptr;  // split-BF16 exchange: factor and X chunk
+    size_t tcwork_bytes = 0;
     int* d_info = nullptr;
     double* d_scalar = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -127,6 +132,8 @@ int check_table(hf_ctx* ctx, const hf_shell_table* t, const char* name, int max_
         if (l < 0 || l > max_l)
             return fail(ctx, HF_ERR_ARG, std::string(name) + ": angular momentum " + std::to_string(l) +
                                              " exceeds the device kernels' maximum " + std::to_string(max_l));
+        if (!aux && np > 16)
+            return fail(ctx, HF_ERR_ARG, std::string(name) + ": more than 16 primitives in a shell");
         if (aux ? (k != 1) : (k > kMaxOrbContr[l]))
             return fail(ctx, HF_ERR_ARG, std::string(name) + ": too many general contractions (" + std::to_string(k) +
                                              ") for l = " + std::to_string(l));
@@ -374,6 +381,8 @@ int hf_ctx_destroy(hf_ctx* ctx) {
     release(ctx->d_io);
     release(ctx->d_kscratch);
     release(ctx->d_stage);
+    release(ctx->d_bf16_b);
+    release(ctx->d_tcwork);
     release(ctx->d_info);
     release(ctx->d_scalar);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -400,6 +409,7 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
     free_shells(ctx);
     release(ctx->d_B);
     release(ctx->d_metric);
+    release(ctx->d_bf16_b);
     ctx->built = false;
     std::vector<double> exps, coefs;
     auto add = [&](const hf_shell_table* t, int64_t sh, int fn) {
@@ -461,6 +471,8 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
     if (!ctx->aux.empty())
         HF_CU(cudaMemcpy(ctx->d_aux, ctx->aux.data(), sizeof(DevShell) * ctx->aux.size(), cudaMemcpyHostToDevice));
     HF_CU(cudaMemcpy(ctx->d_exps, exps.data(), sizeof(double) * exps.size(), cudaMemcpyHostToDevice));
+    ctx->h_exps = exps;
+    ctx->h_coefs = coefs;
     HF_CU(cudaMemcpy(ctx->d_coefs, coefs.data(), sizeof(double) * coefs.size(), cudaMemcpyHostToDevice));
     for (int l = 0; l <= kMaxAuxL; ++l) {
         ctx->aux_count[l] = (int)by_l[l].size();
@@ -492,7 +504,29 @@ static int build_metric(hf_ctx* ctx) {
     return check_async(ctx, "metric");
 }
 
-// Pair tasks for tile rows [row0, row1): pairs (a <= b) with a touching those rows.
+// The screening bound of integrals.cu for a whole shell pair: the largest
+// |c_a c_b| exp(-mu R_AB^2) over its primitive pairs.
+static double pair_bound(const hf_ctx* ctx, const DevShell& A, const DevShell& B, const std::vector<double>& exps,
+                         const std::vector<double>& coefs) {
+    const double dx = A.x - B.x, dy = A.y - B.y, dz = A.z - B.z;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    double best = 0.0;
+    for (int i = 0; i < A.nprim; ++i)
+        for (int j = 0; j < B.nprim; ++j) {
+            const double a = exps[A.prim + i], b = exps[B.prim + j];
+            const double e = std::exp(-a * b / (a + b) * r2);
+            double cmax = 0.0;
+            for (int ka = 0; ka < A.ncontr; ++ka)
+                for (int kb = 0; kb < B.ncontr; ++kb)
+                    cmax = std::max(cmax, std::fabs(coefs[A.coef + ka * A.nprim + i] * coefs[B.coef + kb * B.nprim + j]));
+            best = std::max(best, cmax * e);
+        }
+    (void)ctx;
+    return best;
+}
+
+// Pair tasks for tile rows [row0, row1): pairs (a <= b) with a touching those rows
+// and at least one primitive pair above the screening bound.
 static void chunk_tasks(const hf_ctx* ctx, int row0, int row1, std::vector<PairTask> (&tasks)[3][3],
                         int (&max_npp)[3][3]) {
     for (auto& r : tasks)
@@ -506,6 +540,7 @@ static void chunk_tasks(const hf_ctx* ctx, int row0, int row1, std::vector<PairT
         if ((f1 >> 6) < row0 || (f0 >> 6) >= row1) continue;
         for (int b = a; b < ns; ++b) {
             const DevShell& B = ctx->orb[b];
+            if (pair_bound(ctx, A, B, ctx->h_exps, ctx->h_coefs) < 1e-22) continue;
             int la = A.l, lb = B.l, swap = 0;
             if (la > lb) {
                 std::swap(la, lb);
@@ -696,7 +731,7 @@ int hf_coulomb(hf_ctx* ctx, const double* D, double* J, int on_device) {
 // K from Ct ([opad][npad], device) and sign ([opad]).
 static int exchange_from_ct(hf_ctx* ctx, const double* Ct, int opad, const double* sign, bool any_negative,
                             double* dK, int precision) {
-    if (precision != HF_PREC_FP64) return fail(ctx, HF_ERR_ARG, "this precision is not available in this build");
+    if (precision != HF_PREC_FP64) return fail(ctx, HF_ERR_ARG, "unknown precision");
     const JkPlan p = plan_of(ctx);
     const int64_t npad = (int64_t)ctx->nt * 64;
     // X chunk: npad x qchunk x opad doubles, within a budget
@@ -716,6 +751,46 @@ static int exchange_from_ct(hf_ctx* ctx, const double* Ct, int opad, const doubl
     ctx->stats.kernel_launches += 3 * ((ctx->naux + qchunk - 1) / qchunk) + 2;
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("exchange: ") + cudaGetErrorString(e));
     return check_async(ctx, "exchange");
+}
+
+// Split-BF16 exchange from Ct_tc ([t.opad][t.npad], FP64, zero padded) into dK (n x n).
+static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, double* dK) {
+    const JkPlan p = plan_of(ctx);
+    if (!ctx->d_bf16_b) {
+        if (alloc(ctx, &ctx->d_bf16_b, tc_b_bytes(ctx->n, ctx->naux)))
+            return fail(ctx, HF_ERR_OOM, "no room for the BF16 copies of the fitted tensor (" +
+                                             std::to_string(tc_b_bytes(ctx->n, ctx->naux)) + " bytes)");
+        HF_CU(tc_split_b(p, t.npad, ctx->d_bf16_b, ctx->stream));
+        int s = check_async(ctx, "BF16 copy of B");
+        if (s != HF_OK) {
+            release(ctx->d_bf16_b);
+            return s;
+        }
+    }
+    size_t freeb = 0, totalb = 0;
+    cudaMemGetInfo(&freeb, &totalb);
+    const size_t ct_bytes = 2 * 2 * (size_t)t.opad * t.npad;
+    const size_t per_q = 2 * 2 * (size_t)t.npad * t.opad;
+    const size_t kp_doubles = (size_t)round_up(t.npad * t.npad, 32);
+    size_t budget = std::min<size_t>((size_t)2 << 30, freeb / 3);
+    size_t want = ct_bytes + per_q * std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)ctx->naux));
+    want = round_up((int64_t)want, 256) + sizeof(double) * kp_doubles;
+    int st = ensure_scratch(ctx, &ctx->d_tcwork, &ctx->tcwork_bytes, want);
+    if (st != HF_OK) return st;
+    double* Kp = ctx->d_tcwork;
+    void* work = ctx->d_tcwork + kp_doubles;
+    HF_CU(cudaMemsetAsync(ctx->d_info + 2, 0, sizeof(int), ctx->stream));
+    cudaError_t e = exchange_build_bf16(t, ctx->d_bf16_b, Ct_tc, t.npad, dK, Kp, work, want - sizeof(double) * kp_doubles,
+                                        ctx->d_info + 2, ctx->stream, ctx->n);
+    ctx->stats.kernel_launches += 3 * ((ctx->naux + 1023) / 1024) + 3;
+    if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("split-BF16 exchange: ") + cudaGetErrorString(e));
+    int s = check_async(ctx, "split-BF16 exchange");
+    if (s != HF_OK) return s;
+    int flag = 0;
+    HF_CU(cudaMemcpy(&flag, ctx->d_info + 2, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) return fail(ctx, HF_ERR_TIMEOUT, "split-BF16 exchange: a pipeline wait ran out (code " +
+                                                   std::to_string(flag) + ")");
+    return HF_OK;
 }
 
 int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const double* w, double* K, int precision,
@@ -751,6 +826,23 @@ int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const doub
         if (w) cudaMemcpyAsync(sw, w, sizeof(double) * ncols, cudaMemcpyHostToDevice, ctx->stream);
         dC = sC;
         dw = w ? sw : nullptr;
+    }
+    if (precision == HF_PREC_BF16X3) {
+        if (neg) return fail(ctx, HF_ERR_ARG, "the split-BF16 exchange takes non-negative weights");
+        const TcPlan t = tc_plan(n, ctx->naux, ncols);
+        double* Ct_tc = nullptr;
+        if (alloc(ctx, (void**)&Ct_tc, sizeof(double) * ((size_t)t.opad * t.npad + t.opad))) return HF_ERR_OOM;
+        time_begin(ctx);
+        k_factor_transpose<<<(unsigned)((t.opad * t.npad + 255) / 256), 256, 0, ctx->stream>>>(
+            dC, n, ncols, dw, Ct_tc, t.npad, t.opad, Ct_tc + (size_t)t.opad * t.npad);
+        double* dK = on_device ? K : sK;
+        int s = exchange_bf16(ctx, t, Ct_tc, dK);
+        if (s == HF_OK && !on_device) cudaMemcpyAsync(K, sK, sizeof(double) * n * n, cudaMemcpyDeviceToHost, ctx->stream);
+        ctx->stats.ms_exchange = time_end(ctx);
+        ctx->stats.exchange_rank = ncols;
+        release(Ct_tc);
+        if (s == HF_OK) s = check_async(ctx, "hf_exchange_factored");
+        return s;
     }
     time_begin(ctx);
     k_factor_transpose<<<(unsigned)((opad * npad + 255) / 256), 256, 0, ctx->stream>>>(dC, n, ncols, dw, Ct, npad, opad,
@@ -800,6 +892,22 @@ int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_d
         return fail(ctx, HF_ERR_NUMERIC, "the density is not positive semidefinite; pass a signed factor to "
                                          "hf_exchange_factored");
     const int64_t rank = res[0];
+    if (precision == HF_PREC_BF16X3) {
+        const TcPlan t = tc_plan(n, ctx->naux, rank);
+        double* Ct_tc = nullptr;
+        if (alloc(ctx, (void**)&Ct_tc, sizeof(double) * ((size_t)t.opad * t.npad + t.opad))) return HF_ERR_OOM;
+        time_begin(ctx);
+        k_factor_pad<<<(unsigned)((t.opad * t.npad + 255) / 256), 256, 0, ctx->stream>>>(
+            Lc, n, rank, Ct_tc, t.npad, t.opad, Ct_tc + (size_t)t.opad * t.npad);
+        double* dK = on_device ? K : sK;
+        int s = exchange_bf16(ctx, t, Ct_tc, dK);
+        if (s == HF_OK && !on_device) cudaMemcpyAsync(K, sK, sizeof(double) * nn, cudaMemcpyDeviceToHost, ctx->stream);
+        ctx->stats.ms_exchange = time_end(ctx);
+        ctx->stats.exchange_rank = rank;
+        release(Ct_tc);
+        if (s == HF_OK) s = check_async(ctx, "hf_exchange");
+        return s;
+    }
     const int64_t opad = std::max<int64_t>(64, round_up(rank, 64));
     double* Ct = buf + oCt;
     double* sign = buf + osg;

@@ -226,16 +226,46 @@ struct PairLayout {
     static constexpr int STRIDE = 4 + KK + NSAB * NH;
 };
 
+// Primitive pairs whose |c_a c_b| exp(-mu R_AB^2) falls below this contribute
+// less than ~1e-15 to any (P|ab) and are skipped (the reference evaluates every
+// primitive triple; the difference is far below its 1e-12 integral tolerance).
+constexpr double kPairScreen = 1e-22;
+
+constexpr int kMaxPrimPairs = 256;
+
 template <int LA, int LB>
-__device__ void pair_prologue(const DevShell& A, const DevShell& B, const double* __restrict__ exps,
-                              const double* __restrict__ coefs, double* smem) {
+__device__ int pair_prologue(const DevShell& A, const DevShell& B, const double* __restrict__ exps,
+                             const double* __restrict__ coefs, double* smem, int* s_pos) {
     using PL = PairLayout<LA, LB>;
     constexpr int NCA = ncart(LA), NCB = ncart(LB);
     const int npp = A.nprim * B.nprim;
     const double abx = A.x - B.x, aby = A.y - B.y, abz = A.z - B.z;
     const double rab2 = abx * abx + aby * aby + abz * abz;
-    for (int pp = threadIdx.x; pp < npp; pp += blockDim.x) {
-        const int i = pp / B.nprim, j = pp % B.nprim;
+    // significance flags, then a serial prefix (npp <= 256) for a deterministic order
+    for (int pp0 = threadIdx.x; pp0 < npp; pp0 += blockDim.x) {
+        const int i = pp0 / B.nprim, j = pp0 % B.nprim;
+        const double a = exps[A.prim + i], b = exps[B.prim + j];
+        double cmax = 0.0;
+        for (int ka = 0; ka < A.ncontr; ++ka)
+            for (int kb = 0; kb < B.ncontr; ++kb)
+                cmax = fmax(cmax, fabs(coefs[A.coef + ka * A.nprim + i] * coefs[B.coef + kb * B.nprim + j]));
+        s_pos[pp0] = (cmax * exp(-(a * b / (a + b)) * rab2) >= kPairScreen) ? 1 : 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int k = 0;
+        for (int pp0 = 0; pp0 < npp; ++pp0) {
+            const int keep = s_pos[pp0];
+            s_pos[pp0] = keep ? k : -1;
+            k += keep;
+        }
+        s_pos[kMaxPrimPairs] = k;
+    }
+    __syncthreads();
+    for (int pp0 = threadIdx.x; pp0 < npp; pp0 += blockDim.x) {
+        const int pp = s_pos[pp0];
+        if (pp < 0) continue;
+        const int i = pp0 / B.nprim, j = pp0 % B.nprim;
         const double a = exps[A.prim + i], b = exps[B.prim + j];
         const double p = a + b;
         const double mu = a * b / p;
@@ -284,6 +314,8 @@ __device__ void pair_prologue(const DevShell& A, const DevShell& B, const double
                         }
             }
     }
+    __syncthreads();
+    return s_pos[kMaxPrimPairs];
 }
 
 template <int LA, int LB, int LP>
@@ -301,11 +333,12 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
     constexpr int NCP = ncart(LP), NSP = nsph(LP);
     constexpr int SPB = 128 / NSP;  // aux shells per CTA
     extern __shared__ double smem[];
+    __shared__ int s_pos[kMaxPrimPairs + 1];
     const PairTask task = tasks[blockIdx.x];
     const DevShell A = orb[task.swap ? task.second : task.first];
     const DevShell B = orb[task.swap ? task.first : task.second];
-    pair_prologue<LA, LB>(A, B, exps, coefs, smem);
-    __syncthreads();
+    const int npp = pair_prologue<LA, LB>(A, B, exps, coefs, smem, s_pos);
+    if (npp == 0) return;  // the chunk was zeroed; nothing survives screening
 
     const int slot = threadIdx.x / NSP, mp = threadIdx.x % NSP;
     const int ia = blockIdx.y * SPB + slot;
@@ -321,7 +354,6 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
 #pragma unroll
         for (int m = 0; m < PL::NSAB; ++m) acc[k][m] = 0.0;
 
-    const int npp = A.nprim * B.nprim;
     for (int i = 0; i < P.nprim; ++i) {
         const double q = exps[P.prim + i];
         double cq = coefs[P.coef + i] * pow(2.0 * q, -(double)LP);

@@ -1,0 +1,492 @@
+// Split-BF16 exchange on the 5th-generation tensor cores (tcgen05 + TMEM).
+//
+// K = sum_q X_q X_q^T with X_q = B_q C (the factored form of the reference's
+// K = sum_P B_P D B_P, hafnium/scf/coulomb_exchange.py:184-190). Every operand is
+// split into two BF16 parts, x = hi + lo, and each product keeps the three
+// leading terms hi*hi + hi*lo + lo*hi, accumulated in FP32 in tensor memory:
+//
+//   stage 1  X[(q,p)][i] = sum_r B[(q,p)][r] C[r][i]   one GEMM, M = rows (q,p),
+//            A = BF16 copies of B stored in full (both triangles, K-major),
+//            B-operand = C^T; the epilogue splits X into BF16 hi/lo, p-major.
+//   stage 2  K[p][p'] += sum_(q,i) X[p][(q,i)] X[p'][(q,i)], split over k,
+//            upper 128-row tiles only, FP64 atomics into K.
+//
+// One CTA computes one 128 x BN output tile: warp 4 drives TMA (no multicast),
+// warp 5 allocates TMEM and one thread issues tcgen05.mma (kind::f16, BF16
+// inputs, FP32 accumulate, M = 128), warps 0-3 drain TMEM with tcgen05.ld.
+// Shared-memory tiles use the 128-byte swizzle that both TMA and the UMMA
+// descriptors understand. Every mbarrier wait is bounded: past the limit the
+// waiting thread records an error and stops waiting, so a fault in the
+// pipeline ends the kernel instead of hanging the GPU.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "jk.cuh"
+#include "tc_exchange.cuh"
+
+namespace hf {
+
+namespace {
+
+constexpr int BM = 128;
+constexpr int BK = 64;  // one 128-byte swizzle row of BF16
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: far above any legitimate wait here
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: gives up after kWaitNs, or as soon as another CTA has recorded
+// an error, and records its own failure; returns whether the phase completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t start = global_ns();
+    for (uint32_t i = 1;; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 255) == 0) {
+            if (*(volatile int*)err != 0) return false;
+            if (global_ns() - start > kWaitNs) {
+                atomicExch(err, 1);
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];\n" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void prefetch_map(const CUtensorMap* map) {
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+// K-major, 128-byte swizzle UMMA shared-memory descriptor: rows of 128 bytes,
+// 8-row groups 1024 bytes apart (SBO), version 1, layout type 2.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFF) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// Instruction descriptor: D FP32, A/B BF16, both K-major, N = bn, M = 128.
+__host__ __device__ constexpr uint32_t idesc_bf16(int bn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "setp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n"
+        "}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+struct TcParams {
+    int m_tiles, n_tiles;     // output tiles of 128 x bn
+    int bn;                   // N tile (multiple of 16, <= 256)
+    int k_tiles;              // k tiles of 64 per CTA (split range)
+    int k_tiles_total;
+    int mode;                 // 0: stage-1 epilogue, 1: stage-2 epilogue
+    int stages;
+    // stage 1: output row m = q_local * npad + p, column i -> X[p][q_local * ldq + i]
+    __nv_bfloat16* xh;
+    __nv_bfloat16* xl;
+    int64_t ldx;  // row stride of X (= qchunk * opad)
+    int npad, opad;
+    int ocols;    // valid columns (the rest of the tile is padding)
+    // stage 2: K[p][p'] += acc (upper tiles only)
+    double* kout;
+    int64_t ldk;
+    int* err;
+};
+
+__global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CUtensorMap mAh,
+                                                      const __grid_constant__ CUtensorMap mAl,
+                                                      const __grid_constant__ CUtensorMap mBh,
+                                                      const __grid_constant__ CUtensorMap mBl, TcParams P) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-byte alignment for the swizzled tiles
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int a_bytes = BM * BK * 2;       // 16 KB
+    const int b_bytes = P.bn * BK * 2;     // bn * 128
+    const int stage_bytes = 2 * a_bytes + 2 * b_bytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + P.stages * stage_bytes);
+    uint64_t* empty = full + P.stages;
+    uint64_t* acc_full = empty + P.stages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nt = blockIdx.x % P.n_tiles;
+    const int mt = blockIdx.x / P.n_tiles;
+    const int split = blockIdx.y;
+    const int m0 = mt * BM, n0 = nt * P.bn;
+    // stage 2 computes only tiles that touch the upper triangle
+    if (P.mode == 1 && n0 + P.bn <= m0) return;
+    const int kt0 = split * P.k_tiles;
+    const int kt1 = min(P.k_tiles_total, kt0 + P.k_tiles);
+    if (kt0 >= kt1) return;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < P.stages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 4 && lane == 0) {
+        prefetch_map(&mAh);
+        prefetch_map(&mAl);
+        prefetch_map(&mBh);
+        prefetch_map(&mBl);
+    }
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;\n" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const int nk = kt1 - kt0;
+
+    if (warp == 4) {
+        if (lane == 0) {
+            int issued = 0;
+            for (int it = 0; it < nk; ++it) {
+                const int s = it % P.stages;
+                const uint32_t ph = (it / P.stages) & 1;
+                if (!mbar_wait(&empty[s], ph ^ 1, P.err)) break;
+                uint8_t* base = smem + s * stage_bytes;
+                mbar_expect_tx(&full[s], stage_bytes);
+                const int kx = (kt0 + it) * BK;
+                tma_load_2d(base, &mAh, &full[s], kx, m0);
+                tma_load_2d(base + a_bytes, &mAl, &full[s], kx, m0);
+                tma_load_2d(base + 2 * a_bytes, &mBh, &full[s], kx, n0);
+                tma_load_2d(base + 2 * a_bytes + b_bytes, &mBl, &full[s], kx, n0);
+                issued = it + 1;
+            }
+            // Before the CTA can exit, every copy this thread issued has landed
+            // (already true on the normal path, where the MMA thread consumed them).
+            for (int it = max(0, issued - P.stages); it < issued; ++it)
+                mbar_wait(&full[it % P.stages], (it / P.stages) & 1, P.err);
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {
+            const uint32_t idesc = idesc_bf16(P.bn);
+            for (int it = 0; it < nk; ++it) {
+                const int s = it % P.stages;
+                const uint32_t ph = (it / P.stages) & 1;
+                if (!mbar_wait(&full[s], ph, P.err)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                uint8_t* base = smem + s * stage_bytes;
+                const uint64_t ah = umma_desc(smem_u32(base)), al = umma_desc(smem_u32(base + a_bytes));
+                const uint64_t bh = umma_desc(smem_u32(base + 2 * a_bytes));
+                const uint64_t bl = umma_desc(smem_u32(base + 2 * a_bytes + b_bytes));
+#pragma unroll
+                for (int k = 0; k < BK / 16; ++k) {
+                    const uint64_t adv = (uint64_t)(k * 32) >> 4;  // 16 BF16 = 32 bytes along the swizzled row
+                    const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
+                    umma_bf16(tmem, ah + adv, bh + adv, idesc, acc);
+                    umma_bf16(tmem, ah + adv, bl + adv, idesc, 1u);
+                    umma_bf16(tmem, al + adv, bh + adv, idesc, 1u);
+                }
+                umma_commit(&empty[s]);
+            }
+            // Arrives once every MMA issued above has completed, also on the error
+            // path, so TMEM is never freed under a running MMA.
+            umma_commit(acc_full);
+        }
+    } else {
+        // epilogue: warps 0-3 own TMEM lanes 32w .. 32w+31 (output rows)
+        const bool ready = mbar_wait(acc_full, 0, P.err) && *(volatile int*)P.err == 0;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const int row = m0 + warp * 32 + lane;
+        if (ready) {
+            for (int c = 0; c < P.bn; c += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+                if (P.mode == 0) {
+                    const int ql = row / P.npad, p = row % P.npad;
+                    const int i0 = n0 + c;
+                    __nv_bfloat16* dh = P.xh + (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
+                    __nv_bfloat16* dl = P.xl + (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
+                    if (row < P.m_tiles * BM) {
+#pragma unroll
+                        for (int j = 0; j < 16; j += 2) {
+                            const __nv_bfloat16 h0 = __float2bfloat16_rn(v[j]), h1 = __float2bfloat16_rn(v[j + 1]);
+                            const __nv_bfloat16 l0 = __float2bfloat16_rn(v[j] - __bfloat162float(h0));
+                            const __nv_bfloat16 l1 = __float2bfloat16_rn(v[j + 1] - __bfloat162float(h1));
+                            *reinterpret_cast<__nv_bfloat162*>(dh + j) = __halves2bfloat162(h0, h1);
+                            *reinterpret_cast<__nv_bfloat162*>(dl + j) = __halves2bfloat162(l0, l1);
+                        }
+                    }
+                } else {
+                    double* dst = P.kout + (int64_t)row * P.ldk + n0 + c;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) atomicAdd(dst + j, (double)v[j]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 5) {
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;\n" ::"r"(tmem));
+    }
+}
+
+// Full BF16 hi/lo copies of B: Bh[q][p][r] from the FP64 upper-tile packing.
+__global__ void k_split_b_full(const double* __restrict__ B, int64_t ldb, int nt, int npad, int q0, int qc,
+                               __nv_bfloat16* __restrict__ bh, __nv_bfloat16* __restrict__ bl) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t per_q = (int64_t)npad * npad;
+    if (e >= per_q * qc) return;
+    const int ql = (int)(e / per_q);
+    const int64_t rem = e % per_q;
+    int p = (int)(rem / npad), r = (int)(rem % npad);
+    int I = p >> 6, J = r >> 6, a = p & 63, b = r & 63;
+    if (I > J) {
+        const int t = I;
+        I = J;
+        J = t;
+        const int u = a;
+        a = b;
+        b = u;
+    }
+    const int64_t tile = (int64_t)I * nt - (int64_t)I * (I - 1) / 2 + (J - I);
+    const double x = B[(int64_t)(q0 + ql) * ldb + tile * 4096 + a * 64 + b];
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    bh[e] = h;
+    bl[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+}
+
+// C^T in FP64 ([opad][npad]) -> BF16 hi/lo.
+__global__ void k_split_ct(const double* __restrict__ ct, int64_t count, __nv_bfloat16* __restrict__ h,
+                           __nv_bfloat16* __restrict__ l) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    const double x = ct[e];
+    const __nv_bfloat16 hi = __double2bfloat16(x);
+    h[e] = hi;
+    l[e] = __double2bfloat16(x - (double)__bfloat162float(hi));
+}
+
+__global__ void k_symmetrize_upper128(const double* __restrict__ Kp, int64_t ldk, int64_t n, double* __restrict__ K) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * n) return;
+    const int64_t mu = e / n, nu = e % n;
+    const bool upper = (mu >> 7) <= (nu >> 7);
+    K[e] = upper ? Kp[mu * ldk + nu] : Kp[nu * ldk + mu];
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 2D BF16 tensor map: rows x cols (cols contiguous), box 64 cols x box_rows, 128B swizzle.
+bool make_map(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {cols, rows};
+    cuuint64_t strides[1] = {cols * 2};
+    cuuint32_t box[2] = {BK, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+size_t smem_for(int bn, int stages) { return (size_t)stages * (2 * BM * BK * 2 + 2 * bn * BK * 2) + 1024 + 256; }
+
+cudaError_t launch_tc(const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh, const CUtensorMap& bl,
+                      const TcParams& P, int splits, cudaStream_t stream) {
+    const size_t smem = smem_for(P.bn, P.stages);
+    cudaError_t e = cudaFuncSetAttribute(k_tc_split3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(P.m_tiles * P.n_tiles, splits);
+    k_tc_split3<<<grid, 192, smem, stream>>>(ah, al, bh, bl, P);
+    return cudaGetLastError();
+}
+
+int stages_for(int bn) {
+    const size_t per = 2 * BM * BK * 2 + 2 * (size_t)bn * BK * 2;
+    return (int)std::min<size_t>(4, (200 * 1024) / per);
+}
+
+}  // namespace
+
+TcPlan tc_plan(int64_t n, int naux, int64_t ncols) {
+    TcPlan t{};
+    t.npad = (n + 127) / 128 * 128;
+    const int64_t o = std::max<int64_t>(ncols, 1);
+    t.n_tiles1 = (int)((o + 255) / 256);
+    t.bn1 = (int)(((o + t.n_tiles1 - 1) / t.n_tiles1 + 15) / 16 * 16);
+    t.opad = t.bn1 * t.n_tiles1;
+    t.naux = naux;
+    return t;
+}
+
+size_t tc_b_bytes(int64_t n, int naux) {
+    const int64_t npad = (n + 127) / 128 * 128;
+    return sizeof(__nv_bfloat16) * 2 * (size_t)npad * npad * naux;
+}
+
+cudaError_t tc_split_b(const JkPlan& p, int64_t npad, void* bf16_b, cudaStream_t stream) {
+    __nv_bfloat16* bh = static_cast<__nv_bfloat16*>(bf16_b);
+    const int64_t per_q = npad * npad;
+    __nv_bfloat16* bl = bh + per_q * p.naux;
+    const int qblock = 256;
+    for (int q0 = 0; q0 < p.naux; q0 += qblock) {
+        const int qc = std::min(qblock, p.naux - q0);
+        const int64_t total = per_q * qc;
+        k_split_b_full<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(p.B, p.ldb, p.nt, (int)npad, q0, qc,
+                                                                             bh + per_q * q0, bl + per_q * q0);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const double* Ct_fp64, int64_t ct_ld,
+                                double* K, double* Kp, void* work, size_t work_bytes, int* d_err,
+                                cudaStream_t stream, int64_t n) {
+    (void)ct_ld;
+    const int64_t npad = t.npad;
+    const __nv_bfloat16* bh = static_cast<const __nv_bfloat16*>(bf16_b);
+    const __nv_bfloat16* bl = bh + npad * npad * t.naux;
+    // work: Ct hi/lo [opad][npad] | X hi/lo [npad][qchunk*opad]
+    __nv_bfloat16* cth = static_cast<__nv_bfloat16*>(work);
+    __nv_bfloat16* ctl = cth + (int64_t)t.opad * npad;
+    __nv_bfloat16* xbase = ctl + (int64_t)t.opad * npad;
+    const size_t ct_bytes = sizeof(__nv_bfloat16) * 2 * (size_t)t.opad * npad;
+    if (work_bytes <= ct_bytes) return cudaErrorInvalidValue;
+    const size_t per_q = sizeof(__nv_bfloat16) * 2 * (size_t)npad * t.opad;
+    int qchunk = (int)std::min<size_t>((work_bytes - ct_bytes) / per_q, (size_t)t.naux);
+    if (qchunk < 1) return cudaErrorInvalidValue;
+    const int64_t cnt = (int64_t)t.opad * npad;
+    k_split_ct<<<(unsigned)((cnt + 255) / 256), 256, 0, stream>>>(Ct_fp64, cnt, cth, ctl);
+    cudaMemsetAsync(Kp, 0, sizeof(double) * npad * npad, stream);
+    CUtensorMap mCh, mCl;
+    if (!make_map(&mCh, cth, t.opad, npad, t.bn1) || !make_map(&mCl, ctl, t.opad, npad, t.bn1))
+        return cudaErrorInvalidValue;
+    for (int q0 = 0; q0 < t.naux; q0 += qchunk) {
+        const int qc = std::min(qchunk, t.naux - q0);
+        const int64_t ldx = (int64_t)qc * t.opad;
+        __nv_bfloat16* xh = xbase;
+        __nv_bfloat16* xl = xbase + npad * ldx;
+        // stage 1: rows (q, p) of the full BF16 B for q in [q0, q0 + qc)
+        CUtensorMap mAh, mAl;
+        const uint64_t rows = (uint64_t)qc * npad;
+        if (!make_map(&mAh, bh + (int64_t)q0 * npad * npad, rows, npad, BM) ||
+            !make_map(&mAl, bl + (int64_t)q0 * npad * npad, rows, npad, BM))
+            return cudaErrorInvalidValue;
+        TcParams P{};
+        P.m_tiles = (int)(rows / BM);
+        P.n_tiles = t.n_tiles1;
+        P.bn = t.bn1;
+        P.k_tiles_total = (int)(npad / BK);
+        P.k_tiles = P.k_tiles_total;
+        P.mode = 0;
+        P.stages = stages_for(P.bn);
+        P.xh = xh;
+        P.xl = xl;
+        P.ldx = ldx;
+        P.npad = (int)npad;
+        P.opad = t.opad;
+        P.ocols = t.opad;
+        P.err = d_err;
+        cudaError_t e = launch_tc(mAh, mAl, mCh, mCl, P, 1, stream);
+        if (e != cudaSuccess) return e;
+        // stage 2: K += X X^T over this chunk, split over k
+        const int bn2 = 256 <= npad ? 256 : 128;
+        CUtensorMap mXh, mXl, mXh2, mXl2;
+        if (!make_map(&mXh, xh, npad, ldx, BM) || !make_map(&mXl, xl, npad, ldx, BM) ||
+            !make_map(&mXh2, xh, npad, ldx, bn2) || !make_map(&mXl2, xl, npad, ldx, bn2))
+            return cudaErrorInvalidValue;
+        TcParams Q{};
+        Q.m_tiles = (int)(npad / BM);
+        Q.n_tiles = (int)(npad / bn2);
+        Q.bn = bn2;
+        Q.k_tiles_total = (int)((ldx + BK - 1) / BK);  // the ragged last tile reads zeros past ldx
+        int upper = 0;
+        for (int mt = 0; mt < Q.m_tiles; ++mt)
+            for (int ntile = 0; ntile < Q.n_tiles; ++ntile)
+                if ((ntile + 1) * bn2 > mt * BM) ++upper;
+        const int splits = std::max(1, std::min(Q.k_tiles_total, (2 * 148 + upper - 1) / upper));
+        Q.k_tiles = (Q.k_tiles_total + splits - 1) / splits;
+        Q.mode = 1;
+        Q.stages = stages_for(bn2);
+        Q.kout = Kp;
+        Q.ldk = npad;
+        Q.err = d_err;
+        e = launch_tc(mXh, mXl, mXh2, mXl2, Q, splits, stream);
+        if (e != cudaSuccess) return e;
+    }
+    k_symmetrize_upper128<<<(unsigned)((n * n + 255) / 256), 256, 0, stream>>>(Kp, npad, n, K);
+    return cudaGetLastError();
+}
+
+}  // namespace hf

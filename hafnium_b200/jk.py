@@ -130,15 +130,25 @@ class B200DensityFittedCoulombExchange:
         self.context.exchange_factored_device(c, out, sign, self.precision)
         return out if on_device else out.cpu().numpy()
 
-    def exchange_factored(self, factor, weights=None):
-        """``K`` for ``D = C diag(w) C^T`` with ``C`` of shape ``[n_ao, k]`` (device tensors)."""
+    def exchange_factored(self, factor, weights=None, precision: int | None = None):
+        """``K`` for ``D = C diag(w) C^T`` with ``C`` of shape ``[n_ao, k]``."""
+        prec = self.precision if precision is None else precision
         if _is_torch(factor) and factor.is_cuda:
             import torch
 
             out = torch.empty((self._n_ao, self._n_ao), dtype=torch.float64, device=factor.device)
-            self.context.exchange_factored_device(factor.contiguous(), out, weights, self.precision)
+            self.context.exchange_factored_device(factor.contiguous(), out, weights, prec)
             return out
-        return self.context.exchange_factored_host(np.asarray(factor), weights, self.precision)
+        return self.context.exchange_factored_host(np.asarray(factor), weights, prec)
+
+    def context_exchange_bf16(self, density):
+        """Split-BF16 K of a positive semidefinite device density."""
+        import torch
+
+        d = density.to(torch.float64).contiguous()
+        out = torch.empty_like(d)
+        self.context.exchange_device(d, out, _lib.PREC_BF16X3)
+        return out
 
     def stats(self) -> dict:
         return self.context.stats()

@@ -1,0 +1,370 @@
+"""The learned initial density: a message-passing network over waters.
+
+Nodes are the waters of a cluster, edges the ordered pairs whose oxygens are
+closer than ``R_CUT``. Every edge carries the geometry of water j seen from the
+frame of water i (oxygen and hydrogen positions, the relative rotation, a radial
+basis of the O-O distance), so everything the network sees and predicts is
+independent of how the cluster sits in space. Four residual message-passing
+layers of width 128 feed two heads: the 24 x 24 diagonal block of each water's
+density in its own frame (300 upper entries, on top of the training set's mean
+block) and the 24 x 24 block between the two waters of each edge. Blocks between
+waters further apart than ``R_CUT`` are zero.
+
+Forward, backward and Adam run on the device through the kernels of
+include/hfnn.h (FP32). ``predict`` turns the blocks into a global density and
+projects it onto the occupied space (the n_occ leading natural orbitals in the
+overlap metric), so the SCF starts from an idempotent density with the right
+electron count. Without trained weights or for anything but water clusters the
+caller falls back to the superposition of atomic densities.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import json
+import math
+import pathlib
+
+import numpy as np
+
+from hafnium_b200.learned.frames import ao_rotation, cluster_frames
+
+R_CUT = 9.0  # bohr, O-O
+N_RBF = 16
+EDGE_FEATURES = 3 * 3 + 9 + N_RBF  # positions of j's atoms in i's frame, R_i^T R_j, RBF
+WIDTH = 128
+LAYERS = 4
+NW_AO = 24  # cc-pVDZ functions per water
+DIAG = NW_AO * (NW_AO + 1) // 2
+OFF = NW_AO * NW_AO
+WEIGHTS = pathlib.Path(__file__).resolve().parent / "weights_ccpvdz_water.npz"
+_IU = np.triu_indices(NW_AO)
+
+WATER_LAYOUT = None  # (l, n_contractions) per shell of one water in cc-pVDZ
+
+
+def water_layout():
+    global WATER_LAYOUT
+    if WATER_LAYOUT is None:
+        from hafnium_b200.basis import ShellTable
+        from hafnium_b200.molecule import water
+
+        mol = water()
+        t = ShellTable.build("cc-pvdz", mol.symbols, mol.positions)
+        WATER_LAYOUT = [(int(l), int(k)) for l, k in zip(t.angular_momenta, t.n_contractions)]
+    return WATER_LAYOUT
+
+
+def is_water_cluster(molecule) -> bool:
+    s = molecule.symbols
+    return len(s) % 3 == 0 and all(s[3 * w: 3 * w + 3] == ("O", "H", "H") for w in range(len(s) // 3))
+
+
+def build_graph(molecule) -> dict:
+    """Nodes, edges, edge features and the per-water AO rotations (host arrays)."""
+    frames = cluster_frames(molecule)
+    pos = np.asarray(molecule.positions)
+    nw = len(frames)
+    layout = water_layout()
+    rot = np.stack([ao_rotation(r, layout) for _, r in frames])  # [nw, 24, 24]
+    src, dst, feats, fcut = [], [], [], []
+    centers = np.linspace(1.5, R_CUT, N_RBF)
+    width = centers[1] - centers[0]
+    for i in range(nw):
+        oi, ri = frames[i]
+        for j in range(nw):
+            if i == j:
+                continue
+            oj, rj = frames[j]
+            d = np.linalg.norm(oj - oi)
+            if d >= R_CUT:
+                continue
+            rel = np.concatenate([ri.T @ (pos[3 * j + a] - oi) for a in range(3)]) / R_CUT
+            rbf = np.exp(-((d - centers) / width) ** 2)
+            feats.append(np.concatenate([rel, (ri.T @ rj).reshape(-1), rbf]))
+            src.append(i)
+            dst.append(j)
+            fcut.append(0.5 * (math.cos(math.pi * d / R_CUT) + 1.0))
+    return {
+        "n_nodes": nw,
+        "src": np.asarray(src, dtype=np.int32),
+        "dst": np.asarray(dst, dtype=np.int32),
+        "edge": np.asarray(feats, dtype=np.float64).reshape(-1, EDGE_FEATURES),
+        "fcut": np.asarray(fcut, dtype=np.float64),
+        "rot": rot,
+    }
+
+
+def local_targets(graph: dict, density: np.ndarray, mean_diag: np.ndarray | None = None) -> dict:
+    """Blocks of a converged (per-spin) density in the frames of their waters."""
+    rot = graph["rot"]
+    nw = graph["n_nodes"]
+    blk = lambda i, j: density[NW_AO * i: NW_AO * (i + 1), NW_AO * j: NW_AO * (j + 1)]  # noqa: E731
+    d = np.stack([(rot[i].T @ blk(i, i) @ rot[i])[_IU] for i in range(nw)])
+    if mean_diag is not None:
+        d = d - mean_diag
+    o = np.stack([(rot[i].T @ blk(i, j) @ rot[j]).reshape(-1) for i, j in zip(graph["src"], graph["dst"])]) \
+        if len(graph["src"]) else np.zeros((0, OFF))
+    return {"d": d, "o": o}
+
+
+def init_params(seed: int = 0) -> dict:
+    rng = np.random.default_rng(seed)
+
+    def dense(i, o, scale=1.0):
+        return (rng.normal(size=(i, o)) * scale / math.sqrt(i)).astype(np.float32), np.zeros(o, np.float32)
+
+    p = {"h0": (rng.normal(size=WIDTH) * 0.5).astype(np.float32)}
+    for l in range(LAYERS):
+        p[f"Wm{l}"], p[f"bm{l}"] = dense(2 * WIDTH + EDGE_FEATURES, WIDTH)
+        p[f"Wu{l}"], p[f"bu{l}"] = dense(2 * WIDTH, WIDTH, 0.5)
+    p["Wd"], p["bd"] = dense(WIDTH, DIAG, 0.1)
+    p["We"], p["be"] = dense(2 * WIDTH + EDGE_FEATURES, WIDTH)
+    p["Wo"], p["bo"] = dense(WIDTH, OFF, 0.1)
+    return p
+
+
+def param_names(layers: int = LAYERS):
+    names = ["h0"]
+    for l in range(layers):
+        names += [f"Wm{l}", f"bm{l}", f"Wu{l}", f"bu{l}"]
+    return names + ["Wd", "bd", "We", "be", "Wo", "bo"]
+
+
+class DeviceNet:
+    """Parameters on the device and the forward/backward passes over one graph."""
+
+    def __init__(self, params: dict, layers: int = LAYERS, device: int = 0) -> None:
+        import torch
+
+        from hafnium_b200 import _lib
+
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.layers = layers
+        self.lib = _lib.load()
+        self._bind()
+        self.p = {k: torch.as_tensor(np.asarray(v, dtype=np.float32), device=self.dev).contiguous()
+                  for k, v in params.items()}
+        self.width = int(self.p["h0"].shape[0])
+
+    def _bind(self) -> None:
+        L, v, f, i, i64 = self.lib, ctypes.c_void_p, ctypes.c_float, ctypes.c_int, ctypes.c_int64
+        L.hfnn_sgemm.argtypes = [i, i, i, v, i, v, i, v, v, i, v]
+        L.hfnn_silu.argtypes = [i64, i, v, v, v, i, v]
+        L.hfnn_dsilu.argtypes = [i64, i, v, v, v, v, v]
+        L.hfnn_gather.argtypes = [i64, i, v, v, v, i, i, v]
+        L.hfnn_scatter_add.argtypes = [i64, i, v, i, i, v, v, v, v]
+        L.hfnn_colsum.argtypes = [i64, i, v, v, v]
+        L.hfnn_sq_loss.argtypes = [i64, v, v, f, v, v, v]
+        L.hfnn_adam.argtypes = [i64, v, v, v, v, f, f, f, f, i, v]
+
+    @staticmethod
+    def _ptr(t):
+        return None if t is None else t.data_ptr()
+
+    def _ok(self, status: int, what: str) -> None:
+        if status != 0:
+            from hafnium_b200.errors import BackendError
+
+            raise BackendError(f"{what} failed with status {status}")
+
+    def _stream(self):
+        return self.torch.cuda.current_stream(self.dev).cuda_stream
+
+    def linear(self, x, w, b, out=None, ta=0, tb=0, accumulate=0):
+        """out = op(x) op(w) + b with the shapes hfnn_sgemm takes."""
+        m = x.shape[1] if ta else x.shape[0]
+        k = x.shape[0] if ta else x.shape[1]
+        n = w.shape[0] if tb else w.shape[1]
+        if out is None:
+            out = self.torch.empty((m, n), dtype=self.torch.float32, device=self.dev)
+        self._ok(self.lib.hfnn_sgemm(m, n, k, self._ptr(x), ta, self._ptr(w), tb, self._ptr(b), self._ptr(out),
+                                     accumulate, self._stream()), "hfnn_sgemm")
+        return out
+
+    def upload_graph(self, graph: dict) -> dict:
+        t = self.torch
+        return {
+            "n": graph["n_nodes"],
+            "src": t.as_tensor(graph["src"], dtype=t.int32, device=self.dev),
+            "dst": t.as_tensor(graph["dst"], dtype=t.int32, device=self.dev),
+            "edge": t.as_tensor(graph["edge"], dtype=t.float32, device=self.dev).contiguous(),
+            "fcut": t.as_tensor(graph["fcut"], dtype=t.float32, device=self.dev).contiguous(),
+            "ne": int(len(graph["src"])),
+        }
+
+    def _edge_input(self, h, g):
+        t, W = self.torch, self.width
+        ne = g["ne"]
+        x = t.empty((ne, 2 * W + EDGE_FEATURES), dtype=t.float32, device=self.dev)
+        s = self._stream()
+        ld = 2 * W + EDGE_FEATURES
+        self._ok(self.lib.hfnn_gather(ne, W, self._ptr(h), self._ptr(g["src"]), self._ptr(x), ld, 0, s), "gather")
+        self._ok(self.lib.hfnn_gather(ne, W, self._ptr(h), self._ptr(g["dst"]), self._ptr(x), ld, W, s), "gather")
+        self._ok(self.lib.hfnn_gather(ne, EDGE_FEATURES, self._ptr(g["edge"]), None, self._ptr(x), ld, 2 * W, s),
+                 "gather")
+        return x
+
+    def forward(self, g):
+        t, W, s = self.torch, self.width, self._stream()
+        n, ne = g["n"], g["ne"]
+        h = self.p["h0"].unsqueeze(0).repeat(n, 1).contiguous()
+        cache = []
+        for l in range(self.layers):
+            xm = self._edge_input(h, g)
+            zm = self.linear(xm, self.p[f"Wm{l}"], self.p[f"bm{l}"])
+            m = t.empty_like(zm)
+            self._ok(self.lib.hfnn_silu(ne, W, self._ptr(zm), self._ptr(g["fcut"]), self._ptr(m), 0, s), "silu")
+            a = t.zeros((n, W), dtype=t.float32, device=self.dev)
+            self._ok(self.lib.hfnn_scatter_add(ne, W, self._ptr(m), W, 0, self._ptr(g["src"]), None, self._ptr(a), s),
+                     "scatter")
+            xu = t.cat([h, a], dim=1).contiguous()
+            zu = self.linear(xu, self.p[f"Wu{l}"], self.p[f"bu{l}"])
+            cache.append((xm, zm, xu, zu))
+            h = h.clone()
+            self._ok(self.lib.hfnn_silu(n, W, self._ptr(zu), None, self._ptr(h), 1, s), "silu")
+        d = self.linear(h, self.p["Wd"], self.p["bd"])
+        xe = self._edge_input(h, g)
+        ze = self.linear(xe, self.p["We"], self.p["be"])
+        ge = t.empty_like(ze)
+        self._ok(self.lib.hfnn_silu(ne, W, self._ptr(ze), None, self._ptr(ge), 0, s), "silu")
+        o = self.linear(ge, self.p["Wo"], self.p["bo"])
+        return {"d": d, "o": o, "h": h}, (cache, xe, ze, ge)
+
+    def loss_and_grad(self, g, targets: dict, w_edge: float = 1.0):
+        t, W, s = self.torch, self.width, self._stream()
+        n, ne = g["n"], g["ne"]
+        out, (cache, xe, ze, ge) = self.forward(g)
+        loss = t.zeros(1, dtype=t.float32, device=self.dev)
+        dd = t.empty_like(out["d"])
+        do = t.empty_like(out["o"])
+        self._ok(self.lib.hfnn_sq_loss(dd.numel(), self._ptr(out["d"]), self._ptr(targets["d"]), 1.0, self._ptr(dd),
+                                       self._ptr(loss), s), "loss")
+        self._ok(self.lib.hfnn_sq_loss(do.numel(), self._ptr(out["o"]), self._ptr(targets["o"]), w_edge,
+                                       self._ptr(do), self._ptr(loss), s), "loss")
+        grads = {}
+        h = out["h"]
+
+        def dense_bwd(x, dz, wname, bname):
+            grads[wname] = self.linear(x, dz, None, ta=1)  # x^T dz
+            gb = t.empty(dz.shape[1], dtype=t.float32, device=self.dev)
+            self._ok(self.lib.hfnn_colsum(dz.shape[0], dz.shape[1], self._ptr(dz), self._ptr(gb), s), "colsum")
+            grads[bname] = gb
+            return self.linear(dz, self.p[wname], None, tb=1)  # dz W^T
+
+        dh = dense_bwd(h, dd, "Wd", "bd")
+        dg = dense_bwd(ge, do, "Wo", "bo")
+        dze = t.empty_like(ze)
+        self._ok(self.lib.hfnn_dsilu(ne, W, self._ptr(dg), self._ptr(ze), None, self._ptr(dze), s), "dsilu")
+        dxe = dense_bwd(xe, dze, "We", "be")
+        ld = 2 * W + EDGE_FEATURES
+        self._ok(self.lib.hfnn_scatter_add(ne, W, self._ptr(dxe), ld, 0, self._ptr(g["src"]), None, self._ptr(dh), s),
+                 "scatter")
+        self._ok(self.lib.hfnn_scatter_add(ne, W, self._ptr(dxe), ld, W, self._ptr(g["dst"]), None, self._ptr(dh), s),
+                 "scatter")
+        for l in reversed(range(self.layers)):
+            xm, zm, xu, zu = cache[l]
+            dzu = t.empty_like(zu)
+            self._ok(self.lib.hfnn_dsilu(n, W, self._ptr(dh), self._ptr(zu), None, self._ptr(dzu), s), "dsilu")
+            dxu = dense_bwd(xu, dzu, f"Wu{l}", f"bu{l}")
+            dh_in = dh + dxu[:, :W]
+            da = dxu[:, W:].contiguous()
+            dm = t.empty((ne, W), dtype=t.float32, device=self.dev)
+            self._ok(self.lib.hfnn_gather(ne, W, self._ptr(da), self._ptr(g["src"]), self._ptr(dm), W, 0, s),
+                     "gather")
+            dzm = t.empty_like(zm)
+            self._ok(self.lib.hfnn_dsilu(ne, W, self._ptr(dm), self._ptr(zm), self._ptr(g["fcut"]), self._ptr(dzm), s),
+                     "dsilu")
+            dxm = dense_bwd(xm, dzm, f"Wm{l}", f"bm{l}")
+            dh_in = dh_in.contiguous()
+            self._ok(self.lib.hfnn_scatter_add(ne, W, self._ptr(dxm), ld, 0, self._ptr(g["src"]), None,
+                                               self._ptr(dh_in), s), "scatter")
+            self._ok(self.lib.hfnn_scatter_add(ne, W, self._ptr(dxm), ld, W, self._ptr(g["dst"]), None,
+                                               self._ptr(dh_in), s), "scatter")
+            dh = dh_in
+        gh0 = t.empty(W, dtype=t.float32, device=self.dev)
+        self._ok(self.lib.hfnn_colsum(n, W, self._ptr(dh.contiguous()), self._ptr(gh0), s), "colsum")
+        grads["h0"] = gh0
+        return loss, grads
+
+
+class Adam:
+    def __init__(self, net: DeviceNet, lr: float = 1e-3) -> None:
+        t = net.torch
+        self.net, self.lr, self.step = net, lr, 0
+        self.m = {k: t.zeros_like(v) for k, v in net.p.items()}
+        self.v = {k: t.zeros_like(v) for k, v in net.p.items()}
+
+    def apply(self, grads: dict, scale: float = 1.0) -> None:
+        self.step += 1
+        net = self.net
+        for k, p in net.p.items():
+            g = grads[k] * scale if scale != 1.0 else grads[k]
+            net._ok(net.lib.hfnn_adam(p.numel(), p.data_ptr(), g.contiguous().data_ptr(), self.m[k].data_ptr(),
+                                      self.v[k].data_ptr(), self.lr, 0.9, 0.999, 1e-8, self.step, net._stream()),
+                    "adam")
+
+
+def save_weights(path: pathlib.Path, params: dict, mean_diag: np.ndarray, meta: dict) -> str:
+    arrays = {k: np.asarray(v, dtype=np.float32) for k, v in params.items()}
+    arrays["mean_diag"] = np.asarray(mean_diag, dtype=np.float64)
+    digest = hashlib.sha256()
+    for k in sorted(arrays):
+        digest.update(k.encode())
+        digest.update(np.ascontiguousarray(arrays[k]).tobytes())
+    meta = dict(meta, sha256=digest.hexdigest(), version=1, layers=LAYERS, width=WIDTH, r_cut=R_CUT)
+    np.savez_compressed(path, meta=json.dumps(meta), **arrays)
+    return meta["sha256"]
+
+
+def load_weights(path: pathlib.Path = WEIGHTS):
+    """Parameters, the mean diagonal block and the metadata; None when absent or corrupt."""
+    if not pathlib.Path(path).exists():
+        return None
+    with np.load(path) as z:
+        meta = json.loads(str(z["meta"]))
+        arrays = {k: z[k] for k in z.files if k != "meta"}
+    digest = hashlib.sha256()
+    for k in sorted(arrays):
+        digest.update(k.encode())
+        digest.update(np.ascontiguousarray(arrays[k]).tobytes())
+    if digest.hexdigest() != meta.get("sha256"):
+        return None
+    mean_diag = arrays.pop("mean_diag")
+    return arrays, mean_diag, meta
+
+
+def blocks_to_density(graph: dict, d_blocks: np.ndarray, o_blocks: np.ndarray, mean_diag: np.ndarray) -> np.ndarray:
+    """Global per-spin density from local-frame blocks (symmetrised over edge pairs)."""
+    nw = graph["n_nodes"]
+    rot = graph["rot"]
+    n = NW_AO * nw
+    dens = np.zeros((n, n))
+    for i in range(nw):
+        b = np.zeros((NW_AO, NW_AO))
+        b[_IU] = d_blocks[i] + mean_diag
+        b = b + np.triu(b, 1).T
+        dens[NW_AO * i: NW_AO * (i + 1), NW_AO * i: NW_AO * (i + 1)] = rot[i] @ b @ rot[i].T
+    for e, (i, j) in enumerate(zip(graph["src"], graph["dst"])):
+        b = rot[i] @ o_blocks[e].reshape(NW_AO, NW_AO) @ rot[j].T
+        dens[NW_AO * i: NW_AO * (i + 1), NW_AO * j: NW_AO * (j + 1)] += 0.5 * b
+        dens[NW_AO * j: NW_AO * (j + 1), NW_AO * i: NW_AO * (i + 1)] += 0.5 * b.T
+    return dens
+
+
+def predict_density(molecule, weights=None, device: int = 0):
+    """The network's per-spin density of a water cluster, or None (fall back to SAD)."""
+    if not is_water_cluster(molecule):
+        return None
+    loaded = load_weights() if weights is None else weights
+    if loaded is None:
+        return None
+    params, mean_diag, _ = loaded
+    graph = build_graph(molecule)
+    net = DeviceNet(params, device=device)
+    out, _ = net.forward(net.upload_graph(graph))
+    d = out["d"].double().cpu().numpy()
+    o = out["o"].double().cpu().numpy()
+    return blocks_to_density(graph, d, o, mean_diag)

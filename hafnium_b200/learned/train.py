@@ -1,0 +1,153 @@
+"""Train the learned initial density on converged densities from this SCF.
+
+    python -m hafnium_b200.learned.train --clusters 400 --epochs 40 --out weights.npz
+
+1. Seeded water clusters (H2O)n, n uniform in [2, 12], are converged with the
+   device DF-RHF (SAD guess, FP64, the reference's default tolerances); their
+   per-spin densities, expressed in the frames of their waters, are the targets.
+2. The network (hafnium_b200.learned.model) is trained with Adam on the device,
+   forward and backward running on the hfnn kernels, several clusters per step.
+3. Held-out (H2O)16-24 clusters are converged from the SAD guess and from the
+   learned guess; the iteration counts, times and energies are recorded in the
+   weights file's metadata.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import pathlib
+import time
+
+import numpy as np
+
+from hafnium_b200.learned import model as M
+
+BASIS, AUX = "cc-pvdz", "def2-universal-jkfit"
+
+
+def converged_density(mol, device: int = 0):
+    from hafnium_b200.scf import DeviceHamiltonian, atomic_density_guess, solve_rhf
+
+    ham = DeviceHamiltonian.build(mol, BASIS, AUX, device=device)
+    res = solve_rhf(ham, guess=atomic_density_guess(mol, BASIS, device=device))
+    return res.density.cpu().numpy(), res
+
+
+def make_dataset(count: int, seed0: int, n_range=(2, 12), device: int = 0):
+    from hafnium_b200.molecule import water_cluster
+
+    rng = np.random.default_rng(seed0)
+    data = []
+    for k in range(count):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        mol = water_cluster(n, seed0 + 1000 + k)
+        dens, _ = converged_density(mol, device)
+        graph = M.build_graph(mol)
+        data.append((graph, M.local_targets(graph, dens)))
+    return data
+
+
+def union(batch):
+    """Disjoint union of several graphs and their targets (one training step)."""
+    offset = 0
+    src, dst, edge, fcut, d, o = [], [], [], [], [], []
+    for graph, tgt in batch:
+        src.append(graph["src"] + offset)
+        dst.append(graph["dst"] + offset)
+        edge.append(graph["edge"])
+        fcut.append(graph["fcut"])
+        d.append(tgt["d"])
+        o.append(tgt["o"])
+        offset += graph["n_nodes"]
+    g = {"n_nodes": offset, "src": np.concatenate(src).astype(np.int32), "dst": np.concatenate(dst).astype(np.int32),
+         "edge": np.concatenate(edge), "fcut": np.concatenate(fcut)}
+    return g, {"d": np.concatenate(d), "o": np.concatenate(o)}
+
+
+def train(data, epochs: int, batch: int = 8, lr: float = 1e-3, seed: int = 0, device: int = 0, log=print):
+    import torch
+
+    mean_diag = np.mean(np.concatenate([t["d"] for _, t in data]), axis=0)
+    net = M.DeviceNet(M.init_params(seed), device=device)
+    opt = M.Adam(net, lr)
+    rng = np.random.default_rng(seed)
+    dev = net.dev
+    prepared = []
+    for i in range(0, len(data), batch):
+        g, t = union(data[i:i + batch])
+        gd = net.upload_graph(g)
+        td = {"d": torch.as_tensor(t["d"] - mean_diag, dtype=torch.float32, device=dev).contiguous(),
+              "o": torch.as_tensor(t["o"], dtype=torch.float32, device=dev).contiguous()}
+        prepared.append((gd, td, float(len(t["d"]))))
+    history = []
+    for epoch in range(epochs):
+        total, nodes = 0.0, 0.0
+        for k in rng.permutation(len(prepared)):
+            gd, td, nn = prepared[k]
+            loss, grads = net.loss_and_grad(gd, td)
+            opt.apply(grads, scale=1.0 / nn)
+            total += float(loss.item())
+            nodes += nn
+        if epoch >= epochs // 2:
+            opt.lr = lr * 0.5 * (1 + np.cos(np.pi * (epoch - epochs // 2) / max(1, epochs - epochs // 2)))
+        history.append(total / nodes)
+        log(f"epoch {epoch:3d}  loss per water {total / nodes:.4e}")
+    params = {k: v.cpu().numpy() for k, v in net.p.items()}
+    return params, mean_diag, history
+
+
+def evaluate(weights, sizes, seed0: int, device: int = 0):
+    """Iterations and time of the plain FP64 SCF from SAD and from the learned guess."""
+    import torch
+
+    from hafnium_b200.molecule import water_cluster
+    from hafnium_b200.scf import DeviceHamiltonian, atomic_density_guess, learned_density_guess, solve_rhf
+
+    rows = []
+    for k, n in enumerate(sizes):
+        mol = water_cluster(n, seed0 + 50000 + k)
+        ham = DeviceHamiltonian.build(mol, BASIS, AUX, device=device)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r_sad = solve_rhf(ham, guess=atomic_density_guess(mol, BASIS, device=device))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        r_ml = solve_rhf(ham, guess=learned_density_guess(mol, ham, weights=weights, device=device))
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        rows.append({"n_waters": n, "sad_iterations": r_sad.n_iterations, "learned_iterations": r_ml.n_iterations,
+                     "sad_s": t1 - t0, "learned_s": t2 - t1, "dE": r_ml.energy - r_sad.energy})
+    return rows
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--clusters", type=int, default=400)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--eval", type=str, default="16,20,24")
+    ap.add_argument("--out", type=str, default=str(M.WEIGHTS))
+    args = ap.parse_args()
+    t0 = time.perf_counter()
+    data = make_dataset(args.clusters, args.seed)
+    t1 = time.perf_counter()
+    print(f"dataset: {len(data)} clusters in {t1 - t0:.1f} s", flush=True)
+    params, mean_diag, history = train(data, args.epochs, args.batch, args.lr, args.seed)
+    t2 = time.perf_counter()
+    meta = {"clusters": args.clusters, "n_range": [2, 12], "epochs": args.epochs, "batch": args.batch, "lr": args.lr,
+            "seed": args.seed, "basis": BASIS, "auxiliary": AUX, "loss_history": history,
+            "dataset_s": t1 - t0, "train_s": t2 - t1}
+    out = pathlib.Path(args.out)
+    M.save_weights(out, params, mean_diag, meta)
+    rows = evaluate((params, mean_diag, meta), [int(x) for x in args.eval.split(",") if x], args.seed)
+    meta["evaluation"] = rows
+    digest = M.save_weights(out, params, mean_diag, meta)
+    print(json.dumps({"weights": str(out), "sha256": digest, "evaluation": rows, "final_loss": history[-1]}),
+          flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -60,15 +60,23 @@ class ScfOptions:
 
 @dataclass(frozen=True)
 class PrecisionSchedule:
-    """Which arithmetic the exchange build uses per iteration.
+    """Which arithmetic each exchange build uses.
 
-    ``fp64``: every build in FP64. ``mixed``: split-BF16 builds of the
-    incremental exchange K(D_new) = K(D_old) + K(dD) while the orbital gradient
-    is above ``switch_gradient``, then FP64 full rebuilds to the end.
+    ``fp64``: every build in FP64 (the plain path).
+
+    ``mixed``: split-BF16 builds (three BF16 products, FP32 accumulation) while
+    the orbital gradient is above ``anchor_gradient``; then incremental builds
+    anchored on an FP64 one, K(C_n) = K64(C_a) + [K16(C_n) - K16(C_a)], so the
+    BF16 error scales with the change of the orbitals since the anchor, with a
+    new anchor each time the gradient falls by ``reanchor_factor``; once the
+    mixed iteration meets the convergence test, FP64 builds to the end, and the
+    test is only passed on two consecutive FP64 energies. DIIS, the eigensolves,
+    J and the energy are FP64 throughout.
     """
 
     mode: str = "fp64"
-    switch_gradient: float = 1e-4
+    anchor_gradient: float = 1e-2
+    reanchor_factor: float = 1e-2
 
     def __post_init__(self) -> None:
         if self.mode not in ("fp64", "mixed"):
@@ -245,6 +253,32 @@ def atomic_density_guess(molecule, basis: str, *, device: int = 0):
     return torch.block_diag(*blocks).contiguous()
 
 
+def project_occupied(ham: DeviceHamiltonian, density, threshold: float = DEFAULT_OVERLAP_THRESHOLD):
+    """The idempotent density of the n_alpha leading natural orbitals of ``density``
+    in the overlap metric: D' = C C^T with X^T S D S X = V diag(w) V^T, C = X V_top."""
+    torch = _torch()
+    x = canonical_orthogonalizer(ham.s, threshold)
+    d = torch.as_tensor(density, dtype=torch.float64, device=ham.s.device)
+    d = 0.5 * (d + d.T)
+    m = x.T @ ham.s @ d @ ham.s @ x
+    w, v = torch.linalg.eigh(0.5 * (m + m.T))
+    c = x @ v[:, -int(ham.n_alpha):]
+    return (c @ c.T).contiguous()
+
+
+def learned_density_guess(molecule, ham: DeviceHamiltonian, *, weights=None, basis: str = "cc-pvdz",
+                          device: int = 0):
+    """The learned network's density projected onto the occupied space; the SAD
+    guess (atoms.py:76-120) when the network does not apply (no weights, not a
+    water cluster in cc-pVDZ)."""
+    from hafnium_b200.learned.model import predict_density
+
+    predicted = predict_density(molecule, weights, device=device) if basis == "cc-pvdz" else None
+    if predicted is None or not np.all(np.isfinite(predicted)):
+        return atomic_density_guess(molecule, basis, device=device)
+    return project_occupied(ham, predicted)
+
+
 class _Rhf:
     def __init__(self, ham: DeviceHamiltonian, options: ScfOptions, schedule: PrecisionSchedule,
                  host_io: bool = False, averaged: bool = False) -> None:
@@ -259,7 +293,8 @@ class _Rhf:
         self.schedule = schedule
         self.x = canonical_orthogonalizer(ham.s, options.overlap_threshold)
         self.n = ham.n_ao
-        self.k_prev = None  # (factor, K) of the last mixed-precision build
+        self.anchor = None  # (K64, K16) of the last FP64 anchor build
+        self.anchor_due = False
         self.timings = {"coulomb_ms": 0.0, "exchange_ms": 0.0, "eigh_ms": 0.0, "fock_builds": 0}
 
     def solve(self, f):
@@ -278,28 +313,39 @@ class _Rhf:
         factor = (c[:, idx] * self.torch.sqrt(occ_t)[None, :]).contiguous()
         return factor @ factor.T, factor
 
+    def _timed(self, key: str, fn):
+        torch = self.torch
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        e1.synchronize()
+        self.timings[f"exchange_ms_{key}"] = self.timings.get(f"exchange_ms_{key}", 0.0) + e0.elapsed_time(e1)
+        self.timings[f"exchange_builds_{key}"] = self.timings.get(f"exchange_builds_{key}", 0) + 1
+        return out
+
     def exchange(self, d, factor, precision: str):
+        """K for this iteration in the arithmetic ``precision`` names:
+        ``fp64``, ``bf16`` (plain split-BF16) or ``anchored`` (incremental on the
+        last FP64 anchor)."""
         two_body = self.ham.two_body
-        if factor is None:
-            return two_body.exchange(d)
         if precision == "fp64":
-            self.k_prev = None
-            return two_body.exchange_factored(factor)
-        # mixed: K(D) = K(D_prev) + K(dD), dD = [C | C_prev] diag(+1, -1) [C | C_prev]^T
-        if self.k_prev is None:
-            k = two_body.exchange_factored(factor)
-        else:
-            f_prev, k_prev = self.k_prev
-            both = self.torch.cat([factor, f_prev], dim=1).contiguous()
-            sign = self.torch.cat([
-                self.torch.ones(factor.shape[1], dtype=self.torch.float64, device=factor.device),
-                -self.torch.ones(f_prev.shape[1], dtype=self.torch.float64, device=factor.device),
-            ])
-            out = self.torch.empty_like(k_prev)
-            two_body.context.exchange_factored_device(both, out, sign, _lib.PREC_BF16X3)
-            k = k_prev + out
-        self.k_prev = (factor, k)
-        return k
+            if factor is None:
+                return self._timed("fp64", lambda: two_body.exchange(d))
+            return self._timed("fp64", lambda: two_body.exchange_factored(factor))
+        if factor is None:
+            return self._timed("bf16", lambda: two_body.context_exchange_bf16(d))
+        k16 = self._timed("bf16", lambda: two_body.exchange_factored(factor, precision=_lib.PREC_BF16X3))
+        if precision == "bf16":
+            return k16
+        if self.anchor is None or self.anchor_due:
+            k64 = self._timed("fp64", lambda: two_body.exchange_factored(factor))
+            self.anchor = (k64, k16)
+            self.anchor_due = False
+            self.timings["anchors"] = self.timings.get("anchors", 0) + 1
+            return k64
+        k64_a, k16_a = self.anchor
+        return k64_a + (k16 - k16_a)
 
     def fock(self, d, factor, precision: str = "fp64"):
         """hamiltonian.py:331-370 for one restricted block."""
@@ -343,24 +389,31 @@ class _Rhf:
             factor = None
         s = self.ham.s
         focks, errors, history = [], [], []
-        precision = "fp64" if self.schedule.mode == "fp64" else "bf16x3"
+        mixed = self.schedule.mode == "mixed"
+        precision = "bf16" if mixed else "fp64"
+        anchor_g = math.inf
         f = None
         for index in range(opts.max_iterations):
             f, _, energy = self.fock(d, factor, precision)
             g = self.x.T @ (f @ d @ s - s @ d @ f) @ self.x
             gnorm = math.sqrt(2.0 * float(torch.sum(g * g)))
-            change = energy - history[-1].energy if history else math.inf
+            previous = history[-1] if history else None
+            change = energy - previous.energy if previous else math.inf
             history.append(Iteration(index, energy, change, gnorm, precision))
-            if precision != "fp64" and gnorm < self.schedule.switch_gradient:
+            converged = abs(change) < opts.energy_tolerance and gnorm < opts.gradient_tolerance
+            if precision == "fp64":
+                # the test counts only when both energies of the pair are FP64
+                if converged and (previous is None or previous.precision == "fp64" or not mixed):
+                    return self.finish(f, history, True, t_start)
+            elif converged or (precision == "anchored" and gnorm < opts.gradient_tolerance):
                 precision = "fp64"
-                # the mixed energies are not final: restart the convergence test in FP64
-                continue_fp64 = True
-            else:
-                continue_fp64 = False
-            if not continue_fp64 and precision == "fp64" and history[-1].precision == "fp64" and (
-                abs(change) < opts.energy_tolerance and gnorm < opts.gradient_tolerance
-            ):
-                return self.finish(f, history, True, t_start)
+            elif precision == "bf16" and gnorm < self.schedule.anchor_gradient:
+                precision = "anchored"
+                self.anchor_due = True
+                anchor_g = gnorm
+            elif precision == "anchored" and gnorm < anchor_g * self.schedule.reanchor_factor:
+                self.anchor_due = True
+                anchor_g = gnorm
             focks = (focks + [f])[-opts.diis_size:]
             errors = (errors + [g])[-opts.diis_size:]
             if len(focks) == 1:

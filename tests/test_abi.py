@@ -14,9 +14,13 @@ import pytest
 ROOT = pathlib.Path(__file__).resolve().parent.parent
 
 
-def declared() -> list[str]:
-    text = (ROOT / "include" / "hfjk.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(hf_\w+)\s*\(", text, flags=re.M)))
+def declared(header: str = "hfjk.h") -> list[str]:
+    text = (ROOT / "include" / header).read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(hf\w+)\s*\(", text, flags=re.M)))
+
+
+def all_declared() -> list[str]:
+    return sorted({name for h in (ROOT / "include").glob("*.h") for name in declared(h.name)})
 
 
 def test_header_declares_the_boundary():
@@ -32,9 +36,10 @@ def test_library_exports_every_declared_symbol():
     if not build.LIBRARY.exists():
         pytest.skip("libhfjk.so is not built (python -m hafnium_b200.build)")
     lib = ctypes.CDLL(str(build.LIBRARY))
-    missing = [name for name in declared() if not hasattr(lib, name)]
+    missing = [name for name in all_declared() if not hasattr(lib, name)]
     assert not missing, missing
-    assert set(declared()) == set(_lib.EXPORTS)
+    assert set(declared("hfjk.h")) == set(_lib.EXPORTS)
+    assert len(declared("hfnn.h")) == 8
 
 
 def test_context_creation_without_a_device_fails_cleanly():

@@ -1,0 +1,57 @@
+"""Split-BF16 exchange on tcgen05 against the FP64 exchange (B200).
+
+Three BF16 products (hi*hi + hi*lo + lo*hi) with FP32 accumulation keep about
+16 significant bits of each operand: the bound checked here is a relative
+error of 5e-5 of the largest |K| element.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from hafnium_b200 import _lib
+from hafnium_b200.jk import B200DensityFittedCoulombExchange
+from tests.helpers import molecule, tables
+
+pytestmark = pytest.mark.gpu
+REL_TOL = 5e-5
+
+
+@pytest.fixture(scope="module", params=["water", "h2o4_s1", "h2o8_s2"])
+def two_body(request):
+    mol = molecule(request.param)
+    orb, aux = tables(mol)
+    return B200DensityFittedCoulombExchange.from_tables(orb, aux)
+
+
+@pytest.mark.parametrize("ncols", [5, 40, 300])
+def test_bf16_factored_exchange_matches_fp64(two_body, ncols):
+    rng = np.random.default_rng(ncols)
+    c = rng.normal(size=(two_body.n_ao, ncols)) / np.sqrt(two_body.n_ao * ncols)
+    ctx = two_body.context
+    k64 = ctx.exchange_factored_host(c, None, _lib.PREC_FP64)
+    k16 = ctx.exchange_factored_host(c, None, _lib.PREC_BF16X3)
+    scale = np.max(np.abs(k64))
+    err = np.max(np.abs(k16 - k64))
+    print(f"n={two_body.n_ao} ncols={ncols}: max|K16-K64| = {err:.2e}, relative {err / scale:.2e}")
+    assert err <= REL_TOL * scale
+    np.testing.assert_allclose(k16, k16.T, atol=0, rtol=0)
+
+
+def test_bf16_exchange_from_a_density(two_body):
+    rng = np.random.default_rng(3)
+    c = rng.normal(size=(two_body.n_ao, 12)) / np.sqrt(two_body.n_ao)
+    d = c @ c.T
+    ctx = two_body.context
+    k64 = ctx.exchange_host(d, _lib.PREC_FP64)
+    k16 = ctx.exchange_host(d, _lib.PREC_BF16X3)
+    assert np.max(np.abs(k16 - k64)) <= REL_TOL * np.max(np.abs(k64))
+
+
+def test_bf16_rejects_negative_weights(two_body):
+    from hafnium_b200.errors import InputError
+
+    c = np.ones((two_body.n_ao, 2))
+    with pytest.raises(InputError, match="non-negative"):
+        two_body.context.exchange_factored_host(c, np.array([1.0, -1.0]), _lib.PREC_BF16X3)
