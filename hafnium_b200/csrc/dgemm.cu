@@ -1,12 +1,37 @@
 // FP64 DMMA GEMM (see dgemm.cuh for the contract).
+//
+// 128 x 64 CTA tiles, 8 warps of 32 x 32, mma.sync.m16n8k8 (FP64 tensor cores),
+// a 3-stage cp.async pipeline from global memory into shared tiles stored
+// row-major with a 20-double row pitch (conflict-free fragment loads), BK = 16.
+// Operands are K-contiguous rows (A[m][k], B[n][k]); copies are 8 bytes so any
+// row stride and offset is legal, and out-of-range elements are zero-filled.
 #include "dgemm.cuh"
 
 namespace hf {
 
 namespace {
-constexpr int BM = 64, BN = 64, BK = 16, LDS = 72;  // LDS: padded row of the k-major tile
+constexpr int BM = 128, BN = 64, BK = 16, LD = BK + 4, STAGES = 3, THREADS = 256;
 
-__global__ void __launch_bounds__(128) k_dgemm_nt(GemmArgs g) {
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// 8-byte asynchronous copy; an invalid element copies nothing and zero-fills
+// (the source then points at the matrix base, which is never read).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, const double* base, bool valid) {
+    const int bytes = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_addr(dst)), "l"(valid ? src : base),
+                 "r"(bytes));
+}
+
+__device__ __forceinline__ void mma16x8x8(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+__global__ void __launch_bounds__(THREADS, 2) k_dgemm_nt(GemmArgs g) {
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     if (g.epi == 2 && n0 > m0 + BM - 1) return;
     if (g.epi == 3 && m0 > n0 + BN - 1) return;
@@ -17,86 +42,107 @@ __global__ void __launch_bounds__(128) k_dgemm_nt(GemmArgs g) {
     if (g.kmode == 1) kb = n0;
     if (g.kmode == 2) ke = min(g.K, m0 + BM);
     kb = (kb / BK) * BK;
+    const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
 
-    __shared__ double As[2][BK][LDS];
-    __shared__ double Bs[2][BK][LDS];
+    extern __shared__ double smem[];
+    double* As = smem;                          // [STAGES][BM][LD]
+    double* Bs = smem + STAGES * BM * LD;       // [STAGES][BN][LD]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g8 = lane >> 2, t4 = lane & 3;
+    const int gq = lane >> 2, tq = lane & 3;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
 
-    // Loader mapping: 64 rows x 16 k per operand = 1024 values, 8 per thread:
-    // thread -> row r = tid >> 1, k half h = (tid & 1) * 8.
-    const int lr = tid >> 1, lk = (tid & 1) * 8;
-    double ra[8], rb[8];
-    auto load = [&](int k0) {
-        const int am = m0 + lr, bn = n0 + lr;
+    auto load = [&](int stage, int k0) {
+        double* as = As + stage * BM * LD;
+        double* bs = Bs + stage * BN * LD;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int k = k0 + lk + j;
-            ra[j] = (am < g.M && k < ke) ? A[(int64_t)am * g.lda + k] : 0.0;
-            rb[j] = (bn < g.N && k < ke) ? B[(int64_t)bn * g.ldb + k] : 0.0;
+        for (int i = 0; i < (BM * BK) / THREADS; ++i) {
+            const int e = tid + i * THREADS;
+            const int r = e / BK, k = e % BK;
+            const int gm = m0 + r, gk = k0 + k;
+            cp_async8(as + r * LD + k, A + (int64_t)gm * g.lda + gk, A, gm < g.M && gk < ke);
+        }
+#pragma unroll
+        for (int i = 0; i < (BN * BK) / THREADS; ++i) {
+            const int e = tid + i * THREADS;
+            const int r = e / BK, k = e % BK;
+            const int gn = n0 + r, gk = k0 + k;
+            cp_async8(bs + r * LD + k, B + (int64_t)gn * g.ldb + gk, B, gn < g.N && gk < ke);
         }
     };
-    auto store = [&](int buf) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            As[buf][lk + j][lr] = ra[j];
-            Bs[buf][lk + j][lr] = rb[j];
-        }
-    };
 
-    double acc[4][4][2];
+    double acc[2][4][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-    int buf = 0;
-    if (kb < ke) {
-        load(kb);
-        store(0);
-    }
-    __syncthreads();
-    for (int k0 = kb; k0 < ke; k0 += BK) {
-        const bool more = k0 + BK < ke;
-        if (more) load(k0 + BK);
-#pragma unroll
-        for (int kk = 0; kk < BK; kk += 4) {
-            double af[4], bf[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) af[i] = As[buf][kk + t4][wm + i * 8 + g8];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) bf[j] = Bs[buf][kk + t4][wn + j * 8 + g8];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
-        }
-        if (more) store(buf ^ 1);
-        __syncthreads();
-        buf ^= 1;
-    }
-
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int m = m0 + wm + i * 8 + g8;
-                const int n = n0 + wn + j * 8 + 2 * t4 + h;
+            for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < nk) load(s, kb + s * BK);
+        asm volatile("cp.async.commit_group;\n" ::);
+    }
+    for (int it = 0; it < nk; ++it) {
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(STAGES - 2));
+        __syncthreads();
+        const int nxt = it + STAGES - 1;
+        if (nxt < nk) load(nxt % STAGES, kb + nxt * BK);
+        asm volatile("cp.async.commit_group;\n" ::);
+        const double* as = As + (it % STAGES) * BM * LD;
+        const double* bs = Bs + (it % STAGES) * BN * LD;
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 8) {
+            double af[2][4], bf[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const double* r0 = as + (wm + i * 16 + gq) * LD + kk + tq;
+                af[i][0] = r0[0];
+                af[i][1] = r0[8 * LD];
+                af[i][2] = r0[4];
+                af[i][3] = r0[8 * LD + 4];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double* c0 = bs + (wn + j * 8 + gq) * LD + kk + tq;
+                bf[j][0] = c0[0];
+                bf[j][1] = c0[4];
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma16x8x8(acc[i][j], af[i], bf[j]);
+        }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
+
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int m = m0 + wm + i * 16 + gq + (v >> 1) * 8;
+                const int n = n0 + wn + j * 8 + 2 * tq + (v & 1);
                 if (m >= g.M || n >= g.N) continue;
                 double* dst = (g.epi == 1) ? &C[(int64_t)n * g.ldc + m] : &C[(int64_t)m * g.ldc + n];
-                const double v = g.alpha * acc[i][j][h];
-                *dst = (g.beta == 0.0) ? v : v + g.beta * *dst;
+                const double val = g.alpha * acc[i][j][v];
+                *dst = (g.beta == 0.0) ? val : val + g.beta * *dst;
             }
 }
 }  // namespace
 
 cudaError_t dgemm_nt(const GemmArgs& g, int batch, cudaStream_t stream) {
     if (g.M <= 0 || g.N <= 0 || batch <= 0) return cudaSuccess;
+    static bool configured = false;
+    const int smem = STAGES * (BM + BN) * LD * (int)sizeof(double);
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_dgemm_nt, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
     dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, batch);
-    k_dgemm_nt<<<grid, 128, 0, stream>>>(g);
+    k_dgemm_nt<<<grid, THREADS, smem, stream>>>(g);
     return cudaGetLastError();
 }
 

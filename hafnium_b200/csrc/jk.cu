@@ -128,104 +128,122 @@ __global__ void k_symmetrize_upper(const double* __restrict__ Kp, int64_t ldk, i
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n * n) return;
     const int64_t mu = e / n, nu = e % n;
-    const bool upper = (mu >> 6) <= (nu >> 6);
-    K[e] = upper ? Kp[mu * ldk + nu] : Kp[nu * ldk + mu];
+    K[e] = mu <= nu ? Kp[mu * ldk + nu] : Kp[nu * ldk + mu];
 }
 
-// X[p][ql][i] = sum_r B_q[p][r] Ct[i][r] for q = q0 + ql, p in row tile I.
-constexpr int BM = 64, BN = 64, BK = 16, LDS = 72;
-__global__ void __launch_bounds__(128) k_exchange_half(const double* __restrict__ B, int64_t ldb, int q0, int nt,
-                                                       const double* __restrict__ Ct, int64_t ldc_t, int npad,
-                                                       double* __restrict__ X, int64_t ldx, int opad) {
-    const int I = blockIdx.y;
-    const int n0 = blockIdx.x * BN;
+// X[p][ql][i] = sum_r B_q[p][r] Ct[i][r] for q = q0 + ql: 128 x 64 tiles, 8 warps,
+// mma.sync.m16n8k8 (FP64), a 3-stage cp.async pipeline. The A operand is
+// gathered from the packed tiles element by element: tile (Ip, J) when Ip <= J,
+// else the transposed tile (J, Ip); 8-byte copies make the transposition free.
+constexpr int XBM = 128, XBN = 64, XBK = 16, XLD = XBK + 4, XST = 3, XTHREADS = 256;
+
+__device__ __forceinline__ uint32_t xsmem(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void xcp8(double* dst, const double* src, const double* base, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(xsmem(dst)), "l"(valid ? src : base),
+                 "r"(valid ? 8 : 0));
+}
+
+__device__ __forceinline__ void xmma(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+__global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* __restrict__ B, int64_t ldb, int q0, int nt,
+                                                             const double* __restrict__ Ct, int64_t ldc_t, int npad,
+                                                             double* __restrict__ X, int64_t ldx, int opad) {
+    const int m0 = blockIdx.y * XBM, n0 = blockIdx.x * XBN;
     const int ql = blockIdx.z;
     const double* Bq = B + (int64_t)(q0 + ql) * ldb;
-    __shared__ double As[2][BK][LDS];
-    __shared__ double Bs[2][BK][LDS];
+    extern __shared__ double xs[];
+    double* As = xs;
+    double* Bs = xs + XST * XBM * XLD;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g8 = lane >> 2, t4 = lane & 3;
+    const int gq = lane >> 2, tq = lane & 3;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    double ra[8], rb[8];
-    // k-contiguous loader (row = tid>>1, 8 k) and m-contiguous loader (k = tid>>3, 8 m)
-    auto load = [&](int k0) {
-        const int Jt = k0 >> 6, kl = k0 & 63;
-        if (Jt >= I) {
-            const double* tile = Bq + ((int64_t)I * nt - (int64_t)I * (I - 1) / 2 + (Jt - I)) * 4096;
-            const double2* src = reinterpret_cast<const double2*>(tile + (tid >> 1) * 64 + kl + (tid & 1) * 8);
+    const int nk = npad / XBK;
+
+    auto load = [&](int stage, int k0) {
+        double* as = As + stage * XBM * XLD;
+        double* bs = Bs + stage * XBN * XLD;
+        const int J = k0 >> 6;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const double2 v = __ldcs(src + j);
-                ra[2 * j] = v.x;
-                ra[2 * j + 1] = v.y;
-            }
-        } else {
-            const double* tile = Bq + ((int64_t)Jt * nt - (int64_t)Jt * (Jt - 1) / 2 + (I - Jt)) * 4096;
-            const double2* src = reinterpret_cast<const double2*>(tile + (kl + (tid >> 3)) * 64 + (tid & 7) * 8);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const double2 v = __ldcs(src + j);
-                ra[2 * j] = v.x;
-                ra[2 * j + 1] = v.y;
-            }
+        for (int i = 0; i < (XBM * XBK) / XTHREADS; ++i) {
+            const int e = tid + i * XTHREADS;
+            const int r = e / XBK, k = e % XBK;  // row r of the tile, k along the reduction
+            const int p = m0 + r, kk = k0 + k;
+            const int Ip = p >> 6;
+            const double* src = Bq;
+            if (Ip <= J) src = Bq + ((int64_t)Ip * nt - (int64_t)Ip * (Ip - 1) / 2 + (J - Ip)) * 4096 + (p & 63) * 64 + (kk & 63);
+            else src = Bq + ((int64_t)J * nt - (int64_t)J * (J - 1) / 2 + (Ip - J)) * 4096 + (kk & 63) * 64 + (p & 63);
+            xcp8(as + r * XLD + k, src, Bq, p < npad);
         }
-        const double2* bsrc = reinterpret_cast<const double2*>(Ct + (int64_t)(n0 + (tid >> 1)) * ldc_t + k0 + (tid & 1) * 8);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const double2 v = __ldg(bsrc + j);
-            rb[2 * j] = v.x;
-            rb[2 * j + 1] = v.y;
+        for (int i = 0; i < (XBN * XBK) / XTHREADS; ++i) {
+            const int e = tid + i * XTHREADS;
+            const int r = e / XBK, k = e % XBK;
+            xcp8(bs + r * XLD + k, Ct + (int64_t)(n0 + r) * ldc_t + k0 + k, Ct, true);
         }
     };
-    auto store = [&](int buf, int k0) {
-        const int Jt = k0 >> 6;
-        if (Jt >= I) {
+
+    double acc[2][4][4];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) As[buf][(tid & 1) * 8 + j][tid >> 1] = ra[j];
-        } else {
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-            for (int j = 0; j < 8; ++j) As[buf][tid >> 3][(tid & 7) * 8 + j] = ra[j];
-        }
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) Bs[buf][(tid & 1) * 8 + j][tid >> 1] = rb[j];
-    };
-    double acc[4][4][2];
+            for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    int buf = 0;
-    load(0);
-    store(0, 0);
-    __syncthreads();
-    for (int k0 = 0; k0 < npad; k0 += BK) {
-        const bool more = k0 + BK < npad;
-        if (more) load(k0 + BK);
-#pragma unroll
-        for (int kk = 0; kk < BK; kk += 4) {
-            double af[4], bf[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) af[i] = As[buf][kk + t4][wm + i * 8 + g8];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) bf[j] = Bs[buf][kk + t4][wn + j * 8 + g8];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
-        }
-        if (more) store(buf ^ 1, k0 + BK);
-        __syncthreads();
-        buf ^= 1;
+    for (int s = 0; s < XST - 1; ++s) {
+        if (s < nk) load(s, s * XBK);
+        asm volatile("cp.async.commit_group;\n" ::);
     }
+    for (int it = 0; it < nk; ++it) {
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(XST - 2));
+        __syncthreads();
+        const int nxt = it + XST - 1;
+        if (nxt < nk) load(nxt % XST, nxt * XBK);
+        asm volatile("cp.async.commit_group;\n" ::);
+        const double* as = As + (it % XST) * XBM * XLD;
+        const double* bs = Bs + (it % XST) * XBN * XLD;
+#pragma unroll
+        for (int kk = 0; kk < XBK; kk += 8) {
+            double af[2][4], bf[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const double* r0 = as + (wm + i * 16 + gq) * XLD + kk + tq;
+                af[i][0] = r0[0];
+                af[i][1] = r0[8 * XLD];
+                af[i][2] = r0[4];
+                af[i][3] = r0[8 * XLD + 4];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double* c0 = bs + (wn + j * 8 + gq) * XLD + kk + tq;
+                bf[j][0] = c0[0];
+                bf[j][1] = c0[4];
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) xmma(acc[i][j], af[i], bf[j]);
+        }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
     double* xo = X + (int64_t)ql * opad;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int m = I * 64 + wm + i * 8 + g8;
-            const int nn = n0 + wn + j * 8 + 2 * t4;
-            *reinterpret_cast<double2*>(xo + (int64_t)m * ldx + nn) = make_double2(acc[i][j][0], acc[i][j][1]);
-        }
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int m = m0 + wm + i * 16 + gq + h * 8;
+                const int nn = n0 + wn + j * 8 + 2 * tq;
+                if (m < npad)
+                    *reinterpret_cast<double2*>(xo + (int64_t)m * ldx + nn) = make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
+            }
 }
 
 __global__ void k_scale_columns(const double* __restrict__ X, double* __restrict__ Xs, int64_t rows, int64_t ld,
@@ -262,8 +280,15 @@ cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int opad, con
     for (int q0 = 0; q0 < p.naux; q0 += qchunk) {
         const int qc = (p.naux - q0 < qchunk) ? p.naux - q0 : qchunk;
         const int64_t ldx = (int64_t)qc * opad;
-        dim3 grid(opad / 64, p.nt, qc);
-        k_exchange_half<<<grid, 128, 0, stream>>>(p.B, p.ldb, q0, p.nt, Ct, npad, (int)npad, X, ldx, opad);
+        static bool configured = false;
+        const int smem = XST * (XBM + XBN) * XLD * (int)sizeof(double);
+        if (!configured) {
+            cudaError_t e = cudaFuncSetAttribute(k_exchange_half, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess) return e;
+            configured = true;
+        }
+        dim3 grid(opad / 64, (unsigned)((npad + XBM - 1) / XBM), qc);
+        k_exchange_half<<<grid, XTHREADS, smem, stream>>>(p.B, p.ldb, q0, p.nt, Ct, npad, (int)npad, X, ldx, opad);
         const double* Xb = X;
         if (sign != nullptr) {
             const int64_t tot = npad * ldx;

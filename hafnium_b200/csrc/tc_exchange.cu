@@ -331,8 +331,8 @@ __global__ void k_symmetrize_upper128(const double* __restrict__ Kp, int64_t ldk
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n * n) return;
     const int64_t mu = e / n, nu = e % n;
-    const bool upper = (mu >> 7) <= (nu >> 7);
-    K[e] = upper ? Kp[mu * ldk + nu] : Kp[nu * ldk + mu];
+    // element-level mirror: K is exactly symmetric (every mu <= nu lies in a computed tile)
+    K[e] = mu <= nu ? Kp[mu * ldk + nu] : Kp[nu * ldk + mu];
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {

@@ -68,15 +68,16 @@ class PrecisionSchedule:
     the orbital gradient is above ``anchor_gradient``; then incremental builds
     anchored on an FP64 one, K(C_n) = K64(C_a) + [K16(C_n) - K16(C_a)], so the
     BF16 error scales with the change of the orbitals since the anchor, with a
-    new anchor each time the gradient falls by ``reanchor_factor``; once the
-    mixed iteration meets the convergence test, FP64 builds to the end, and the
-    test is only passed on two consecutive FP64 energies. DIIS, the eigensolves,
-    J and the energy are FP64 throughout.
+    new anchor each time the gradient falls by ``reanchor_factor``; below
+    ``fp64_gradient`` (or when the gradient stops falling) FP64 builds to the
+    end, and the convergence test is only passed on two consecutive FP64
+    energies. DIIS, the eigensolves, J and the energy are FP64 throughout.
     """
 
     mode: str = "fp64"
     anchor_gradient: float = 1e-2
     reanchor_factor: float = 1e-2
+    fp64_gradient: float = 1e-5
 
     def __post_init__(self) -> None:
         if self.mode not in ("fp64", "mixed"):
@@ -401,11 +402,13 @@ class _Rhf:
             change = energy - previous.energy if previous else math.inf
             history.append(Iteration(index, energy, change, gnorm, precision))
             converged = abs(change) < opts.energy_tolerance and gnorm < opts.gradient_tolerance
+            stalled = len(history) > 3 and precision != "fp64" and all(
+                h.precision != "fp64" for h in history[-4:]) and gnorm > 0.5 * history[-4].gradient_norm
             if precision == "fp64":
                 # the test counts only when both energies of the pair are FP64
                 if converged and (previous is None or previous.precision == "fp64" or not mixed):
                     return self.finish(f, history, True, t_start)
-            elif converged or (precision == "anchored" and gnorm < opts.gradient_tolerance):
+            elif converged or stalled or gnorm < self.schedule.fp64_gradient:
                 precision = "fp64"
             elif precision == "bf16" and gnorm < self.schedule.anchor_gradient:
                 precision = "anchored"
