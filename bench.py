@@ -56,6 +56,19 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def max_over_ranks(values, device=None):
+    """Element-wise max of per-rank step times across the process group (a no-op
+    without one): the whole-job time of replicas is the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
 
@@ -118,20 +131,49 @@ def measure_fp64_peak(torch, dev) -> float:
     return 2 * 8192 ** 3 / best / 1e12
 
 
-def one_scf(torch, mol, dev, host_io=False, mode="mixed"):
-    from hafnium_b200.scf import DeviceHamiltonian, PrecisionSchedule, ScfOptions, atomic_density_guess, solve_rhf
+def exchange_kernel_ms(torch, ham, result, repeats: int = 3) -> dict:
+    """Device time of one K build from the converged occupied orbitals, split-BF16
+    and FP64 (CUDA events on the launching stream, after one warm-up call)."""
+    from hafnium_b200 import _lib
+
+    n_occ = int(ham.n_alpha)
+    order = torch.argsort(result.mo_energies)[:n_occ]
+    c = result.mo_coefficients[:, order].contiguous()
+    out = {}
+    for name, prec, reps in (("bf16", _lib.PREC_BF16X3, repeats), ("fp64", _lib.PREC_FP64, 1)):
+        ham.two_body.exchange_factored(c, precision=prec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            ham.two_body.exchange_factored(c, precision=prec)
+        e1.record()
+        e1.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+    return out
+
+
+def one_scf(torch, mol, dev, host_io=False, mode="mixed", guess_kind="sad", probe_kernels=False):
+    from hafnium_b200.scf import (DeviceHamiltonian, PrecisionSchedule, ScfOptions, atomic_density_guess,
+                                  learned_density_guess, solve_rhf)
 
     ham = DeviceHamiltonian.build(mol, BASIS, AUX, device=dev.index or 0)
-    guess = atomic_density_guess(mol, BASIS, device=dev.index or 0)
+    if guess_kind == "learned":
+        guess = learned_density_guess(mol, ham, device=dev.index or 0)
+    else:
+        guess = atomic_density_guess(mol, BASIS, device=dev.index or 0)
     result = solve_rhf(ham, guess=guess, options=ScfOptions(), host_io=host_io,
                        schedule=PrecisionSchedule(mode=mode))
+    kernel_ms = None
+    if probe_kernels:
+        kernel_ms = exchange_kernel_ms(torch, ham, result)
     stats = ham.two_body.stats()
     out = {"energy": result.energy, "iterations": result.n_iterations, "converged": result.converged,
            "build": {k: ham.timings.get(k) for k in ("ms_metric", "ms_factor", "ms_three_center", "ms_fit",
                                                      "one_electron_s", "fitted_tensor_s")},
            "scf": result.timings, "launches": stats["kernel_launches"], "n_ao": ham.n_ao,
            "n_aux": ham.two_body.n_aux, "b_bytes": stats["b_bytes"],
-           "precisions": [h.precision for h in result.history]}
+           "precisions": [h.precision for h in result.history], "kernel_ms": kernel_ms}
     del ham, result
     torch.cuda.empty_cache()
     return out
@@ -150,8 +192,12 @@ def run_b200(args) -> None:
     from hafnium_b200.molecule import water_cluster
 
     mol = water_cluster(args.waters, args.seed + rank)
+    from hafnium_b200.learned.model import load_weights
+
+    weights = load_weights()
+    guess_kind = "learned" if weights is not None else "sad"
     for i in range(args.warmup):
-        one_scf(torch, mol, dev, mode="mixed")
+        one_scf(torch, mol, dev, mode="mixed", guess_kind=guess_kind)
         if i == 0:
             one_scf(torch, mol, dev, mode="fp64")
     if world > 1:
@@ -164,7 +210,7 @@ def run_b200(args) -> None:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(dev)
         e0.record()
-        info = one_scf(torch, mol, dev, mode=mode)
+        info = one_scf(torch, mol, dev, mode=mode, guess_kind=guess_kind if mode == "mixed" else "sad")
         e1.record()
         e1.synchronize()
         return e0.elapsed_time(e1) / 1e3, info
@@ -180,13 +226,11 @@ def run_b200(args) -> None:
         plain_details.append(info)
     torch.cuda.synchronize(dev)
     clocks = sampler.stop()
+    # kernel-only timing of the exchange builds for the roofline, outside the timed steps
+    probe = one_scf(torch, mol, dev, mode="mixed", guess_kind=guess_kind, probe_kernels=True)["kernel_ms"]
+    step_max, plain_max = max_over_ranks([max(times), max(plain_times)], dev)
     if world > 1:
-        t = torch.tensor([max(times), max(plain_times)], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-        step_max, plain_max = float(t[0].item()), float(t[1].item())
-    else:
-        step_max, plain_max = max(times), max(plain_times)
     e2e = None
     if not args.no_e2e:
         torch.cuda.synchronize(dev)
@@ -211,8 +255,10 @@ def run_b200(args) -> None:
     j_ms = plain["scf"]["coulomb_ms"] / fock_builds
     k_flops = 4.0 * naux * n * n * o
     j_bytes = 2.0 * last["b_bytes"]
-    k16_builds = last["scf"].get("exchange_builds_bf16", 0)
-    k16_ms = last["scf"]["exchange_ms_bf16"] / k16_builds if k16_builds else None
+    k16_ms = probe["bf16"]
+    k64_probe_ms = probe["fp64"]
+    inc_builds = last["scf"].get("exchange_builds_incremental", 0)
+    inc_ms = last["scf"]["exchange_ms_incremental"] / inc_builds if inc_builds else None
     fp64_peak = measure_fp64_peak(torch, dev)
     peaks = {}
     try:
@@ -227,7 +273,8 @@ def run_b200(args) -> None:
     if k16_ms:
         executed = 3.0 * k_flops  # three BF16 products per FP64-equivalent product
         k16_exec_tflops = executed / (k16_ms / 1e3) / 1e12
-        roofline = {"bound": "tensor", "kernel": "split-BF16 exchange on tcgen05 (k_tc_split3, both stages)",
+        roofline = {"bound": "tensor", "kernel": "split-BF16 exchange on tcgen05 (k_tc_split3, both stages), "
+                              "one K build from the converged occupied orbitals",
                     "achieved": k16_exec_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
                     "frac": k16_exec_tflops / bf16_peak, "traffic": None,
                     "algorithmic": "3 x 4 naux n^2 nocc BF16 flops per K build (the three split products)",
@@ -249,9 +296,12 @@ def run_b200(args) -> None:
         "dtype": "f64",
         "data": "synthetic: seeded rigid-water clusters (no dataset)",
         "config": {"workload": f"DF-RHF (H2O){args.waters} seed {args.seed}, cc-pVDZ/def2-universal-jkfit "
-                               f"(n={n}, naux={naux}, nocc={o}), SAD guess, mixed split-BF16/FP64 exchange",
+                               f"(n={n}, naux={naux}, nocc={o}), {guess_kind} guess, mixed split-BF16/FP64 "
+                               f"exchange; compared with plain FP64 from the SAD guess",
                    "waters": args.waters, "basis": BASIS, "auxiliary": AUX, "precision_path": "mixed",
-                   "guess": "SAD (the learned guess is not built yet)",
+                   "guess": guess_kind if weights is None else
+                   f"learned (weights sha256 {weights[2].get('sha256', '')[:12]}, trained on "
+                   f"{weights[2].get('clusters')} clusters); SAD fallback",
                    "l2": "inputs larger than L2 (B tensor %.1f GB)" % (last["b_bytes"] / 1e9),
                    "parallelism": f"replicas x{world}"},
         "energy": last["energy"],
@@ -263,7 +313,9 @@ def run_b200(args) -> None:
                        "iterations": plain["iterations"], "speedup_of_mixed": plain_max / step_max,
                        "dE_mixed_vs_fp64": last["energy"] - plain["energy"]},
         "stages": {"build": last["build"], "per_build_ms": {"coulomb": j_ms, "exchange_fp64": k64_ms,
-                                                             "exchange_bf16": k16_ms},
+                                                             "exchange_bf16_kernel": k16_ms,
+                                                             "exchange_fp64_kernel": k64_probe_ms,
+                                                             "exchange_incremental": inc_ms},
                    "mixed_scf": last["scf"], "plain_scf": plain["scf"]},
         "roofline": roofline,
         "roofline_exchange_fp64": {"bound": "tensor", "achieved": k64_tflops, "peak": fp64_peak, "unit": "TFLOP/s",

@@ -27,6 +27,25 @@ EXPORTS = (
     "hf_coulomb_static",
 )
 
+BATCH_EXPORTS = (
+    "hf_batch_default_options", "hf_batch_create", "hf_batch_destroy", "hf_batch_last_error", "hf_batch_set_stream",
+    "hf_batch_dims", "hf_batch_load", "hf_batch_run", "hf_batch_run_group", "hf_batch_results", "hf_batch_coulomb",
+    "hf_batch_exchange", "hf_dgemm_nt",
+)
+
+
+class BatchOptionsC(ctypes.Structure):
+    _fields_ = [
+        ("max_iterations", ctypes.c_int),
+        ("diis_size", ctypes.c_int),
+        ("energy_tolerance", ctypes.c_double),
+        ("gradient_tolerance", ctypes.c_double),
+        ("purify_steps", ctypes.c_int),
+        ("purify_tolerance", ctypes.c_double),
+        ("gemm_tile", ctypes.c_int),
+        ("use_graph", ctypes.c_int),
+    ]
+
 
 class ShellTableC(ctypes.Structure):
     _fields_ = [
@@ -99,8 +118,23 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_four_center.argtypes = [v, v, i]
     lib.hf_coulomb_static.argtypes = [v, v, v]
     lib.hf_get_stats.argtypes = [v, p(StatsC)]
-    for name in EXPORTS:
-        getattr(lib, name).restype = ctypes.c_int if name != "hf_last_error" else ctypes.c_char_p
+    d = ctypes.c_double
+    lib.hf_batch_default_options.argtypes = [p(BatchOptionsC)]
+    lib.hf_batch_create.argtypes = [p(v), i, i64, p(v)]
+    lib.hf_batch_destroy.argtypes = [v]
+    lib.hf_batch_last_error.argtypes = [v]
+    lib.hf_batch_set_stream.argtypes = [v, v]
+    lib.hf_batch_dims.argtypes = [v, p(i), p(i64), p(i64), p(i64)]
+    lib.hf_batch_load.argtypes = [v, v, v, v, v, i64]
+    lib.hf_batch_run.argtypes = [v, p(BatchOptionsC)]
+    lib.hf_batch_run_group.argtypes = [p(v), i, p(BatchOptionsC)]
+    lib.hf_batch_results.argtypes = [v, v, v, v, v]
+    lib.hf_batch_coulomb.argtypes = [v, v, d, v]
+    lib.hf_batch_exchange.argtypes = [v, v, i64, v]
+    lib.hf_dgemm_nt.argtypes = [i64, i64, i64, v, i64, i64, v, i64, i64, v, i64, i64, d, d, i, i, v]
+    for name in EXPORTS + BATCH_EXPORTS:
+        text = name in ("hf_last_error", "hf_batch_last_error")
+        getattr(lib, name).restype = ctypes.c_char_p if text else ctypes.c_int
     _lib = lib
     return lib
 

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/hfjk.h"
+#include "context.cuh"
 #include "dgemm.cuh"
 #include "integrals.cuh"
 #include "jk.cuh"
@@ -179,114 +180,6 @@ __global__ void k_factor_transpose(const double* __restrict__ C, int64_t n, int6
     if (mu == 0) sign[i] = s;
 }
 
-// Pivoted Cholesky of a symmetric PSD n x n matrix D in one CTA: rows of Lc
-// ([rank][n]) with D ~= Lc^T Lc, stopping when the largest remaining diagonal
-// entry falls to tol times the largest initial one. status: 0 ok, 1 indefinite.
-__global__ void __launch_bounds__(1024) k_pivoted_cholesky(const double* __restrict__ D, int n, double tol, int maxr,
-                                                           double* __restrict__ Lc, int* __restrict__ out) {
-    extern __shared__ double sm[];
-    double* d = sm;                                      // n
-    unsigned char* used = (unsigned char*)(sm + n);      // n
-    __shared__ double rv[32];
-    __shared__ int ri[32];
-    __shared__ double s_dmax0, s_piv;
-    __shared__ int s_p, s_stop;
-    const int tid = threadIdx.x;
-    for (int i = tid; i < n; i += blockDim.x) {
-        d[i] = D[(int64_t)i * n + i];
-        used[i] = 0;
-    }
-    __syncthreads();
-    // largest |diagonal|
-    double m = 0.0;
-    for (int i = tid; i < n; i += blockDim.x) m = fmax(m, fabs(d[i]));
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((tid & 31) == 0) rv[tid >> 5] = m;
-    __syncthreads();
-    if (tid == 0) {
-        double v = 0.0;
-        for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) v = fmax(v, rv[w]);
-        s_dmax0 = v;
-    }
-    __syncthreads();
-    int k = 0;
-    for (; k < maxr; ++k) {
-        double best = -1.0;
-        int bi = -1;
-        for (int i = tid; i < n; i += blockDim.x)
-            if (!used[i] && d[i] > best) {
-                best = d[i];
-                bi = i;
-            }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) {
-                best = ob;
-                bi = oi;
-            }
-        }
-        if ((tid & 31) == 0) {
-            rv[tid >> 5] = best;
-            ri[tid >> 5] = bi;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double b = -1.0;
-            int p = -1;
-            for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w)
-                if (rv[w] > b || (rv[w] == b && ri[w] >= 0 && (p < 0 || ri[w] < p))) {
-                    b = rv[w];
-                    p = ri[w];
-                }
-            s_stop = (p < 0 || !(b > tol * s_dmax0)) ? 1 : 0;
-            s_p = p;
-            s_piv = s_stop ? 0.0 : sqrt(b);
-        }
-        __syncthreads();
-        if (s_stop) break;
-        const int p = s_p;
-        const double piv = s_piv;
-        for (int i = tid; i < n; i += blockDim.x) {
-            double l = 0.0;
-            if (i == p) l = piv;
-            else if (!used[i]) {
-                double s = D[(int64_t)p * n + i];
-                for (int j = 0; j < k; ++j) s -= Lc[(int64_t)j * n + i] * Lc[(int64_t)j * n + p];
-                l = s / piv;
-            }
-            Lc[(int64_t)k * n + i] = l;
-        }
-        __syncthreads();
-        for (int i = tid; i < n; i += blockDim.x) {
-            if (i == p) used[i] = 1;
-            else if (!used[i]) {
-                const double l = Lc[(int64_t)k * n + i];
-                d[i] -= l * l;
-            }
-        }
-        __syncthreads();
-    }
-    // indefinite if a remaining diagonal entry is clearly negative
-    int bad = 0;
-    for (int i = tid; i < n; i += blockDim.x)
-        if (!used[i] && d[i] < -1e3 * tol * s_dmax0) bad = 1;
-    bad = __syncthreads_or(bad);
-    if (tid == 0) {
-        out[0] = k;
-        out[1] = bad;
-    }
-}
-
-__global__ void k_factor_pad(const double* __restrict__ Lc, int64_t n, int64_t rank, double* __restrict__ Ct,
-                             int64_t npad, int64_t opad, double* __restrict__ sign) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= opad * npad) return;
-    const int64_t i = e / npad, mu = e % npad;
-    Ct[e] = (i < rank && mu < n) ? Lc[i * n + mu] : 0.0;
-    if (mu == 0) sign[i] = 1.0;
-}
-
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 // Carves 256-byte aligned sub-buffers out of one allocation.
@@ -317,6 +210,20 @@ int check_async(hf_ctx* ctx, const char* what) {
 }
 
 }  // namespace
+
+namespace hf {
+int context_view(const hf_ctx* ctx, TensorView* out) {
+    if (!ctx || !out) return HF_ERR_ARG;
+    out->device = ctx->device;
+    out->B = ctx->d_B;
+    out->n = ctx->n;
+    out->nt = ctx->nt;
+    out->ntiles = ctx->ntiles;
+    out->naux = ctx->naux;
+    out->built = ctx->built;
+    return HF_OK;
+}
+}  // namespace hf
 
 extern "C" {
 
@@ -620,7 +527,8 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     }
     {
         std::vector<double> diag(N);
-        for (int i = 0; i < N; ++i) HF_CU(cudaMemcpy(&diag[i], ctx->d_metric + (size_t)i * N + i, 8, cudaMemcpyDeviceToHost));
+        HF_CU(cudaMemcpy2D(diag.data(), sizeof(double), ctx->d_metric, sizeof(double) * ((size_t)N + 1), sizeof(double),
+                           N, cudaMemcpyDeviceToHost));
         const double dmax = *std::max_element(diag.begin(), diag.end());
         ctx->stats.min_pivot_ratio = pivmin * pivmin / dmax;
     }
@@ -641,6 +549,7 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     ctx->stats.b_bytes = (int64_t)sizeof(double) * N * ldb;
     const size_t row_bytes = sizeof(double) * 4096 * (size_t)N * ctx->nt;  // the widest row
     size_t budget = std::max<size_t>(row_bytes, (size_t)4 << 30);
+    budget = std::min<size_t>(budget, sizeof(double) * 4096 * (size_t)N * ctx->ntiles);
     size_t freeb = 0, totalb = 0;
     cudaMemGetInfo(&freeb, &totalb);
     if (budget > freeb / 2) budget = std::max(row_bytes, freeb / 2);
@@ -878,11 +787,8 @@ int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_d
         dD = sD;
     }
     time_begin(ctx);
-    const size_t smem = sizeof(double) * n + n + 16;
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_pivoted_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaMemsetAsync(ctx->d_info, 0, 2 * sizeof(int), ctx->stream);
-    k_pivoted_cholesky<<<1, 1024, smem, ctx->stream>>>(dD, (int)n, 1e-14, (int)n, Lc, ctx->d_info);
+    HF_CU(pivoted_cholesky(dD, 0, (int)n, 1e-14, (int)n, Lc, 0, ctx->d_info, 1, nullptr, ctx->stream));
     int res[2] = {0, 0};
     cudaMemcpyAsync(res, ctx->d_info, sizeof(res), cudaMemcpyDeviceToHost, ctx->stream);
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
@@ -897,10 +803,11 @@ int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_d
         double* Ct_tc = nullptr;
         if (alloc(ctx, (void**)&Ct_tc, sizeof(double) * ((size_t)t.opad * t.npad + t.opad))) return HF_ERR_OOM;
         time_begin(ctx);
-        k_factor_pad<<<(unsigned)((t.opad * t.npad + 255) / 256), 256, 0, ctx->stream>>>(
-            Lc, n, rank, Ct_tc, t.npad, t.opad, Ct_tc + (size_t)t.opad * t.npad);
+        const cudaError_t fe = factor_pad(Lc, 0, n, ctx->d_info, Ct_tc, 0, t.npad, t.opad,
+                                          Ct_tc + (size_t)t.opad * t.npad, 1, nullptr, ctx->stream);
         double* dK = on_device ? K : sK;
-        int s = exchange_bf16(ctx, t, Ct_tc, dK);
+        int s = fe == cudaSuccess ? exchange_bf16(ctx, t, Ct_tc, dK)
+                                  : fail(ctx, HF_ERR_CUDA, std::string("factor_pad: ") + cudaGetErrorString(fe));
         if (s == HF_OK && !on_device) cudaMemcpyAsync(K, sK, sizeof(double) * nn, cudaMemcpyDeviceToHost, ctx->stream);
         ctx->stats.ms_exchange = time_end(ctx);
         ctx->stats.exchange_rank = rank;
@@ -912,7 +819,7 @@ int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_d
     double* Ct = buf + oCt;
     double* sign = buf + osg;
     time_begin(ctx);
-    k_factor_pad<<<(unsigned)((opad * npad + 255) / 256), 256, 0, ctx->stream>>>(Lc, n, rank, Ct, npad, opad, sign);
+    HF_CU(factor_pad(Lc, 0, n, ctx->d_info, Ct, 0, npad, opad, sign, 1, nullptr, ctx->stream));
     double* dK = on_device ? K : sK;
     int s = exchange_from_ct(ctx, Ct, (int)opad, sign, false, dK, precision);
     if (s == HF_OK && !on_device) cudaMemcpyAsync(K, sK, sizeof(double) * nn, cudaMemcpyDeviceToHost, ctx->stream);

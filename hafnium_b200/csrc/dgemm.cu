@@ -1,16 +1,18 @@
 // FP64 DMMA GEMM (see dgemm.cuh for the contract).
 //
-// 128 x 64 CTA tiles, 8 warps of 32 x 32, mma.sync.m16n8k8 (FP64 tensor cores),
-// a 3-stage cp.async pipeline from global memory into shared tiles stored
-// row-major with a 20-double row pitch (conflict-free fragment loads), BK = 16.
-// Operands are K-contiguous rows (A[m][k], B[n][k]); copies are 8 bytes so any
-// row stride and offset is legal, and out-of-range elements are zero-filled.
+// Warps of 32 x 32 output (2 x 4 mma.sync.m16n8k8 FP64 tiles), a 3-stage
+// cp.async pipeline from global memory into shared tiles stored row-major with
+// a 20-double row pitch (conflict-free fragment loads), BK = 16. Operands are
+// K-contiguous rows (A[m][k], B[n][k]); copies are 8 bytes so any row stride and
+// offset is legal, and out-of-range elements are zero-filled.
+#include <mutex>
+
 #include "dgemm.cuh"
 
 namespace hf {
 
 namespace {
-constexpr int BM = 128, BN = 64, BK = 16, LD = BK + 4, STAGES = 3, THREADS = 256;
+constexpr int BK = 16, LD = BK + 4, STAGES = 3;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -31,13 +33,31 @@ __device__ __forceinline__ void mma16x8x8(double (&c)[4], const double (&a)[4], 
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-__global__ void __launch_bounds__(THREADS, 2) k_dgemm_nt(GemmArgs g) {
+template <int BM, int BN>
+__host__ __device__ constexpr int threads_of() {
+    return (BM / 32) * (BN / 32) * 32;
+}
+
+template <int BM, int BN>
+__host__ __device__ constexpr int smem_of() {
+    return STAGES * (BM + BN) * LD * (int)sizeof(double);
+}
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN>()) < 1 ? 1 : 512 / threads_of<BM, BN>())
+    k_dgemm_nt(GemmArgs g) {
+    constexpr int THREADS = threads_of<BM, BN>();
+    constexpr int WARPS_N = BN / 32;
+    const int z = blockIdx.z;
+    if (g.active && g.active[z] == 0) return;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     if (g.epi == 2 && n0 > m0 + BM - 1) return;
     if (g.epi == 3 && m0 > n0 + BN - 1) return;
-    const double* A = g.A + (int64_t)blockIdx.z * g.strideA;
-    const double* B = g.B + (int64_t)blockIdx.z * g.strideB;
-    double* C = g.C + (int64_t)blockIdx.z * g.strideC;
+    const double alpha = g.alpha_v ? g.alpha_v[z] : g.alpha;
+    const double beta = g.beta_v ? g.beta_v[z] : g.beta;
+    const double* A = g.A + (int64_t)z * g.strideA;
+    const double* B = g.B + (int64_t)z * g.strideB;
+    double* C = g.C + (int64_t)z * g.strideC;
     int kb = 0, ke = g.K;
     if (g.kmode == 1) kb = n0;
     if (g.kmode == 2) ke = min(g.K, m0 + BM);
@@ -45,11 +65,11 @@ __global__ void __launch_bounds__(THREADS, 2) k_dgemm_nt(GemmArgs g) {
     const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
 
     extern __shared__ double smem[];
-    double* As = smem;                          // [STAGES][BM][LD]
-    double* Bs = smem + STAGES * BM * LD;       // [STAGES][BN][LD]
+    double* As = smem;                     // [STAGES][BM][LD]
+    double* Bs = smem + STAGES * BM * LD;  // [STAGES][BN][LD]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int gq = lane >> 2, tq = lane & 3;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int wm = (warp / WARPS_N) * 32, wn = (warp % WARPS_N) * 32;
 
     auto load = [&](int stage, int k0) {
         double* as = As + stage * BM * LD;
@@ -126,24 +146,57 @@ __global__ void __launch_bounds__(THREADS, 2) k_dgemm_nt(GemmArgs g) {
                 const int n = n0 + wn + j * 8 + 2 * tq + (v & 1);
                 if (m >= g.M || n >= g.N) continue;
                 double* dst = (g.epi == 1) ? &C[(int64_t)n * g.ldc + m] : &C[(int64_t)m * g.ldc + n];
-                const double val = g.alpha * acc[i][j][v];
-                *dst = (g.beta == 0.0) ? val : val + g.beta * *dst;
+                const double val = alpha * acc[i][j][v];
+                *dst = (beta == 0.0) ? val : val + beta * *dst;
             }
 }
+
+template <int BM, int BN>
+cudaError_t configure_one() {
+    return cudaFuncSetAttribute(k_dgemm_nt<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_of<BM, BN>());
+}
+
+template <int BM, int BN>
+cudaError_t launch(const GemmArgs& g, int batch, cudaStream_t stream) {
+    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, batch);
+    k_dgemm_nt<BM, BN><<<grid, threads_of<BM, BN>(), smem_of<BM, BN>(), stream>>>(g);
+    return cudaGetLastError();
+}
+
+constexpr int kMaxDevices = 64;
+std::mutex g_config_mutex;
+bool g_configured[kMaxDevices] = {};
 }  // namespace
+
+cudaError_t dgemm_configure() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_config_mutex);
+    if (g_configured[dev]) return cudaSuccess;
+    if ((e = configure_one<128, 64>()) != cudaSuccess) return e;
+    if ((e = configure_one<64, 64>()) != cudaSuccess) return e;
+    if ((e = configure_one<64, 32>()) != cudaSuccess) return e;
+    if ((e = configure_one<32, 32>()) != cudaSuccess) return e;
+    if ((e = configure_one<128, 128>()) != cudaSuccess) return e;
+    g_configured[dev] = true;
+    return cudaSuccess;
+}
 
 cudaError_t dgemm_nt(const GemmArgs& g, int batch, cudaStream_t stream) {
     if (g.M <= 0 || g.N <= 0 || batch <= 0) return cudaSuccess;
-    static bool configured = false;
-    const int smem = STAGES * (BM + BN) * LD * (int)sizeof(double);
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_dgemm_nt, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
+    if (batch > 65535) return cudaErrorInvalidValue;
+    cudaError_t e = dgemm_configure();
+    if (e != cudaSuccess) return e;
+    switch (g.tile) {
+        case 0: return launch<128, 64>(g, batch, stream);
+        case 1: return launch<64, 64>(g, batch, stream);
+        case 2: return launch<64, 32>(g, batch, stream);
+        case 3: return launch<32, 32>(g, batch, stream);
+        case 4: return launch<128, 128>(g, batch, stream);
+        default: return cudaErrorInvalidValue;
     }
-    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, batch);
-    k_dgemm_nt<<<grid, THREADS, smem, stream>>>(g);
-    return cudaGetLastError();
 }
 
 }  // namespace hf

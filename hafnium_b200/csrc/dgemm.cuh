@@ -1,19 +1,22 @@
 // FP64 tensor-core GEMM for sm_100a: C = alpha * A * Bop^T + beta * C.
 //
 // Both operands are K-contiguous ("NT"): A[m][k] with row stride lda, Bop[n][k]
-// with row stride ldb. 64x64x16 CTA tiles, 4 warps of 32x32, DMMA
-// mma.sync.m8n8k4.f64 (the FP64 tensor path; tcgen05 has no FP64 kind).
-// Global tiles are staged through registers into shared memory stored
-// k-major ([k][m], padded so a fragment load touches every bank once per
-// half-warp), double-buffered across k-steps.
+// with row stride ldb. DMMA mma.sync.m16n8k8.f64 (the FP64 tensor path;
+// tcgen05 has no FP64 kind), warps of 32x32 output, a 3-stage cp.async pipeline
+// of BK = 16 slices. The CTA tile is one of kTileShapes (selected by `tile`):
+// an autotuner picks the shape per problem size.
 //
 // kmode restricts the k range per output tile (triangular operands):
 //   0: [0, K)   1: [n0, K) (Bop upper: Bop[n][k] = 0 for k < n)
-//   2: [0, min(K, m0 + 64)) (A lower: A[m][k] = 0 for k > m)
+//   2: [0, min(K, m0 + BM)) (A lower: A[m][k] = 0 for k > m)
 // epi selects the store:
 //   0: C[m][n] (row stride ldc)      1: C[n][m] (transposed store)
-//   2: as 0, only tiles touching the lower triangle (n0 <= m0 + 63)
-//   3: as 0, only tiles touching the upper triangle (m0 <= n0 + 63)
+//   2: as 0, only tiles touching the lower triangle (n0 <= m0 + BM - 1)
+//   3: as 0, only tiles touching the upper triangle (m0 <= n0 + BN - 1)
+//
+// Batching runs over blockIdx.z with per-batch pointer strides. Optional
+// per-batch arrays: `active` (a batch whose entry is 0 is skipped and its C is
+// left untouched), `alpha_v` / `beta_v` (replace alpha / beta for that batch).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -32,14 +35,20 @@ struct GemmArgs {
     int kmode, epi;
     // Optional batching over blockIdx.z: pointer strides per batch.
     int64_t strideA, strideB, strideC;
+    const int* active;
+    const double* alpha_v;
+    const double* beta_v;
+    int tile;  // index into kTileShapes
 };
+
+// CTA tile shapes (BM x BN); warps = (BM / 32) * (BN / 32).
+constexpr int kTileCount = 5;
+constexpr int kTileShapes[kTileCount][2] = {{128, 64}, {64, 64}, {64, 32}, {32, 32}, {128, 128}};
 
 cudaError_t dgemm_nt(const GemmArgs& g, int batch, cudaStream_t stream);
 
-__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
+// Sets the shared-memory attributes of every tile instance on the current
+// device (done lazily by dgemm_nt; call it before a stream capture).
+cudaError_t dgemm_configure();
 
 }  // namespace hf

@@ -12,6 +12,7 @@
 //       B_q (transposed for tiles below the diagonal); the second product is a
 //       GEMM over the q-chunk, only upper 64x64 output tiles computed.
 #include <cmath>
+#include <mutex>
 
 #include "dgemm.cuh"
 #include "jk.cuh"
@@ -20,8 +21,17 @@ namespace hf {
 
 namespace {
 
-// Dw[t][r][c] = w_t D[64I + r][64J + c], zero outside n.
-__global__ void k_pack_density(const double* __restrict__ D, int64_t n, int nt, double* __restrict__ Dw) {
+__device__ __forceinline__ const double* cluster_tensor(const double* const* Btab, const double* B, int c) {
+    return Btab ? Btab[c] : B;
+}
+
+// Dw[t][r][c] = scale w_t D[64I + r][64J + c], zero outside n; cluster blockIdx.y.
+__global__ void k_pack_density(const double* __restrict__ D, int64_t strideD, double scale, int64_t n, int nt,
+                               double* __restrict__ Dw, int64_t strideW, const int* __restrict__ active) {
+    const int cl = blockIdx.y;
+    if (active && active[cl] == 0) return;
+    D += cl * strideD;
+    Dw += cl * strideW;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t ntiles = (int64_t)nt * (nt + 1) / 2;
     if (e >= ntiles * 4096) return;
@@ -37,14 +47,20 @@ __global__ void k_pack_density(const double* __restrict__ D, int64_t n, int nt, 
     const int J = I + (int)(t - base);
     const int64_t mu = 64 * (int64_t)I + r, nu = 64 * (int64_t)J + c;
     double v = 0.0;
-    if (mu < n && nu < n) v = (I == J ? 1.0 : 2.0) * D[mu * n + nu];
+    if (mu < n && nu < n) v = (I == J ? scale : 2.0 * scale) * D[mu * n + nu];
     Dw[e] = v;
 }
 
-// c[q] = sum_e B[q][e] Dw[e]; one CTA per q, 128-bit loads.
-__global__ void __launch_bounds__(512) k_coulomb_charges(const double* __restrict__ B, int64_t ldb, int64_t nelem,
-                                                         const double* __restrict__ Dw, double* __restrict__ c) {
-    const int q = blockIdx.x;
+// c[q] = sum_e B[q][e] Dw[e]; one CTA per (q, cluster), 128-bit loads.
+__global__ void __launch_bounds__(512) k_coulomb_charges(const double* const* __restrict__ Btab,
+                                                         const double* __restrict__ B, int64_t ldb, int64_t nelem,
+                                                         const double* __restrict__ Dw, double* __restrict__ c,
+                                                         int64_t strideW, const int* __restrict__ active) {
+    const int q = blockIdx.x, cl = blockIdx.y;
+    if (active && active[cl] == 0) return;
+    B = cluster_tensor(Btab, B, cl);
+    Dw += cl * strideW;
+    c += cl * strideW;
     const double2* row = reinterpret_cast<const double2*>(B + (int64_t)q * ldb);
     const double2* d = reinterpret_cast<const double2*>(Dw);
     const int64_t n2 = nelem / 2;
@@ -77,9 +93,16 @@ __global__ void __launch_bounds__(512) k_coulomb_charges(const double* __restric
 
 // Jt[e] += sum_{q in slab} c[q] B[q][e]; each thread owns two adjacent elements.
 constexpr int kJSlab = 256;
-__global__ void __launch_bounds__(256) k_coulomb_assemble(const double* __restrict__ B, int64_t ldb, int64_t nelem,
+__global__ void __launch_bounds__(256) k_coulomb_assemble(const double* const* __restrict__ Btab,
+                                                          const double* __restrict__ B, int64_t ldb, int64_t nelem,
                                                           int naux, const double* __restrict__ c,
-                                                          double* __restrict__ Jt) {
+                                                          double* __restrict__ Jt, int64_t strideW,
+                                                          const int* __restrict__ active) {
+    const int cl = blockIdx.z;
+    if (active && active[cl] == 0) return;
+    B = cluster_tensor(Btab, B, cl);
+    c += cl * strideW;
+    Jt += cl * strideW;
     const int64_t e2 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (2 * e2 >= nelem) return;
     const int q0 = blockIdx.y * kJSlab;
@@ -106,7 +129,12 @@ __global__ void __launch_bounds__(256) k_coulomb_assemble(const double* __restri
 }
 
 // Full symmetric matrix from upper 64x64 tiles: J[mu][nu] = tiles(min, max).
-__global__ void k_unpack_tiles(const double* __restrict__ Jt, int64_t n, int nt, double* __restrict__ J) {
+__global__ void k_unpack_tiles(const double* __restrict__ Jt, int64_t strideW, int64_t n, int nt,
+                               double* __restrict__ J, int64_t strideJ, const int* __restrict__ active) {
+    const int cl = blockIdx.y;
+    if (active && active[cl] == 0) return;
+    Jt += cl * strideW;
+    J += cl * strideJ;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n * n) return;
     int64_t mu = e / n, nu = e % n;
@@ -124,7 +152,12 @@ __global__ void k_unpack_tiles(const double* __restrict__ Jt, int64_t n, int nt,
 }
 
 // K[mu][nu] from the upper-tile-valid padded matrix Kp (row stride ldk).
-__global__ void k_symmetrize_upper(const double* __restrict__ Kp, int64_t ldk, int64_t n, double* __restrict__ K) {
+__global__ void k_symmetrize_upper(const double* __restrict__ Kp, int64_t ldk, int64_t n, double* __restrict__ K,
+                                   int64_t strideK, const int* __restrict__ active) {
+    const int cl = blockIdx.y;
+    if (active && active[cl] == 0) return;
+    Kp += cl * ldk * ldk;
+    K += cl * strideK;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n * n) return;
     const int64_t mu = e / n, nu = e % n;
@@ -151,11 +184,20 @@ __device__ __forceinline__ void xmma(double (&c)[4], const double (&a)[4], const
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-__global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* __restrict__ B, int64_t ldb, int q0, int nt,
-                                                             const double* __restrict__ Ct, int64_t ldc_t, int npad,
-                                                             double* __restrict__ X, int64_t ldx, int opad) {
-    const int m0 = blockIdx.y * XBM, n0 = blockIdx.x * XBN;
+__global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* const* __restrict__ Btab,
+                                                             const double* __restrict__ B, int64_t ldb, int q0, int nt,
+                                                             const double* __restrict__ Ct, int64_t ldc_t,
+                                                             int64_t strideCt, int npad, double* __restrict__ X,
+                                                             int64_t ldx, int64_t strideX, int opad,
+                                                             const int* __restrict__ active) {
+    const int row_tiles = (npad + XBM - 1) / XBM;
+    const int cl = blockIdx.y / row_tiles;
+    if (active && active[cl] == 0) return;
+    const int m0 = (blockIdx.y % row_tiles) * XBM, n0 = blockIdx.x * XBN;
     const int ql = blockIdx.z;
+    B = cluster_tensor(Btab, B, cl);
+    Ct += cl * strideCt;
+    X += cl * strideX;
     const double* Bq = B + (int64_t)(q0 + ql) * ldb;
     extern __shared__ double xs[];
     double* As = xs;
@@ -246,6 +288,133 @@ __global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* __r
             }
 }
 
+// Pivoted Cholesky of a symmetric PSD n x n matrix D in one CTA per cluster:
+// rows of Lc ([rank][n]) with D ~= Lc^T Lc, stopping after maxr rows or when the
+// largest remaining diagonal entry falls to tol times the largest initial one.
+// out = {rank, indefinite}.
+__global__ void __launch_bounds__(1024) k_pivoted_cholesky(const double* __restrict__ D, int64_t strideD, int n,
+                                                           double tol, int maxr, double* __restrict__ Lc,
+                                                           int64_t strideL, int* __restrict__ out,
+                                                           const int* __restrict__ active) {
+    const int cl = blockIdx.x;
+    if (active && active[cl] == 0) return;
+    D += cl * strideD;
+    Lc += cl * strideL;
+    out += 2 * cl;
+    extern __shared__ double sm[];
+    double* d = sm;                                  // n
+    unsigned char* used = (unsigned char*)(sm + n);  // n
+    __shared__ double rv[32];
+    __shared__ int ri[32];
+    __shared__ double s_dmax0, s_piv;
+    __shared__ int s_p, s_stop;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n; i += blockDim.x) {
+        d[i] = D[(int64_t)i * n + i];
+        used[i] = 0;
+    }
+    __syncthreads();
+    // largest |diagonal|
+    double m = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) m = fmax(m, fabs(d[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((tid & 31) == 0) rv[tid >> 5] = m;
+    __syncthreads();
+    if (tid == 0) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) v = fmax(v, rv[w]);
+        s_dmax0 = v;
+    }
+    __syncthreads();
+    int k = 0;
+    for (; k < maxr; ++k) {
+        double best = -1.0;
+        int bi = -1;
+        for (int i = tid; i < n; i += blockDim.x)
+            if (!used[i] && d[i] > best) {
+                best = d[i];
+                bi = i;
+            }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) {
+                best = ob;
+                bi = oi;
+            }
+        }
+        if ((tid & 31) == 0) {
+            rv[tid >> 5] = best;
+            ri[tid >> 5] = bi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double b = -1.0;
+            int p = -1;
+            for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w)
+                if (rv[w] > b || (rv[w] == b && ri[w] >= 0 && (p < 0 || ri[w] < p))) {
+                    b = rv[w];
+                    p = ri[w];
+                }
+            s_stop = (p < 0 || !(b > tol * s_dmax0)) ? 1 : 0;
+            s_p = p;
+            s_piv = s_stop ? 0.0 : sqrt(b);
+        }
+        __syncthreads();
+        if (s_stop) break;
+        const int p = s_p;
+        const double piv = s_piv;
+        for (int i = tid; i < n; i += blockDim.x) {
+            double l = 0.0;
+            if (i == p) l = piv;
+            else if (!used[i]) {
+                double s = D[(int64_t)p * n + i];
+                for (int j = 0; j < k; ++j) s -= Lc[(int64_t)j * n + i] * Lc[(int64_t)j * n + p];
+                l = s / piv;
+            }
+            Lc[(int64_t)k * n + i] = l;
+        }
+        __syncthreads();
+        for (int i = tid; i < n; i += blockDim.x) {
+            if (i == p) used[i] = 1;
+            else if (!used[i]) {
+                const double l = Lc[(int64_t)k * n + i];
+                d[i] -= l * l;
+            }
+        }
+        __syncthreads();
+    }
+    // indefinite if a remaining diagonal entry is clearly negative
+    int bad = 0;
+    for (int i = tid; i < n; i += blockDim.x)
+        if (!used[i] && d[i] < -1e3 * tol * s_dmax0) bad = 1;
+    bad = __syncthreads_or(bad);
+    if (tid == 0) {
+        out[0] = k;
+        out[1] = bad;
+    }
+}
+
+// Ct[i][mu] = Lc[i][mu] for i < rank and mu < n (rank = info[2 c]), else 0;
+// sign[i] = 1 when sign is given (single cluster).
+__global__ void k_factor_pad(const double* __restrict__ Lc, int64_t strideL, int64_t n, const int* __restrict__ info,
+                             double* __restrict__ Ct, int64_t strideCt, int64_t npad, int64_t opad,
+                             double* __restrict__ sign, const int* __restrict__ active) {
+    const int cl = blockIdx.y;
+    if (active && active[cl] == 0) return;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= opad * npad) return;
+    const int64_t rank = info[2 * cl];
+    const int64_t i = e / npad, mu = e % npad;
+    Ct[cl * strideCt + e] = (i < rank && mu < n) ? Lc[cl * strideL + i * n + mu] : 0.0;
+    if (sign && mu == 0) sign[i] = 1.0;
+}
+
+constexpr int kMaxDevices = 64;
+constexpr int kPivotSmem = 200 * 1024;
+std::mutex g_jk_mutex;
+bool g_jk_configured[kMaxDevices] = {};
+
 __global__ void k_scale_columns(const double* __restrict__ X, double* __restrict__ Xs, int64_t rows, int64_t ld,
                                 int opad, const double* __restrict__ sign) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -255,40 +424,49 @@ __global__ void k_scale_columns(const double* __restrict__ X, double* __restrict
 
 }  // namespace
 
-cudaError_t coulomb_build(const JkPlan& p, const double* D, double* J, double* work, cudaStream_t stream) {
-    // work: Dw (ntiles*4096) | c (naux) | Jt (ntiles*4096)
+cudaError_t coulomb_build(const JkPlan& p, const double* D, int64_t strideD, double scale, double* J, int64_t strideJ,
+                          double* work, cudaStream_t stream) {
+    // work per cluster: Dw (ntiles*4096) | c (naux) | Jt (ntiles*4096)
     const int64_t nelem = p.ntiles * 4096;
+    const int64_t sw = coulomb_work_doubles(p);
     double* Dw = work;
     double* c = work + nelem;
     double* Jt = c + ((p.naux + 1) / 2) * 2;
-    k_pack_density<<<(unsigned)((nelem + 255) / 256), 256, 0, stream>>>(D, p.n, p.nt, Dw);
-    k_coulomb_charges<<<p.naux, 512, 0, stream>>>(p.B, p.ldb, nelem, Dw, c);
-    cudaMemsetAsync(Jt, 0, sizeof(double) * nelem, stream);
-    dim3 grid((unsigned)((nelem / 2 + 255) / 256), (p.naux + kJSlab - 1) / kJSlab);
-    k_coulomb_assemble<<<grid, 256, 0, stream>>>(p.B, p.ldb, nelem, p.naux, c, Jt);
+    const unsigned cnt = (unsigned)p.count;
+    k_pack_density<<<dim3((unsigned)((nelem + 255) / 256), cnt), 256, 0, stream>>>(D, strideD, scale, p.n, p.nt, Dw, sw,
+                                                                                   p.active);
+    k_coulomb_charges<<<dim3(p.naux, cnt), 512, 0, stream>>>(p.Btab, p.B, p.ldb, nelem, Dw, c, sw, p.active);
+    if (p.count == 1) {
+        cudaMemsetAsync(Jt, 0, sizeof(double) * nelem, stream);
+    } else {
+        cudaMemset2DAsync(Jt, sizeof(double) * sw, 0, sizeof(double) * nelem, p.count, stream);
+    }
+    dim3 grid((unsigned)((nelem / 2 + 255) / 256), (p.naux + kJSlab - 1) / kJSlab, cnt);
+    k_coulomb_assemble<<<grid, 256, 0, stream>>>(p.Btab, p.B, p.ldb, nelem, p.naux, c, Jt, sw, p.active);
     const int64_t nn = p.n * p.n;
-    k_unpack_tiles<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(Jt, p.n, p.nt, J);
+    k_unpack_tiles<<<dim3((unsigned)((nn + 255) / 256), cnt), 256, 0, stream>>>(Jt, sw, p.n, p.nt, J, strideJ, p.active);
     return cudaGetLastError();
 }
 
 int64_t coulomb_work_doubles(const JkPlan& p) { return 2 * p.ntiles * 4096 + ((p.naux + 1) / 2) * 2; }
 
-cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int opad, const double* sign, double* K,
-                                double* Kp, double* X, double* Xs, int qchunk, cudaStream_t stream) {
+cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int64_t strideCt, int opad, const double* sign,
+                                double* K, int64_t strideK, double* Kp, double* X, double* Xs, int qchunk,
+                                cudaStream_t stream) {
     const int64_t npad = (int64_t)p.nt * 64;
-    cudaMemsetAsync(Kp, 0, sizeof(double) * npad * npad, stream);
+    if (sign != nullptr && p.count != 1) return cudaErrorInvalidValue;
+    cudaError_t e = jk_configure();
+    if (e != cudaSuccess) return e;
+    cudaMemsetAsync(Kp, 0, sizeof(double) * npad * npad * p.count, stream);
+    const int smem = XST * (XBM + XBN) * XLD * (int)sizeof(double);
+    const int row_tiles = (int)((npad + XBM - 1) / XBM);
+    const int64_t strideX = npad * (int64_t)qchunk * opad;
     for (int q0 = 0; q0 < p.naux; q0 += qchunk) {
         const int qc = (p.naux - q0 < qchunk) ? p.naux - q0 : qchunk;
         const int64_t ldx = (int64_t)qc * opad;
-        static bool configured = false;
-        const int smem = XST * (XBM + XBN) * XLD * (int)sizeof(double);
-        if (!configured) {
-            cudaError_t e = cudaFuncSetAttribute(k_exchange_half, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            if (e != cudaSuccess) return e;
-            configured = true;
-        }
-        dim3 grid(opad / 64, (unsigned)((npad + XBM - 1) / XBM), qc);
-        k_exchange_half<<<grid, XTHREADS, smem, stream>>>(p.B, p.ldb, q0, p.nt, Ct, npad, (int)npad, X, ldx, opad);
+        dim3 grid(opad / 64, (unsigned)(row_tiles * p.count), qc);
+        k_exchange_half<<<grid, XTHREADS, smem, stream>>>(p.Btab, p.B, p.ldb, q0, p.nt, Ct, npad, strideCt, (int)npad, X,
+                                                          ldx, strideX, opad, p.active);
         const double* Xb = X;
         if (sign != nullptr) {
             const int64_t tot = npad * ldx;
@@ -308,12 +486,49 @@ cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int opad, con
         g.beta = 1.0;
         g.kmode = 0;
         g.epi = 3;
-        cudaError_t e = dgemm_nt(g, 1, stream);
+        g.strideA = g.strideB = strideX;
+        g.strideC = npad * npad;
+        g.active = p.active;
+        e = dgemm_nt(g, p.count, stream);
         if (e != cudaSuccess) return e;
     }
     const int64_t nn = p.n * p.n;
-    k_symmetrize_upper<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(Kp, npad, p.n, K);
+    k_symmetrize_upper<<<dim3((unsigned)((nn + 255) / 256), (unsigned)p.count), 256, 0, stream>>>(Kp, npad, p.n, K,
+                                                                                                 strideK, p.active);
     return cudaGetLastError();
+}
+
+cudaError_t pivoted_cholesky(const double* D, int64_t strideD, int n, double tol, int maxr, double* Lc,
+                             int64_t strideL, int* info, int count, const int* active, cudaStream_t stream) {
+    const size_t smem = sizeof(double) * n + n + 16;
+    if (smem > kPivotSmem) return cudaErrorInvalidValue;
+    cudaError_t e = jk_configure();
+    if (e != cudaSuccess) return e;
+    k_pivoted_cholesky<<<count, 1024, smem, stream>>>(D, strideD, n, tol, maxr, Lc, strideL, info, active);
+    return cudaGetLastError();
+}
+
+cudaError_t factor_pad(const double* Lc, int64_t strideL, int64_t n, const int* info, double* Ct, int64_t strideCt,
+                       int64_t npad, int64_t opad, double* sign, int count, const int* active, cudaStream_t stream) {
+    k_factor_pad<<<dim3((unsigned)((opad * npad + 255) / 256), (unsigned)count), 256, 0, stream>>>(
+        Lc, strideL, n, info, Ct, strideCt, npad, opad, sign, active);
+    return cudaGetLastError();
+}
+
+cudaError_t jk_configure() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_jk_mutex);
+    if (g_jk_configured[dev]) return cudaSuccess;
+    const int smem = XST * (XBM + XBN) * XLD * (int)sizeof(double);
+    e = cudaFuncSetAttribute(k_exchange_half, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_pivoted_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, kPivotSmem);
+    if (e != cudaSuccess) return e;
+    g_jk_configured[dev] = true;
+    return dgemm_configure();
 }
 
 }  // namespace hf

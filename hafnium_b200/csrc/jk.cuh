@@ -4,7 +4,9 @@
 
 namespace hf {
 
-// The packed fitted tensor as the J and K builds see it.
+// The packed fitted tensor as the J and K builds see it. One cluster, or a
+// batch of `count` clusters of equal shape whose tensors are listed in the
+// device table Btab (B is then ignored).
 struct JkPlan {
     const double* B;  // [naux][ntiles][64][64]
     int64_t ldb;      // ntiles * 4096
@@ -12,16 +14,48 @@ struct JkPlan {
     int nt;           // 64-wide tiles per side (n padded to 64 nt)
     int64_t ntiles;   // nt (nt + 1) / 2
     int naux;
+    const double* const* Btab = nullptr;  // [count] per-cluster tensors (device)
+    int count = 1;
+    const int* active = nullptr;  // [count]: clusters whose entry is 0 are skipped
 };
 
-// J = sum_q (B_q . D) B_q for a full symmetric n x n D (device), J full n x n.
-cudaError_t coulomb_build(const JkPlan& p, const double* D, double* J, double* work, cudaStream_t stream);
-int64_t coulomb_work_doubles(const JkPlan& p);
+// J = scale * sum_q (B_q . D) B_q for a full symmetric n x n D (device), J full
+// n x n; per cluster c: D + c strideD, J + c strideJ, work + c coulomb_work_doubles.
+cudaError_t coulomb_build(const JkPlan& p, const double* D, int64_t strideD, double scale, double* J, int64_t strideJ,
+                          double* work, cudaStream_t stream);
+inline cudaError_t coulomb_build(const JkPlan& p, const double* D, double* J, double* work, cudaStream_t stream) {
+    return coulomb_build(p, D, 0, 1.0, J, 0, work, stream);
+}
+int64_t coulomb_work_doubles(const JkPlan& p);  // per cluster
 
 // K = sum_q (B_q C) diag(sign) (B_q C)^T. Ct: [opad][npad] (C^T, zero padded,
-// opad a multiple of 64). sign: [opad] or null for all +1. Kp: npad x npad
-// scratch; X, Xs: npad x (qchunk * opad) scratch (Xs only when sign != null).
-cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int opad, const double* sign, double* K,
-                                double* Kp, double* X, double* Xs, int qchunk, cudaStream_t stream);
+// opad a multiple of 64). sign: [opad] or null for all +1 (single cluster only).
+// Kp: npad x npad scratch; X, Xs: npad x (qchunk * opad) scratch (Xs only when
+// sign != null). Per cluster c: Ct + c strideCt, K + c strideK, Kp + c npad^2,
+// X + c npad qchunk opad.
+cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int64_t strideCt, int opad, const double* sign,
+                                double* K, int64_t strideK, double* Kp, double* X, double* Xs, int qchunk,
+                                cudaStream_t stream);
+inline cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int opad, const double* sign, double* K,
+                                       double* Kp, double* X, double* Xs, int qchunk, cudaStream_t stream) {
+    return exchange_build_fp64(p, Ct, 0, opad, sign, K, 0, Kp, X, Xs, qchunk, stream);
+}
+
+// Pivoted Cholesky of `count` symmetric PSD n x n matrices (D + c strideD), one
+// CTA each: rows of Lc + c strideL ([rank][n]) with D ~= Lc^T Lc, stopping after
+// maxr rows or when the largest remaining diagonal entry falls to tol times the
+// largest initial one. info[2c] = rank, info[2c + 1] = 1 when D is indefinite.
+// n <= 22000 (the pivot state lives in shared memory).
+cudaError_t pivoted_cholesky(const double* D, int64_t strideD, int n, double tol, int maxr, double* Lc,
+                             int64_t strideL, int* info, int count, const int* active, cudaStream_t stream);
+
+// Ct[i][mu] = Lc[i][mu] (i < info[2c], mu < n), zero padded to [opad][npad] per
+// cluster; sign[i] = 1 when sign is given.
+cudaError_t factor_pad(const double* Lc, int64_t strideL, int64_t n, const int* info, double* Ct, int64_t strideCt,
+                       int64_t npad, int64_t opad, double* sign, int count, const int* active, cudaStream_t stream);
+
+// Sets the kernel attributes on the current device (done lazily by the builds;
+// call it before a stream capture).
+cudaError_t jk_configure();
 
 }  // namespace hf

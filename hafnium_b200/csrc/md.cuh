@@ -91,49 +91,75 @@ __device__ __forceinline__ void boys(double T, const double* __restrict__ table,
     }
 }
 
-// R^0_tuv(alpha, X, Y, Z) for t+u+v <= L into R[tet(t,u,v)]. The loops are
-// left rolled: the table lives in thread-local memory (L1-resident), which keeps
-// the kernels compact and their compile time short.
+// R^0_tuv(alpha, X, Y, Z) for t+u+v <= L into R[tet(t,u,v)]. Up to L = 4 the
+// recursion is unrolled so the table stays in registers; above, the loops are
+// left rolled (the table lives in L1-resident local memory), which keeps the
+// kernels compact and their compile time short.
 template <int L>
 __device__ __forceinline__ void hermite_r(double alpha, double X, double Y, double Z,
                                           const double* __restrict__ btable, double* R) {
     double F[L + 1];
     boys<L>(alpha * (X * X + Y * Y + Z * Z), btable, F);
     const double m2a = -2.0 * alpha;
-    double pw = 1.0;
+    double pw[L + 1];
+    pw[0] = 1.0;
 #pragma unroll
-    for (int k = 0; k < L; ++k) pw *= m2a;
-    R[0] = pw * F[L];
-#pragma unroll 1
-    for (int n = L - 1; n >= 0; --n) {
-        pw *= (1.0 / m2a);
-#pragma unroll 1
-        for (int s = L - n; s >= 1; --s) {
-            int idx = s * (s + 1) * (s + 2) / 6;  // tet(s, 0, 0)
-#pragma unroll 1
-            for (int t = s; t >= 0; --t) {
-                // within shell s: index (u+v)(u+v+1)/2 + v with u+v = s-t
-                const int r = s - t;
-#pragma unroll 1
-                for (int v = 0; v <= r; ++v) {
-                    const int u = r - v;
-                    const int at = idx + r * (r + 1) / 2 + v;
-                    double val;
-                    if (t > 0) {
-                        val = X * R[tet(t - 1, u, v)];
-                        if (t > 1) val += (t - 1) * R[tet(t - 2, u, v)];
-                    } else if (u > 0) {
-                        val = Y * R[tet(t, u - 1, v)];
-                        if (u > 1) val += (u - 1) * R[tet(t, u - 2, v)];
-                    } else {
-                        val = Z * R[tet(t, u, v - 1)];
-                        if (v > 1) val += (v - 1) * R[tet(t, u, v - 2)];
+    for (int k = 1; k <= L; ++k) pw[k] = pw[k - 1] * m2a;
+    R[0] = pw[L] * F[L];
+    if constexpr (L <= 4) {
+#pragma unroll
+        for (int n = L - 1; n >= 0; --n) {
+#pragma unroll
+            for (int s = L - n; s >= 1; --s)
+#pragma unroll
+                for (int t = s; t >= 0; --t)
+#pragma unroll
+                    for (int v = 0; v <= s - t; ++v) {
+                        const int u = s - t - v;
+                        double val;
+                        if (t > 0) {
+                            val = X * R[tet(t - 1, u, v)];
+                            if (t > 1) val += (t - 1) * R[tet(t - 2, u, v)];
+                        } else if (u > 0) {
+                            val = Y * R[tet(t, u - 1, v)];
+                            if (u > 1) val += (u - 1) * R[tet(t, u - 2, v)];
+                        } else {
+                            val = Z * R[tet(t, u, v - 1)];
+                            if (v > 1) val += (v - 1) * R[tet(t, u, v - 2)];
+                        }
+                        R[tet(t, u, v)] = val;
                     }
-                    R[at] = val;
+            R[0] = pw[n] * F[n];
+        }
+    } else {
+#pragma unroll 1
+        for (int n = L - 1; n >= 0; --n) {
+#pragma unroll 1
+            for (int s = L - n; s >= 1; --s) {
+                const int idx = s * (s + 1) * (s + 2) / 6;  // tet(s, 0, 0)
+#pragma unroll 1
+                for (int t = s; t >= 0; --t) {
+                    const int r = s - t;  // u + v
+#pragma unroll 1
+                    for (int v = 0; v <= r; ++v) {
+                        const int u = r - v;
+                        double val;
+                        if (t > 0) {
+                            val = X * R[tet(t - 1, u, v)];
+                            if (t > 1) val += (t - 1) * R[tet(t - 2, u, v)];
+                        } else if (u > 0) {
+                            val = Y * R[tet(t, u - 1, v)];
+                            if (u > 1) val += (u - 1) * R[tet(t, u - 2, v)];
+                        } else {
+                            val = Z * R[tet(t, u, v - 1)];
+                            if (v > 1) val += (v - 1) * R[tet(t, u, v - 2)];
+                        }
+                        R[idx + r * (r + 1) / 2 + v] = val;
+                    }
                 }
             }
+            R[0] = pw[n] * F[n];
         }
-        R[0] = pw * F[n];
     }
 }
 

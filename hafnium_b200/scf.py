@@ -64,20 +64,24 @@ class PrecisionSchedule:
 
     ``fp64``: every build in FP64 (the plain path).
 
-    ``mixed``: split-BF16 builds (three BF16 products, FP32 accumulation) while
-    the orbital gradient is above ``anchor_gradient``; then incremental builds
-    anchored on an FP64 one, K(C_n) = K64(C_a) + [K16(C_n) - K16(C_a)], so the
-    BF16 error scales with the change of the orbitals since the anchor, with a
-    new anchor each time the gradient falls by ``reanchor_factor``; below
-    ``fp64_gradient`` (or when the gradient stops falling) FP64 builds to the
-    end, and the convergence test is only passed on two consecutive FP64
-    energies. DIIS, the eigensolves, J and the energy are FP64 throughout.
+    ``mixed``: split-BF16 builds (three BF16 products, FP32 accumulation) from
+    the occupied orbitals while the orbital gradient is at or above
+    ``anchor_gradient``. The next build is an FP64 anchor K64(D_a), where the
+    DIIS history restarts (it held BF16-accurate matrices). After it every
+    build is incremental, K(D_n) = K64(D_a) + K16(D_n - D_a), with the
+    difference density factored exactly into its positive and negative parts,
+    so the BF16 error scales with |D_n - D_a| rather than with |D_n|. Once the
+    gradient of an incremental build is below the convergence tolerance, the
+    builds are FP64 again. The convergence test then needs two FP64 energies,
+    and the finishing build (driver.py:336) serves as the second. If the
+    gradient stops falling (``stall_window`` builds without halving), FP64 takes
+    over at once. DIIS, the eigensolves, J and the energy are FP64 throughout.
     """
 
     mode: str = "fp64"
-    anchor_gradient: float = 1e-2
-    reanchor_factor: float = 1e-2
-    fp64_gradient: float = 1e-5
+    anchor_gradient: float = 3e-3
+    stall_window: int = 4
+    drop_tolerance: float = 1e-13
 
     def __post_init__(self) -> None:
         if self.mode not in ("fp64", "mixed"):
@@ -294,8 +298,8 @@ class _Rhf:
         self.schedule = schedule
         self.x = canonical_orthogonalizer(ham.s, options.overlap_threshold)
         self.n = ham.n_ao
-        self.anchor = None  # (K64, K16) of the last FP64 anchor build
-        self.anchor_due = False
+        self.anchor_k = None  # K64(D_a) of the last FP64 anchor
+        self.anchor_factor = None  # C_a with D_a = C_a C_a^T
         self.timings = {"coulomb_ms": 0.0, "exchange_ms": 0.0, "eigh_ms": 0.0, "fock_builds": 0}
 
     def solve(self, f):
@@ -325,28 +329,52 @@ class _Rhf:
         self.timings[f"exchange_builds_{key}"] = self.timings.get(f"exchange_builds_{key}", 0) + 1
         return out
 
+    def difference_factors(self, factor):
+        """(P, N) with D_n - D_a = P P^T - N N^T, from a thin QR of [C_n, C_a]:
+        [C_n, C_a] = Q R, D_n - D_a = Q (R S R^T) Q^T with S = diag(I, -I), and
+        the small middle matrix diagonalised; eigenvalues below
+        ``drop_tolerance`` of the largest are dropped."""
+        torch = self.torch
+        m = torch.cat([factor, self.anchor_factor], dim=1)
+        q, r = torch.linalg.qr(m)
+        k = factor.shape[1]
+        sign = torch.ones(m.shape[1], dtype=m.dtype, device=m.device)
+        sign[k:] = -1.0
+        t = (r * sign[None, :]) @ r.T
+        w, u = torch.linalg.eigh(0.5 * (t + t.T))
+        v = q @ u
+        cut = self.schedule.drop_tolerance * float(w.abs().max())
+        pos, neg = w > cut, w < -cut
+        return (v[:, pos] * torch.sqrt(w[pos])[None, :]).contiguous(), \
+            (v[:, neg] * torch.sqrt(-w[neg])[None, :]).contiguous()
+
     def exchange(self, d, factor, precision: str):
-        """K for this iteration in the arithmetic ``precision`` names:
-        ``fp64``, ``bf16`` (plain split-BF16) or ``anchored`` (incremental on the
-        last FP64 anchor)."""
+        """K for this iteration in the arithmetic ``precision`` names: ``fp64``,
+        ``bf16`` (split-BF16 from the orbitals), ``anchor`` (FP64, kept as the
+        base of the increments) or ``incremental``."""
         two_body = self.ham.two_body
-        if precision == "fp64":
-            if factor is None:
-                return self._timed("fp64", lambda: two_body.exchange(d))
-            return self._timed("fp64", lambda: two_body.exchange_factored(factor))
-        if factor is None:
-            return self._timed("bf16", lambda: two_body.context_exchange_bf16(d))
-        k16 = self._timed("bf16", lambda: two_body.exchange_factored(factor, precision=_lib.PREC_BF16X3))
+        if precision in ("fp64", "anchor"):
+            k = self._timed("fp64", lambda: two_body.exchange(d) if factor is None else
+                            two_body.exchange_factored(factor))
+            if precision == "anchor":
+                self.anchor_k, self.anchor_factor = k, factor
+                self.timings["anchors"] = self.timings.get("anchors", 0) + 1
+            return k
         if precision == "bf16":
-            return k16
-        if self.anchor is None or self.anchor_due:
-            k64 = self._timed("fp64", lambda: two_body.exchange_factored(factor))
-            self.anchor = (k64, k16)
-            self.anchor_due = False
-            self.timings["anchors"] = self.timings.get("anchors", 0) + 1
-            return k64
-        k64_a, k16_a = self.anchor
-        return k64_a + (k16 - k16_a)
+            if factor is None:
+                return self._timed("bf16", lambda: two_body.context_exchange_bf16(d))
+            return self._timed("bf16", lambda: two_body.exchange_factored(factor, precision=_lib.PREC_BF16X3))
+        pos, neg = self.difference_factors(factor)
+
+        def increment():
+            out = self.anchor_k.clone()
+            if pos.shape[1]:
+                out += two_body.exchange_factored(pos, precision=_lib.PREC_BF16X3)
+            if neg.shape[1]:
+                out -= two_body.exchange_factored(neg, precision=_lib.PREC_BF16X3)
+            return out
+
+        return self._timed("incremental", increment)
 
     def fock(self, d, factor, precision: str = "fp64"):
         """hamiltonian.py:331-370 for one restricted block."""
@@ -392,31 +420,52 @@ class _Rhf:
         focks, errors, history = [], [], []
         mixed = self.schedule.mode == "mixed"
         precision = "bf16" if mixed else "fp64"
-        anchor_g = math.inf
+        pending = None  # a Fock build already made for d (the mixed finish fallback)
         f = None
         for index in range(opts.max_iterations):
-            f, _, energy = self.fock(d, factor, precision)
+            if pending is not None:
+                f, energy = pending
+                pending = None
+            else:
+                f, _, energy = self.fock(d, factor, precision)
             g = self.x.T @ (f @ d @ s - s @ d @ f) @ self.x
             gnorm = math.sqrt(2.0 * float(torch.sum(g * g)))
             previous = history[-1] if history else None
             change = energy - previous.energy if previous else math.inf
-            history.append(Iteration(index, energy, change, gnorm, precision))
+            built = "fp64" if precision == "anchor" else precision
+            history.append(Iteration(index, energy, change, gnorm, built))
             converged = abs(change) < opts.energy_tolerance and gnorm < opts.gradient_tolerance
-            stalled = len(history) > 3 and precision != "fp64" and all(
-                h.precision != "fp64" for h in history[-4:]) and gnorm > 0.5 * history[-4].gradient_norm
-            if precision == "fp64":
-                # the test counts only when both energies of the pair are FP64
-                if converged and (previous is None or previous.precision == "fp64" or not mixed):
+            if built == "fp64" and not mixed:
+                if converged:
                     return self.finish(f, history, True, t_start)
-            elif converged or stalled or gnorm < self.schedule.fp64_gradient:
-                precision = "fp64"
+            elif built == "fp64":
+                # the reference's test on two FP64 energies: the previous one, or
+                # else the finishing build (driver.py:336) made now
+                if converged and previous is not None and previous.precision == "fp64":
+                    return self.finish(f, history, True, t_start)
+                if gnorm < opts.gradient_tolerance:
+                    w, c = self.solve(f)
+                    d2, factor2 = self.density(w, c, averaged=False)
+                    f2, terms2, e2 = self.fock(d2, factor2, "fp64")
+                    if abs(e2 - energy) < opts.energy_tolerance:
+                        self.torch.cuda.synchronize()
+                        return ScfResult(e2, d2, f2, w, c, True, history, terms2, time.perf_counter() - t_start,
+                                         dict(self.timings))
+                    d, factor, pending = d2, factor2, (f2, e2)
+                    continue
+            if precision == "anchor":
+                precision = "incremental"
+                focks, errors = [], []  # the history held BF16-accurate matrices
             elif precision == "bf16" and gnorm < self.schedule.anchor_gradient:
-                precision = "anchored"
-                self.anchor_due = True
-                anchor_g = gnorm
-            elif precision == "anchored" and gnorm < anchor_g * self.schedule.reanchor_factor:
-                self.anchor_due = True
-                anchor_g = gnorm
+                precision = "anchor"
+            elif precision in ("bf16", "incremental"):
+                window = self.schedule.stall_window
+                recent = [h for h in history[-window - 1:] if h.precision == built]
+                stalled = len(recent) > window and gnorm > 0.5 * recent[0].gradient_norm
+                if precision == "bf16" and stalled:
+                    precision = "anchor"
+                elif stalled or (precision == "incremental" and gnorm < opts.gradient_tolerance):
+                    precision = "fp64"
             focks = (focks + [f])[-opts.diis_size:]
             errors = (errors + [g])[-opts.diis_size:]
             if len(focks) == 1:
@@ -427,7 +476,7 @@ class _Rhf:
                 extrapolated = sum(float(cf) * fk for cf, fk in zip(coef, focks))
             w, c = self.solve(extrapolated)
             d, factor = self.density(w, c, averaged=False)
-        result = self.finish(focks[-1], history, False, t_start)
+        result = self.finish(focks[-1] if focks else f, history, False, t_start)
         raise ConvergenceError(f"the SCF did not converge in {opts.max_iterations} iterations", result)
 
     def finish(self, f, history, converged: bool, t_start: float) -> ScfResult:

@@ -39,6 +39,7 @@ def test_library_exports_every_declared_symbol():
     missing = [name for name in all_declared() if not hasattr(lib, name)]
     assert not missing, missing
     assert set(declared("hfjk.h")) == set(_lib.EXPORTS)
+    assert set(declared("hfbatch.h")) == set(_lib.BATCH_EXPORTS)
     assert len(declared("hfnn.h")) == 8
 
 
