@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batched", type=int, default=0,
+                    help="run the batched workload instead: this many seeded (H2O)n, n uniform in [2, 16]")
     return ap.parse_args()
 
 
@@ -398,10 +400,111 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+BATCH_METRIC = "batched DF-RHF throughput: seeded (H2O)n clusters, n uniform in [2,16], converged per second"
+
+
+def batched_clusters(count: int, seed: int):
+    from hafnium_b200.molecule import water_cluster
+
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(2, 17, size=count)
+    return [water_cluster(int(n), seed * 100000 + i) for i, n in enumerate(sizes)]
+
+
+def run_batched(args) -> None:
+    """Many clusters of uneven size through the graph-resident batched SCF (one
+    graph launch per wave). value = clusters converged per second, from the
+    geometries (integrals, fitted tensors, SCF) to host energies."""
+    import torch
+
+    from hafnium_b200 import batch as hb
+
+    rank, world, local = dist_env()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    mols = batched_clusters(args.batched, args.seed + rank)
+    tuner = hb.TileTuner()
+    # warm-up: library load, SAD atoms, and the tile choice of every shape at its batch size
+    hb.solve_batch(mols[:4], device=local, tuner=tuner)
+    counts = {}
+    for m in mols:
+        counts[m.n_atoms] = counts.get(m.n_atoms, 0) + 1
+    for atoms, c in counts.items():
+        tuner.choose(24 * atoms // 3, min(c, 256), local)
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(local)
+    sampler.start()
+    t0 = time.perf_counter()
+    res = hb.solve_batch(mols, device=local, tuner=tuner)
+    torch.cuda.synchronize(dev)
+    seconds = time.perf_counter() - t0
+    clocks = sampler.stop()
+    # accuracy: the plain per-cluster FP64 path (pinned to the oracle) on one cluster of each size,
+    # and the oracle itself on the two smallest clusters
+    from hafnium_b200.scf import DeviceHamiltonian, atomic_density_guess, solve_rhf
+
+    checked, worst = 0, 0.0
+    seen = set()
+    for i, m in enumerate(mols):
+        if m.n_atoms in seen:
+            continue
+        seen.add(m.n_atoms)
+        ham = DeviceHamiltonian.build(m, BASIS, AUX, device=local)
+        ref = solve_rhf(ham, guess=atomic_density_guess(m, BASIS, device=local))
+        worst = max(worst, abs(ref.energy - res.energies[i]))
+        checked += 1
+        del ham
+    torch.cuda.empty_cache()
+    oracle_worst = 0.0
+    small = sorted(range(len(mols)), key=lambda i: mols[i].n_atoms)[:2]
+    from oracle import dfrhf
+    from hafnium_b200.basis import ShellTable
+
+    for i in small:
+        m = mols[i]
+        orb = ShellTable.build(BASIS, m.symbols, m.positions)
+        aux = ShellTable.build(AUX, m.symbols, m.positions)
+        prob = dfrhf.build_problem(orb, aux, m.nuclear_charges, m.positions, m.nuclear_repulsion_energy(), m.n_alpha)
+        guess = dfrhf.atomic_density_guess(orb, m.symbols, {"O": 8.0, "H": 1.0})
+        ref = dfrhf.solve_rhf(prob.s, prob.h, dfrhf.FittedJK(prob.b), prob.e_nuc, m.n_alpha, guess=guess)
+        oracle_worst = max(oracle_worst, abs(ref.energy - res.energies[i]))
+    waters = [m.n_atoms // 3 for m in mols]
+    k_flops = sum(4.0 * (113 * w) * (24 * w) ** 2 * (5 * w) * int(it) for w, it in zip(waters, res.iterations))
+    fp64_peak = measure_fp64_peak(torch, dev)
+    k_tflops = k_flops / res.timings["run_s"] / 1e12
+    line = {
+        "metric": BATCH_METRIC, "value": len(mols) / seconds, "unit": "clusters/s", "n_gpus": world, "steps": 1,
+        "warmup": 1, "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded rigid-water clusters (no dataset)",
+        "config": {"workload": f"{len(mols)} seeded (H2O)n, n uniform in [2,16] (48-384 functions), "
+                               "cc-pVDZ/def2-universal-jkfit, SAD guess, FP64, one graph launch per wave",
+                   "clusters": len(mols), "parallelism": f"replicas x{world}",
+                   "l2": "per-wave tensors of tens of GB, larger than L2"},
+        "converged": int(sum(s == "converged" for s in res.states)),
+        "iterations": {"mean": float(np.mean(res.iterations)), "max": int(np.max(res.iterations))},
+        "timings": {k: v for k, v in res.timings.items()},
+        "scf_only_clusters_per_s": len(mols) / res.timings["run_s"],
+        "max_abs_dE_vs_fp64_single_cluster": worst, "clusters_checked_fp64": checked,
+        "max_abs_dE_vs_oracle": oracle_worst, "clusters_checked_oracle": len(small),
+        "roofline": {"bound": "tensor", "kernel": "batched FP64 exchange (DMMA half-transform + SYRK), whole run",
+                     "achieved": k_tflops, "peak": fp64_peak, "unit": "TFLOP/s", "frac": k_tflops / fp64_peak,
+                     "traffic": None, "algorithmic": "sum over clusters and Fock builds of 4 naux n^2 nocc",
+                     "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run"},
+        "clocks": clocks,
+        "e2e": {"value": len(mols) / seconds, "unit": "clusters/s",
+                "h2d_bytes_per_step": int(sum(m.positions.nbytes for m in mols)),
+                "d2h_bytes_per_step": int(8 * len(mols))},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.batched:
+        run_batched(args)
     else:
         run_b200(args)
 

@@ -64,6 +64,7 @@ class BatchResult:
     states: list
     seconds: float
     timings: dict = field(default_factory=dict)
+    densities: list | None = None  # per-spin densities (host), when requested
 
     @property
     def converged(self) -> np.ndarray:
@@ -284,8 +285,9 @@ def _state_bytes(n: int, count: int) -> int:
 
 def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-universal-jkfit", *, device: int = 0,
                 options: BatchOptions | None = None, tuner: TileTuner | None = None,
-                memory_fraction: float = 0.6, max_batch: int = 256) -> BatchResult:
-    """Converge every molecule's restricted DF-RHF; energies in input order."""
+                memory_fraction: float = 0.6, max_batch: int = 256, keep_densities: bool = False) -> BatchResult:
+    """Converge every molecule's restricted DF-RHF; energies (and, with
+    ``keep_densities``, the converged per-spin densities) in input order."""
     torch = _torch()
     options = options or BatchOptions()
     tuner = tuner or default_tuner()
@@ -302,6 +304,7 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
     energies = np.full(len(molecules), np.nan)
     iterations = np.zeros(len(molecules), dtype=np.int32)
     states = ["not_run"] * len(molecules)
+    densities = [None] * len(molecules) if keep_densities else None
     timings = {"setup_s": 0.0, "run_s": 0.0, "waves": 0, "tiles": {}}
     # waves: groups in order of size, split to fit the memory budget
     pending = []
@@ -354,9 +357,12 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
         torch.cuda.synchronize(dev)
         t2 = time.perf_counter()
         for b, idx, _ in batches:
-            e, it, st = b.results()
+            dens = torch.empty((b.count, b.n, b.n), dtype=torch.float64, device=dev) if keep_densities else None
+            e, it, st = b.results(dens)
             for j, i in enumerate(idx):
                 energies[i], iterations[i], states[i] = e[j], it[j], st[j]
+                if keep_densities:
+                    densities[i] = dens[j].cpu().numpy()
             b.close()
         for ctxs, *_ in keep:
             for c in ctxs:
@@ -365,4 +371,4 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
         timings["setup_s"] += t1 - t0
         timings["run_s"] += t2 - t1
         timings["waves"] += 1
-    return BatchResult(energies, iterations, states, time.perf_counter() - t_start, timings)
+    return BatchResult(energies, iterations, states, time.perf_counter() - t_start, timings, densities)

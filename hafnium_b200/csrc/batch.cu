@@ -1045,8 +1045,10 @@ int hf_batch_exchange(hf_batch* b, const double* density, int64_t max_rank, doub
     cudaSetDevice(b->device);
     const int maxr = (int)std::min<int64_t>(max_rank, b->n);
     const int opad = (int)std::max<int64_t>(64, round_up(maxr, 64));
-    HB_CU(pivoted_cholesky(density, b->nn, (int)b->n, kRankTolerance, maxr, b->Lc, b->nn, b->info, b->count, b->act_all,
-                           b->stream));
+    // one pivot beyond max_rank tells a density of higher rank from one of exactly max_rank
+    const int probe = (int)std::min<int64_t>(maxr + 1, b->n);
+    HB_CU(pivoted_cholesky(density, b->nn, (int)b->n, kRankTolerance, probe, b->Lc, b->nn, b->info, b->count,
+                           b->act_all, b->stream));
     HB_CU(factor_pad(b->Lc, b->nn, b->n, b->info, b->Ct, (int64_t)opad * b->npad, b->npad, opad, nullptr, b->count,
                      b->act_all, b->stream));
     JkPlan p = b->plan;
@@ -1060,7 +1062,7 @@ int hf_batch_exchange(hf_batch* b, const double* density, int64_t max_rank, doub
     for (int c = 0; c < b->count; ++c) {
         if (info[2 * c + 1])
             return fail(b, HF_ERR_NUMERIC, "density of cluster " + std::to_string(c) + " is not positive semidefinite");
-        if (info[2 * c] == maxr && maxr < b->n)
+        if (info[2 * c] > maxr)
             return fail(b, HF_ERR_NUMERIC, "density of cluster " + std::to_string(c) + " has rank above " +
                                                std::to_string(maxr));
     }

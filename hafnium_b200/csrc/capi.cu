@@ -60,6 +60,8 @@ struct hf_ctx {
     void* d_bf16_b = nullptr;  // full BF16 hi/lo copies of B (split-BF16 exchange)
     double* d_tcwork = nullptr;  // split-BF16 exchange: factor and X chunk
     size_t tcwork_bytes = 0;
+    double* d_ctc = nullptr;  // split-BF16 exchange: the padded FP64 factor
+    size_t ctc_bytes = 0;
     int* d_info = nullptr;
     double* d_scalar = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -290,6 +292,7 @@ int hf_ctx_destroy(hf_ctx* ctx) {
     release(ctx->d_stage);
     release(ctx->d_bf16_b);
     release(ctx->d_tcwork);
+    release(ctx->d_ctc);
     release(ctx->d_info);
     release(ctx->d_scalar);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -739,8 +742,9 @@ int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const doub
     if (precision == HF_PREC_BF16X3) {
         if (neg) return fail(ctx, HF_ERR_ARG, "the split-BF16 exchange takes non-negative weights");
         const TcPlan t = tc_plan(n, ctx->naux, ncols);
-        double* Ct_tc = nullptr;
-        if (alloc(ctx, (void**)&Ct_tc, sizeof(double) * ((size_t)t.opad * t.npad + t.opad))) return HF_ERR_OOM;
+        int sc = ensure_scratch(ctx, &ctx->d_ctc, &ctx->ctc_bytes, sizeof(double) * ((size_t)t.opad * t.npad + t.opad));
+        if (sc != HF_OK) return sc;
+        double* Ct_tc = ctx->d_ctc;
         time_begin(ctx);
         k_factor_transpose<<<(unsigned)((t.opad * t.npad + 255) / 256), 256, 0, ctx->stream>>>(
             dC, n, ncols, dw, Ct_tc, t.npad, t.opad, Ct_tc + (size_t)t.opad * t.npad);
@@ -749,7 +753,6 @@ int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const doub
         if (s == HF_OK && !on_device) cudaMemcpyAsync(K, sK, sizeof(double) * n * n, cudaMemcpyDeviceToHost, ctx->stream);
         ctx->stats.ms_exchange = time_end(ctx);
         ctx->stats.exchange_rank = ncols;
-        release(Ct_tc);
         if (s == HF_OK) s = check_async(ctx, "hf_exchange_factored");
         return s;
     }
@@ -800,8 +803,9 @@ int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_d
     const int64_t rank = res[0];
     if (precision == HF_PREC_BF16X3) {
         const TcPlan t = tc_plan(n, ctx->naux, rank);
-        double* Ct_tc = nullptr;
-        if (alloc(ctx, (void**)&Ct_tc, sizeof(double) * ((size_t)t.opad * t.npad + t.opad))) return HF_ERR_OOM;
+        int sc = ensure_scratch(ctx, &ctx->d_ctc, &ctx->ctc_bytes, sizeof(double) * ((size_t)t.opad * t.npad + t.opad));
+        if (sc != HF_OK) return sc;
+        double* Ct_tc = ctx->d_ctc;
         time_begin(ctx);
         const cudaError_t fe = factor_pad(Lc, 0, n, ctx->d_info, Ct_tc, 0, t.npad, t.opad,
                                           Ct_tc + (size_t)t.opad * t.npad, 1, nullptr, ctx->stream);
@@ -811,7 +815,6 @@ int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_d
         if (s == HF_OK && !on_device) cudaMemcpyAsync(K, sK, sizeof(double) * nn, cudaMemcpyDeviceToHost, ctx->stream);
         ctx->stats.ms_exchange = time_end(ctx);
         ctx->stats.exchange_rank = rank;
-        release(Ct_tc);
         if (s == HF_OK) s = check_async(ctx, "hf_exchange");
         return s;
     }

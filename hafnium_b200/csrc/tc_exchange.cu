@@ -373,9 +373,11 @@ cudaError_t launch_tc(const CUtensorMap& ah, const CUtensorMap& al, const CUtens
     return cudaGetLastError();
 }
 
+// As many pipeline stages (<= 4) as fit in 220 KB of shared memory; the
+// launch adds 1280 bytes of alignment slack and barriers (227 KB is the limit).
 int stages_for(int bn) {
     const size_t per = 2 * BM * BK * 2 + 2 * (size_t)bn * BK * 2;
-    return (int)std::min<size_t>(4, (200 * 1024) / per);
+    return (int)std::max<size_t>(2, std::min<size_t>(4, (220 * 1024) / per));
 }
 
 }  // namespace

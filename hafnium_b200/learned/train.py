@@ -34,17 +34,27 @@ def converged_density(mol, device: int = 0):
     return res.density.cpu().numpy(), res
 
 
-def make_dataset(count: int, seed0: int, n_range=(2, 12), device: int = 0):
+def make_dataset(count: int, seed0: int, n_range=(2, 12), device: int = 0, batched: bool = True):
+    """Converged per-spin densities of seeded clusters as training targets: by
+    default all clusters at once through the batched graph-resident SCF (the
+    same converged densities as the per-cluster path, to 1e-6)."""
     from hafnium_b200.molecule import water_cluster
 
     rng = np.random.default_rng(seed0)
+    mols = [water_cluster(int(rng.integers(n_range[0], n_range[1] + 1)), seed0 + 1000 + k) for k in range(count)]
+    if batched:
+        from hafnium_b200.batch import solve_batch
+
+        res = solve_batch(mols, BASIS, AUX, device=device, keep_densities=True)
+        keep = [i for i, s in enumerate(res.states) if s == "converged"]
+        dens = [res.densities[i] for i in keep]
+        mols = [mols[i] for i in keep]
+    else:
+        dens = [converged_density(m, device)[0] for m in mols]
     data = []
-    for k in range(count):
-        n = int(rng.integers(n_range[0], n_range[1] + 1))
-        mol = water_cluster(n, seed0 + 1000 + k)
-        dens, _ = converged_density(mol, device)
+    for mol, d in zip(mols, dens):
         graph = M.build_graph(mol)
-        data.append((graph, M.local_targets(graph, dens)))
+        data.append((graph, M.local_targets(graph, d)))
     return data
 
 
