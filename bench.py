@@ -36,6 +36,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "DF-RHF (H2O)64 time-to-converge at |ΔE|≤1e-8 Eh: learned+mixed vs plain FP64 GPU"
+# one split-BF16 K build of (H2O)16 read+wrote 1.456 GB (ncu, both stages) over N npad^2 units
+TC_TRAFFIC_H2O16 = (1.082401 + 0.221788 + 0.148659 + 0.003629) * 1e9
+TC_UNITS_H2O16 = 1808 * 384 ** 2
 BASIS, AUX = "cc-pvdz", "def2-universal-jkfit"
 
 
@@ -160,10 +163,13 @@ def one_scf(torch, mol, dev, host_io=False, mode="mixed", guess_kind="sad", prob
                                   learned_density_guess, solve_rhf)
 
     ham = DeviceHamiltonian.build(mol, BASIS, AUX, device=dev.index or 0)
+    t_guess = time.perf_counter()
     if guess_kind == "learned":
         guess = learned_density_guess(mol, ham, device=dev.index or 0)
     else:
         guess = atomic_density_guess(mol, BASIS, device=dev.index or 0)
+    torch.cuda.synchronize()
+    t_guess = time.perf_counter() - t_guess
     result = solve_rhf(ham, guess=guess, options=ScfOptions(), host_io=host_io,
                        schedule=PrecisionSchedule(mode=mode))
     kernel_ms = None
@@ -173,7 +179,8 @@ def one_scf(torch, mol, dev, host_io=False, mode="mixed", guess_kind="sad", prob
     out = {"energy": result.energy, "iterations": result.n_iterations, "converged": result.converged,
            "build": {k: ham.timings.get(k) for k in ("ms_metric", "ms_factor", "ms_three_center", "ms_fit",
                                                      "one_electron_s", "fitted_tensor_s")},
-           "scf": result.timings, "launches": stats["kernel_launches"], "n_ao": ham.n_ao,
+           "scf": {**result.timings, "guess_s": t_guess, "scf_s": result.seconds},
+           "launches": stats["kernel_launches"], "n_ao": ham.n_ao,
            "n_aux": ham.two_body.n_aux, "b_bytes": stats["b_bytes"],
            "precisions": [h.precision for h in result.history], "kernel_ms": kernel_ms}
     del ham, result
@@ -275,10 +282,14 @@ def run_b200(args) -> None:
     if k16_ms:
         executed = 3.0 * k_flops  # three BF16 products per FP64-equivalent product
         k16_exec_tflops = executed / (k16_ms / 1e3) / 1e12
+        # DRAM bytes of one split-BF16 K build from the (H2O)16 ncu capture (stage 1 + stage 2,
+        # profiles/k_tc_split3_h2o16.md), scaled by the units a build processes (N npad^2)
+        traffic = TC_TRAFFIC_H2O16 * (naux * ((n + 127) // 128 * 128) ** 2) / TC_UNITS_H2O16
         roofline = {"bound": "tensor", "kernel": "split-BF16 exchange on tcgen05 (k_tc_split3, both stages), "
                               "one K build from the converged occupied orbitals",
+                    "traffic_note": "DRAM bytes per K build, the (H2O)16 ncu capture scaled by N npad^2",
                     "achieved": k16_exec_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
-                    "frac": k16_exec_tflops / bf16_peak, "traffic": None,
+                    "frac": k16_exec_tflops / bf16_peak, "traffic": traffic,
                     "algorithmic": "3 x 4 naux n^2 nocc BF16 flops per K build (the three split products)",
                     "algorithmic_tflops": k_flops / (k16_ms / 1e3) / 1e12,
                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, of measured)"}

@@ -491,7 +491,7 @@ struct hf_batch {
            *F = nullptr, *G = nullptr, *Fx = nullptr, *T1 = nullptr, *T2 = nullptr, *P = nullptr, *P2 = nullptr,
            *Y = nullptr, *Lc = nullptr, *Fring = nullptr, *Gring = nullptr;
     // J/K scratch
-    double *Ct = nullptr, *Kp = nullptr, *Xch = nullptr, *jwork = nullptr;
+    double *Ct = nullptr, *Kp = nullptr, *Xch = nullptr, *jwork = nullptr, *partial = nullptr;
     int opad_max = 0, qchunk = 0;
     // bookkeeping
     double *ov = nullptr, *scal = nullptr, *pm_beta = nullptr;
@@ -567,6 +567,7 @@ cudaError_t fock_build(hf_batch* b, cudaStream_t s, const int* active, int maxr)
     p.active = active;
     const int qchunk = (int)std::max<int64_t>(1, (int64_t)b->qchunk * b->opad_max / opad);
     e = exchange_build_fp64(p, b->Ct, (int64_t)opad * b->npad, opad, nullptr, b->K, b->nn, b->Kp, b->Xch, nullptr,
+                            b->partial,
                             std::min<int>(qchunk, (int)b->naux), s);
     if (e != cudaSuccess) return e;
     e = coulomb_build(p, b->D, b->nn, 2.0, b->J, b->nn, b->jwork, s);
@@ -699,6 +700,7 @@ int hf_batch_create(hf_ctx* const* clusters, int count, int64_t n_occ, hf_batch*
     b->opad_max = (int)std::max<int64_t>(64, round_up(b->n, 64));
     HB_TAKE(b->Ct, (size_t)count * b->opad_max * b->npad);
     HB_TAKE(b->Kp, (size_t)count * b->npad * b->npad);
+    if (syrk_partial_doubles(b->npad, count) > 0) HB_TAKE(b->partial, (size_t)syrk_partial_doubles(b->npad, count));
     const size_t per_q = sizeof(double) * (size_t)count * b->npad * b->opad_max;
     b->qchunk = (int)std::max<size_t>(1, std::min<size_t>(((size_t)2 << 30) / per_q, (size_t)b->naux));
     b->qchunk = std::min(b->qchunk, 65535);
@@ -1055,7 +1057,7 @@ int hf_batch_exchange(hf_batch* b, const double* density, int64_t max_rank, doub
     p.active = b->act_all;
     const int qchunk = (int)std::max<int64_t>(1, (int64_t)b->qchunk * b->opad_max / opad);
     HB_CU(exchange_build_fp64(p, b->Ct, (int64_t)opad * b->npad, opad, nullptr, exchange, b->nn, b->Kp, b->Xch,
-                              nullptr, std::min<int>(qchunk, (int)b->naux), b->stream));
+                              nullptr, b->partial, std::min<int>(qchunk, (int)b->naux), b->stream));
     std::vector<int> info(2 * b->count);
     HB_CU(cudaMemcpyAsync(info.data(), b->info, sizeof(int) * info.size(), cudaMemcpyDeviceToHost, b->stream));
     HB_CU(cudaStreamSynchronize(b->stream));

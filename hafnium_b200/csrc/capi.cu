@@ -654,12 +654,16 @@ static int exchange_from_ct(hf_ctx* ctx, const double* Ct, int opad, const doubl
     int qchunk = (int)std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)ctx->naux));
     qchunk = std::min(qchunk, 65535);
     const size_t kp_doubles = (size_t)round_up(npad * npad, 32);
-    int st = ensure_scratch(ctx, &ctx->d_kscratch, &ctx->kscratch_bytes, sizeof(double) * kp_doubles + per_q * qchunk);
+    const size_t part_doubles = (size_t)round_up(syrk_partial_doubles(npad, 1), 32);
+    int st = ensure_scratch(ctx, &ctx->d_kscratch, &ctx->kscratch_bytes,
+                            sizeof(double) * (kp_doubles + part_doubles) + per_q * qchunk);
     if (st != HF_OK) return st;
     double* Kp = ctx->d_kscratch;
-    double* X = Kp + kp_doubles;
+    double* part = part_doubles ? Kp + kp_doubles : nullptr;
+    double* X = Kp + kp_doubles + part_doubles;
     double* Xs = any_negative ? X + npad * (int64_t)qchunk * opad : nullptr;
-    cudaError_t e = exchange_build_fp64(p, Ct, opad, any_negative ? sign : nullptr, dK, Kp, X, Xs, qchunk, ctx->stream);
+    cudaError_t e = exchange_build_fp64(p, Ct, opad, any_negative ? sign : nullptr, dK, Kp, X, Xs, part, qchunk,
+                                        ctx->stream);
     ctx->stats.kernel_launches += 3 * ((ctx->naux + qchunk - 1) / qchunk) + 2;
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("exchange: ") + cudaGetErrorString(e));
     return check_async(ctx, "exchange");

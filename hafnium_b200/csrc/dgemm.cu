@@ -48,7 +48,12 @@ __global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN
     k_dgemm_nt(GemmArgs g) {
     constexpr int THREADS = threads_of<BM, BN>();
     constexpr int WARPS_N = BN / 32;
-    const int z = blockIdx.z;
+    const int zz = blockIdx.z;
+    int z = zz, sp = 0;
+    if (g.splits > 1) {
+        z = zz / g.splits;
+        sp = zz - z * g.splits;
+    }
     if (g.active && g.active[z] == 0) return;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     if (g.epi == 2 && n0 > m0 + BM - 1) return;
@@ -57,11 +62,16 @@ __global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN
     const double beta = g.beta_v ? g.beta_v[z] : g.beta;
     const double* A = g.A + (int64_t)z * g.strideA;
     const double* B = g.B + (int64_t)z * g.strideB;
-    double* C = g.C + (int64_t)z * g.strideC;
+    double* C = g.C + (int64_t)zz * g.strideC;
     int kb = 0, ke = g.K;
     if (g.kmode == 1) kb = n0;
     if (g.kmode == 2) ke = min(g.K, m0 + BM);
     kb = (kb / BK) * BK;
+    if (g.splits > 1) {
+        const int span = ((ke - kb + g.splits - 1) / g.splits + BK - 1) / BK * BK;
+        kb = kb + sp * span;
+        ke = min(ke, kb + span);
+    }
     const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
 
     extern __shared__ double smem[];
@@ -158,7 +168,7 @@ cudaError_t configure_one() {
 
 template <int BM, int BN>
 cudaError_t launch(const GemmArgs& g, int batch, cudaStream_t stream) {
-    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, batch);
+    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, batch * (g.splits > 1 ? g.splits : 1));
     k_dgemm_nt<BM, BN><<<grid, threads_of<BM, BN>(), smem_of<BM, BN>(), stream>>>(g);
     return cudaGetLastError();
 }
@@ -186,7 +196,7 @@ cudaError_t dgemm_configure() {
 
 cudaError_t dgemm_nt(const GemmArgs& g, int batch, cudaStream_t stream) {
     if (g.M <= 0 || g.N <= 0 || batch <= 0) return cudaSuccess;
-    if (batch > 65535) return cudaErrorInvalidValue;
+    if ((int64_t)batch * (g.splits > 1 ? g.splits : 1) > 65535) return cudaErrorInvalidValue;
     cudaError_t e = dgemm_configure();
     if (e != cudaSuccess) return e;
     switch (g.tile) {

@@ -17,6 +17,9 @@
 // Batching runs over blockIdx.z with per-batch pointer strides. Optional
 // per-batch arrays: `active` (a batch whose entry is 0 is skipped and its C is
 // left untouched), `alpha_v` / `beta_v` (replace alpha / beta for that batch).
+// With splits > 1 each batch's k range is cut into `splits` parts whose
+// products go to separate C matrices (C + (batch * splits + split) * strideC),
+// for the caller to reduce: deterministic split-K.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -38,14 +41,15 @@ struct GemmArgs {
     const int* active;
     const double* alpha_v;
     const double* beta_v;
-    int tile;  // index into kTileShapes
+    int tile;    // index into kTileShapes
+    int splits;  // > 1: split-K; blockIdx.z = batch * splits + split, C + blockIdx.z * strideC
 };
 
 // CTA tile shapes (BM x BN); warps = (BM / 32) * (BN / 32).
 constexpr int kTileCount = 5;
 constexpr int kTileShapes[kTileCount][2] = {{128, 64}, {64, 64}, {64, 32}, {32, 32}, {128, 128}};
 
-cudaError_t dgemm_nt(const GemmArgs& g, int batch, cudaStream_t stream);
+cudaError_t dgemm_nt(const GemmArgs& g, int batch, cudaStream_t stream);  // batch: matrices (not counting splits)
 
 // Sets the shared-memory attributes of every tile instance on the current
 // device (done lazily by dgemm_nt; call it before a stream capture).

@@ -11,6 +11,7 @@
 //       The half-transform runs per q on DMMA tensor cores reading the tiles of
 //       B_q (transposed for tiles below the diagonal); the second product is a
 //       GEMM over the q-chunk, only upper 64x64 output tiles computed.
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 
@@ -410,6 +411,19 @@ __global__ void k_factor_pad(const double* __restrict__ Lc, int64_t strideL, int
     if (sign && mu == 0) sign[i] = 1.0;
 }
 
+// Kp[c][e] += sum_s P[c][s][e] in split order (deterministic split-K reduction).
+__global__ void k_sum_splits(const double* __restrict__ P, int splits, int64_t nn, double* __restrict__ Kp,
+                             const int* __restrict__ active) {
+    const int c = blockIdx.y;
+    if (active && active[c] == 0) return;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nn) return;
+    const double* src = P + (int64_t)c * splits * nn + e;
+    double s = 0.0;
+    for (int k = 0; k < splits; ++k) s += src[(int64_t)k * nn];
+    Kp[(int64_t)c * nn + e] += s;
+}
+
 constexpr int kMaxDevices = 64;
 constexpr int kPivotSmem = 200 * 1024;
 std::mutex g_jk_mutex;
@@ -450,9 +464,27 @@ cudaError_t coulomb_build(const JkPlan& p, const double* D, int64_t strideD, dou
 
 int64_t coulomb_work_doubles(const JkPlan& p) { return 2 * p.ntiles * 4096 + ((p.naux + 1) / 2) * 2; }
 
+int syrk_splits(int64_t npad, int count) {
+    const int64_t mt = (npad + 127) / 128, nt = (npad + 63) / 64;
+    int64_t upper = 0;
+    for (int64_t i = 0; i < mt; ++i)
+        for (int64_t j = 0; j < nt; ++j)
+            if (i * 128 <= j * 64 + 63) ++upper;
+    const int64_t ctas = upper * std::max(1, count);
+    const int64_t want = 2 * 148;
+    int s = (int)std::min<int64_t>(32, (want + ctas - 1) / ctas);
+    while (s > 1 && (int64_t)s * std::max(1, count) > 65535) --s;
+    return std::max(1, s);
+}
+
+int64_t syrk_partial_doubles(int64_t npad, int count) {
+    const int s = syrk_splits(npad, count);
+    return s > 1 ? (int64_t)s * std::max(1, count) * npad * npad : 0;
+}
+
 cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int64_t strideCt, int opad, const double* sign,
-                                double* K, int64_t strideK, double* Kp, double* X, double* Xs, int qchunk,
-                                cudaStream_t stream) {
+                                double* K, int64_t strideK, double* Kp, double* X, double* Xs, double* partial,
+                                int qchunk, cudaStream_t stream) {
     const int64_t npad = (int64_t)p.nt * 64;
     if (sign != nullptr && p.count != 1) return cudaErrorInvalidValue;
     cudaError_t e = jk_configure();
@@ -489,7 +521,20 @@ cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int64_t strid
         g.strideA = g.strideB = strideX;
         g.strideC = npad * npad;
         g.active = p.active;
-        e = dgemm_nt(g, p.count, stream);
+        const int splits = partial ? syrk_splits(npad, p.count) : 1;
+        if (splits > 1) {
+            // partial products per split, then a fixed-order sum into Kp
+            g.C = partial;
+            g.beta = 0.0;
+            g.splits = splits;
+            e = dgemm_nt(g, p.count, stream);
+            if (e != cudaSuccess) return e;
+            const int64_t nn2 = npad * npad;
+            k_sum_splits<<<dim3((unsigned)((nn2 + 255) / 256), (unsigned)p.count), 256, 0, stream>>>(
+                partial, splits, nn2, Kp, p.active);
+        } else {
+            e = dgemm_nt(g, p.count, stream);
+        }
         if (e != cudaSuccess) return e;
     }
     const int64_t nn = p.n * p.n;

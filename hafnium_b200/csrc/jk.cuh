@@ -31,15 +31,22 @@ int64_t coulomb_work_doubles(const JkPlan& p);  // per cluster
 // K = sum_q (B_q C) diag(sign) (B_q C)^T. Ct: [opad][npad] (C^T, zero padded,
 // opad a multiple of 64). sign: [opad] or null for all +1 (single cluster only).
 // Kp: npad x npad scratch; X, Xs: npad x (qchunk * opad) scratch (Xs only when
-// sign != null). Per cluster c: Ct + c strideCt, K + c strideK, Kp + c npad^2,
+// sign != null); partial: syrk_partial_doubles(npad, count) doubles (may be null
+// when that is 0). Per cluster c: Ct + c strideCt, K + c strideK, Kp + c npad^2,
 // X + c npad qchunk opad.
 cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int64_t strideCt, int opad, const double* sign,
-                                double* K, int64_t strideK, double* Kp, double* X, double* Xs, int qchunk,
-                                cudaStream_t stream);
+                                double* K, int64_t strideK, double* Kp, double* X, double* Xs, double* partial,
+                                int qchunk, cudaStream_t stream);
 inline cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int opad, const double* sign, double* K,
-                                       double* Kp, double* X, double* Xs, int qchunk, cudaStream_t stream) {
-    return exchange_build_fp64(p, Ct, 0, opad, sign, K, 0, Kp, X, Xs, qchunk, stream);
+                                       double* Kp, double* X, double* Xs, double* partial, int qchunk,
+                                       cudaStream_t stream) {
+    return exchange_build_fp64(p, Ct, 0, opad, sign, K, 0, Kp, X, Xs, partial, qchunk, stream);
 }
+
+// Split-K factor of the K = X X^T product for `count` clusters of padded size
+// npad (enough CTAs for two per SM), and the partial-product scratch it needs.
+int syrk_splits(int64_t npad, int count);
+int64_t syrk_partial_doubles(int64_t npad, int count);
 
 // Pivoted Cholesky of `count` symmetric PSD n x n matrices (D + c strideD), one
 // CTA each: rows of Lc + c strideL ([rank][n]) with D ~= Lc^T Lc, stopping after

@@ -303,8 +303,15 @@ class _Rhf:
         self.timings = {"coulomb_ms": 0.0, "exchange_ms": 0.0, "eigh_ms": 0.0, "fock_builds": 0}
 
     def solve(self, f):
-        w, v = self.torch.linalg.eigh(self.x.T @ f @ self.x)
-        return w, self.x @ v
+        torch = self.torch
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        w, v = torch.linalg.eigh(self.x.T @ f @ self.x)
+        c = self.x @ v
+        e1.record()
+        e1.synchronize()
+        self.timings["eigh_ms"] += e0.elapsed_time(e1)
+        return w, c
 
     def density(self, w, c, averaged: bool):
         if averaged or self.averaged:
