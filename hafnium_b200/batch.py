@@ -278,17 +278,23 @@ def _b_bytes(n: int, naux: int) -> int:
     return naux * nt * (nt + 1) // 2 * 4096 * 8
 
 
-def _state_bytes(n: int, count: int) -> int:
+def _cluster_state_bytes(n: int) -> int:
+    """Device bytes of one cluster's batch state (matrices, DIIS rings, K scratch)."""
     npad = (n + 63) // 64 * 64
-    return count * (34 * n * n + 2 * npad * npad) * 8 + (2 << 30)
+    return (34 * n * n + 2 * npad * npad) * 8
+
+
+BATCH_FIXED_BYTES = 2 << 30  # the K chunk buffer of one batch
 
 
 def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-universal-jkfit", *, device: int = 0,
                 options: BatchOptions | None = None, tuner: TileTuner | None = None,
-                memory_fraction: float = 0.6, max_batch: int = 256, keep_densities: bool = False) -> BatchResult:
+                memory_fraction: float = 0.6, max_batch: int = 256, keep_densities: bool = False,
+                setup_threads: int = 8) -> BatchResult:
     """Converge every molecule's restricted DF-RHF; energies (and, with
     ``keep_densities``, the converged per-spin densities) in input order."""
     torch = _torch()
+    _lib.load()  # before any worker thread touches the library
     options = options or BatchOptions()
     tuner = tuner or default_tuner()
     dev = torch.device("cuda", device)
@@ -314,18 +320,20 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
             pending.append((key, idx[k:k + max_batch]))
     free, _ = torch.cuda.mem_get_info(dev)
     budget = memory_fraction * free
+    from concurrent.futures import ThreadPoolExecutor
+
+    pool = ThreadPoolExecutor(max_workers=setup_threads)
     while pending:
         wave, used = [], 0.0
         while pending:
             (n, naux, nocc), idx = pending[0]
-            per = _b_bytes(n, naux)
-            fixed = _state_bytes(n, 1)
-            fit = int(max(0, (budget - used - (2 << 30)) // (per + fixed)))
+            per = _b_bytes(n, naux) + _cluster_state_bytes(n)
+            fit = int(max(0, (budget - used - BATCH_FIXED_BYTES) // per))
             if fit <= 0 and wave:
                 break
             take = max(1, min(len(idx), fit))
             wave.append(((n, naux, nocc), idx[:take]))
-            used += take * (per + fixed) + (2 << 30)
+            used += take * per + BATCH_FIXED_BYTES
             if take < len(idx):
                 pending[0] = ((n, naux, nocc), idx[take:])
                 break
@@ -333,7 +341,8 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
         t0 = time.perf_counter()
         batches, keep = [], []
         for (n, naux, nocc), idx in wave:
-            clusters = [_cluster(molecules[i], basis, auxiliary, device) for i in idx]
+            # each cluster's integrals and fitted tensor on its own stream, several at once
+            clusters = list(pool.map(lambda i: _cluster(molecules[i], basis, auxiliary, device), idx))
             ctxs = [c[0] for c in clusters]
             s = torch.stack([c[1] for c in clusters]).contiguous()
             h = torch.stack([c[2] for c in clusters]).contiguous()
@@ -371,4 +380,5 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
         timings["setup_s"] += t1 - t0
         timings["run_s"] += t2 - t1
         timings["waves"] += 1
+    pool.shutdown()
     return BatchResult(energies, iterations, states, time.perf_counter() - t_start, timings, densities)

@@ -99,6 +99,26 @@ void release(T*& p) {
     p = nullptr;
 }
 
+// Stream-ordered temporaries of the build: allocation and release are ordered on
+// the context's stream and, unlike cudaFree, do not synchronise the device, so
+// contexts on other streams (other clusters) keep running.
+int talloc(hf_ctx* ctx, void** p, size_t bytes) {
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 8, ctx->stream);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(ctx, HF_ERR_OOM, "cudaMallocAsync of " + std::to_string(bytes) + " bytes failed: " +
+                                         cudaGetErrorString(e));
+    }
+    return HF_OK;
+}
+
+template <class T>
+void trelease(hf_ctx* ctx, T*& p) {
+    if (p) cudaFreeAsync((void*)p, ctx->stream);
+    p = nullptr;
+}
+
 int ensure_work(hf_ctx* ctx, size_t bytes) {
     if (ctx->work_bytes >= bytes) return HF_OK;
     release(ctx->d_work);
@@ -502,12 +522,12 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     time_begin(ctx);
     double *L = nullptr, *Linv = nullptr, *LinvT = nullptr, *wk = nullptr;
     const size_t nn = (size_t)N * N;
-    if (alloc(ctx, (void**)&L, nn * 8) || alloc(ctx, (void**)&Linv, nn * 8) || alloc(ctx, (void**)&LinvT, nn * 8) ||
-        alloc(ctx, (void**)&wk, (size_t)N * 64 * 8)) {
-        release(L);
-        release(Linv);
-        release(LinvT);
-        release(wk);
+    if (talloc(ctx, (void**)&L, nn * 8) || talloc(ctx, (void**)&Linv, nn * 8) || talloc(ctx, (void**)&LinvT, nn * 8) ||
+        talloc(ctx, (void**)&wk, (size_t)N * 64 * 8)) {
+        trelease(ctx, L);
+        trelease(ctx, Linv);
+        trelease(ctx, LinvT);
+        trelease(ctx, wk);
         return HF_ERR_OOM;
     }
     HF_CU(cudaMemcpyAsync(L, ctx->d_metric, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -521,10 +541,10 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     HF_CU(cudaMemcpyAsync(&pivmin, ctx->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     HF_CU(cudaStreamSynchronize(ctx->stream));
     if (info != 0) {
-        release(L);
-        release(Linv);
-        release(LinvT);
-        release(wk);
+        trelease(ctx, L);
+        trelease(ctx, Linv);
+        trelease(ctx, LinvT);
+        trelease(ctx, wk);
         return fail(ctx, HF_ERR_NUMERIC, "the Coulomb metric is not positive definite (pivot " + std::to_string(info - 1) +
                                              ")");
     }
@@ -538,15 +558,15 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     HF_CU(triangular_inverse(L, N, N, Linv, LinvT, wk, ctx->stream));
     if ((s = check_async(ctx, "inverse factor")) != HF_OK) return s;
     ctx->stats.ms_factor = time_end(ctx);
-    release(L);
-    release(LinvT);
-    release(wk);
+    trelease(ctx, L);
+    trelease(ctx, LinvT);
+    trelease(ctx, wk);
 
     // B = L^-1 (P|mu nu), chunked over tile rows.
     release(ctx->d_B);
     const int64_t ldb = ctx->ntiles * 4096;
     if (alloc(ctx, (void**)&ctx->d_B, sizeof(double) * (size_t)N * ldb)) {
-        release(Linv);
+        trelease(ctx, Linv);
         return HF_ERR_OOM;
     }
     ctx->stats.b_bytes = (int64_t)sizeof(double) * N * ldb;
@@ -560,9 +580,9 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     const size_t ns = ctx->orb.size();
     PairTask* d_tasks = nullptr;
     const size_t task_cap = ns * (ns + 1) / 2 + 16;
-    if (alloc(ctx, (void**)&T, budget) || alloc(ctx, (void**)&d_tasks, sizeof(PairTask) * task_cap)) {
-        release(T);
-        release(Linv);
+    if (talloc(ctx, (void**)&T, budget) || talloc(ctx, (void**)&d_tasks, sizeof(PairTask) * task_cap)) {
+        trelease(ctx, T);
+        trelease(ctx, Linv);
         return HF_ERR_OOM;
     }
     double ms3c = 0.0, msfit = 0.0;
@@ -576,9 +596,9 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
         time_begin(ctx);
         HF_CU(cudaMemsetAsync(T, 0, sizeof(double) * (size_t)ncols * N, ctx->stream));
         if ((s = three_center_chunk(ctx, row0, row1, T, d_tasks, task_cap)) != HF_OK) {
-            release(T);
-            release(d_tasks);
-            release(Linv);
+            trelease(ctx, T);
+            trelease(ctx, d_tasks);
+            trelease(ctx, Linv);
             return s;
         }
         ms3c += time_end(ctx);
@@ -586,17 +606,17 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
         HF_CU(apply_inverse_factor(Linv, N, N, T, N, ncols, ctx->d_B + t0 * 4096, ldb, ctx->stream));
         ++ctx->stats.kernel_launches;
         if ((s = check_async(ctx, "fitted tensor chunk")) != HF_OK) {
-            release(T);
-            release(d_tasks);
-            release(Linv);
+            trelease(ctx, T);
+            trelease(ctx, d_tasks);
+            trelease(ctx, Linv);
             return s;
         }
         msfit += time_end(ctx);
         row0 = row1;
     }
-    release(T);
-    release(d_tasks);
-    release(Linv);
+    trelease(ctx, T);
+    trelease(ctx, d_tasks);
+    trelease(ctx, Linv);
     HF_CU(cudaStreamSynchronize(ctx->stream));
     HF_CU(cudaGetLastError());
     ctx->stats.ms_three_center = ms3c;

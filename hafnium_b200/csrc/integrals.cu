@@ -9,6 +9,7 @@
 // applied to the bra pair's Hermite coefficients once per primitive pair instead
 // of to every output block (cartesian.rs:93-110, two_electron.rs:1028-1060).
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "integrals.cuh"
@@ -73,6 +74,13 @@ std::vector<double> c2s_host(int l) {
 }  // namespace
 
 void upload_c2s(cudaStream_t stream) {
+    // the tables are constants of the library: written once per device
+    static std::mutex mutex;
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lock(mutex);
+    if (done[dev]) return;
     std::vector<double> all;
     for (int l = 0; l <= kMaxAuxL; ++l) {
         auto m = c2s_host(l);
@@ -99,12 +107,16 @@ void upload_c2s(cudaStream_t stream) {
     cudaMemcpyToSymbolAsync(c_tet_u, tu, sizeof(tu), 0, cudaMemcpyHostToDevice, stream);
     cudaMemcpyToSymbolAsync(c_tet_v, tv, sizeof(tv), 0, cudaMemcpyHostToDevice, stream);
     cudaMemcpyToSymbolAsync(c_cart, cc, sizeof(cc), 0, cudaMemcpyHostToDevice, stream);
-    cudaStreamSynchronize(stream);
+    done[dev] = cudaStreamSynchronize(stream) == cudaSuccess;
 }
 
 // F_m(T_j) for T_j = j * step, m < kBoysOrders, by the series of special.rs:67-81
 // for the highest order and the downward recursion for the rest.
 std::vector<double> boys_grid_host() {
+    static std::mutex mutex;
+    static std::vector<double> cached;
+    std::lock_guard<std::mutex> lock(mutex);
+    if (!cached.empty()) return cached;
     std::vector<double> g(kBoysGrid * kBoysOrders);
     const int nmax = kBoysOrders - 1;
     for (int j = 0; j < kBoysGrid; ++j) {
@@ -120,6 +132,7 @@ std::vector<double> boys_grid_host() {
         row[nmax] = et * sum;
         for (int n = nmax; n >= 1; --n) row[n - 1] = (2.0 * t * row[n] + et) / (2 * n - 1);
     }
+    cached = g;
     return g;
 }
 

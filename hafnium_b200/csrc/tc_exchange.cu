@@ -11,9 +11,10 @@
 //   stage 2  K[p][p'] += sum_(q,i) X[p][(q,i)] X[p'][(q,i)], split over k,
 //            upper 128-row tiles only, FP64 atomics into K.
 //
-// One CTA computes one 128 x BN output tile: warp 4 drives TMA (no multicast),
-// warp 5 allocates TMEM and one thread issues tcgen05.mma (kind::f16, BF16
-// inputs, FP32 accumulate, M = 128), warps 0-3 drain TMEM with tcgen05.ld.
+// A persistent CTA per SM walks 128 x BN output tiles: warp 4 drives TMA (no
+// multicast), warp 5 allocates TMEM and one thread issues tcgen05.mma
+// (kind::f16, BF16 inputs, FP32 accumulate, M = 128) into one of two TMEM
+// accumulators, warps 0-3 drain the other with tcgen05.ld meanwhile.
 // Shared-memory tiles use the 128-byte swizzle that both TMA and the UMMA
 // descriptors understand. Every mbarrier wait is bounded: past the limit the
 // waiting thread records an error and stops waiting, so a fault in the
@@ -48,6 +49,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
@@ -140,8 +145,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 struct TcParams {
     int m_tiles, n_tiles;     // output tiles of 128 x bn
     int bn;                   // N tile (multiple of 16, <= 256)
-    int k_tiles;              // k tiles of 64 per CTA (split range)
+    int k_tiles;              // k tiles of 64 per work item (split range)
     int k_tiles_total;
+    int splits;               // k splits (stage 2)
+    int items;                // work items = output tiles x splits (stage 2: upper tiles only)
     int mode;                 // 0: stage-1 epilogue, 1: stage-2 epilogue
     int stages;
     // stage 1: output row m = q_local * npad + p, column i -> X[p][q_local * ldq + i]
@@ -156,6 +163,35 @@ struct TcParams {
     int* err;
 };
 
+// Work item -> (m tile, n tile, split). Stage 1: m-major, n inner (neighbouring
+// items share the A rows through L2). Stage 2: split-major over the output
+// tiles that touch the upper triangle, enumerated row by row.
+__device__ __forceinline__ void decode_item(const TcParams& P, int w, int& mt, int& nt, int& split) {
+    if (P.mode == 0) {
+        mt = w / P.n_tiles;
+        nt = w - mt * P.n_tiles;
+        split = 0;
+        return;
+    }
+    const int per_split = P.items / P.splits;
+    split = w / per_split;
+    int r = w - split * per_split;
+    for (mt = 0; mt < P.m_tiles; ++mt) {
+        const int first = (mt * BM) / P.bn;  // first n tile with (nt + 1) bn > mt BM
+        const int count = P.n_tiles - first;
+        if (r < count) {
+            nt = first + r;
+            return;
+        }
+        r -= count;
+    }
+    nt = 0;  // not reached for w < items
+}
+
+// Persistent: one CTA per SM walks the work items; the TMEM accumulator is
+// double buffered so the epilogue of one item overlaps the MMAs of the next.
+// Warp 4: TMA producer; warp 5: TMEM allocation and the MMA-issuing thread;
+// warps 0-3: epilogue (TMEM lane = output row).
 __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CUtensorMap mAh,
                                                       const __grid_constant__ CUtensorMap mAl,
                                                       const __grid_constant__ CUtensorMap mBh,
@@ -168,26 +204,22 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
     const int stage_bytes = 2 * a_bytes + 2 * b_bytes;
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + P.stages * stage_bytes);
     uint64_t* empty = full + P.stages;
-    uint64_t* acc_full = empty + P.stages;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 1);
+    uint64_t* acc_full = empty + P.stages;   // [2]
+    uint64_t* acc_empty = acc_full + 2;      // [2]
+    uint64_t* mma_done = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nt = blockIdx.x % P.n_tiles;
-    const int mt = blockIdx.x / P.n_tiles;
-    const int split = blockIdx.y;
-    const int m0 = mt * BM, n0 = nt * P.bn;
-    // stage 2 computes only tiles that touch the upper triangle
-    if (P.mode == 1 && n0 + P.bn <= m0) return;
-    const int kt0 = split * P.k_tiles;
-    const int kt1 = min(P.k_tiles_total, kt0 + P.k_tiles);
-    if (kt0 >= kt1) return;
-
     if (threadIdx.x == 0) {
         for (int s = 0; s < P.stages; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(acc_full, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 128);
+        }
+        mbar_init(mma_done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 4 && lane == 0) {
@@ -197,70 +229,103 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
         prefetch_map(&mBl);
     }
     if (warp == 5) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;\n" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(smem_u32(tmem_slot)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = *tmem_slot;
-    const int nk = kt1 - kt0;
 
     if (warp == 4) {
         if (lane == 0) {
-            int issued = 0;
-            for (int it = 0; it < nk; ++it) {
-                const int s = it % P.stages;
-                const uint32_t ph = (it / P.stages) & 1;
-                if (!mbar_wait(&empty[s], ph ^ 1, P.err)) break;
-                uint8_t* base = smem + s * stage_bytes;
-                mbar_expect_tx(&full[s], stage_bytes);
-                const int kx = (kt0 + it) * BK;
-                tma_load_2d(base, &mAh, &full[s], kx, m0);
-                tma_load_2d(base + a_bytes, &mAl, &full[s], kx, m0);
-                tma_load_2d(base + 2 * a_bytes, &mBh, &full[s], kx, n0);
-                tma_load_2d(base + 2 * a_bytes + b_bytes, &mBl, &full[s], kx, n0);
-                issued = it + 1;
+            int it = 0, issued = 0;
+            bool ok = true;
+            for (int w = blockIdx.x; ok && w < P.items; w += gridDim.x) {
+                int mt, nt, split;
+                decode_item(P, w, mt, nt, split);
+                const int kt0 = split * P.k_tiles, kt1 = min(P.k_tiles_total, kt0 + P.k_tiles);
+                for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                    const int s = it % P.stages;
+                    const uint32_t ph = (it / P.stages) & 1;
+                    if (!mbar_wait(&empty[s], ph ^ 1, P.err)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* base = smem + s * stage_bytes;
+                    mbar_expect_tx(&full[s], stage_bytes);
+                    const int kx = kt * BK;
+                    tma_load_2d(base, &mAh, &full[s], kx, mt * BM);
+                    tma_load_2d(base + a_bytes, &mAl, &full[s], kx, mt * BM);
+                    tma_load_2d(base + 2 * a_bytes, &mBh, &full[s], kx, nt * P.bn);
+                    tma_load_2d(base + 2 * a_bytes + b_bytes, &mBl, &full[s], kx, nt * P.bn);
+                    issued = it + 1;
+                }
             }
             // Before the CTA can exit, every copy this thread issued has landed
             // (already true on the normal path, where the MMA thread consumed them).
-            for (int it = max(0, issued - P.stages); it < issued; ++it)
-                mbar_wait(&full[it % P.stages], (it / P.stages) & 1, P.err);
+            for (int j = max(0, issued - P.stages); j < issued; ++j)
+                mbar_wait(&full[j % P.stages], (j / P.stages) & 1, P.err);
         }
     } else if (warp == 5) {
         if (lane == 0) {
             const uint32_t idesc = idesc_bf16(P.bn);
-            for (int it = 0; it < nk; ++it) {
-                const int s = it % P.stages;
-                const uint32_t ph = (it / P.stages) & 1;
-                if (!mbar_wait(&full[s], ph, P.err)) break;
+            int it = 0, local = 0;
+            bool ok = true;
+            for (int w = blockIdx.x; ok && w < P.items; w += gridDim.x, ++local) {
+                int mt, nt, split;
+                decode_item(P, w, mt, nt, split);
+                const int kt0 = split * P.k_tiles, kt1 = min(P.k_tiles_total, kt0 + P.k_tiles);
+                const int buf = local & 1;
+                // the epilogue has drained this buffer's previous item
+                if (!mbar_wait(&acc_empty[buf], ((local >> 1) & 1) ^ 1, P.err)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                uint8_t* base = smem + s * stage_bytes;
-                const uint64_t ah = umma_desc(smem_u32(base)), al = umma_desc(smem_u32(base + a_bytes));
-                const uint64_t bh = umma_desc(smem_u32(base + 2 * a_bytes));
-                const uint64_t bl = umma_desc(smem_u32(base + 2 * a_bytes + b_bytes));
+                const uint32_t acc_tmem = tmem + (uint32_t)(buf * 256);
+                for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                    const int s = it % P.stages;
+                    const uint32_t ph = (it / P.stages) & 1;
+                    if (!mbar_wait(&full[s], ph, P.err)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    uint8_t* base = smem + s * stage_bytes;
+                    const uint64_t ah = umma_desc(smem_u32(base)), al = umma_desc(smem_u32(base + a_bytes));
+                    const uint64_t bh = umma_desc(smem_u32(base + 2 * a_bytes));
+                    const uint64_t bl = umma_desc(smem_u32(base + 2 * a_bytes + b_bytes));
 #pragma unroll
-                for (int k = 0; k < BK / 16; ++k) {
-                    const uint64_t adv = (uint64_t)(k * 32) >> 4;  // 16 BF16 = 32 bytes along the swizzled row
-                    const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
-                    umma_bf16(tmem, ah + adv, bh + adv, idesc, acc);
-                    umma_bf16(tmem, ah + adv, bl + adv, idesc, 1u);
-                    umma_bf16(tmem, al + adv, bh + adv, idesc, 1u);
+                    for (int k = 0; k < BK / 16; ++k) {
+                        const uint64_t adv = (uint64_t)(k * 32) >> 4;  // 16 BF16 = 32 bytes along the swizzled row
+                        const uint32_t acc = (kt > kt0 || k > 0) ? 1u : 0u;
+                        umma_bf16(acc_tmem, ah + adv, bh + adv, idesc, acc);
+                        umma_bf16(acc_tmem, ah + adv, bl + adv, idesc, 1u);
+                        umma_bf16(acc_tmem, al + adv, bh + adv, idesc, 1u);
+                    }
+                    umma_commit(&empty[s]);
                 }
-                umma_commit(&empty[s]);
+                if (ok) umma_commit(&acc_full[buf]);
             }
             // Arrives once every MMA issued above has completed, also on the error
             // path, so TMEM is never freed under a running MMA.
-            umma_commit(acc_full);
+            umma_commit(mma_done);
         }
     } else {
         // epilogue: warps 0-3 own TMEM lanes 32w .. 32w+31 (output rows)
-        const bool ready = mbar_wait(acc_full, 0, P.err) && *(volatile int*)P.err == 0;
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        const int row = m0 + warp * 32 + lane;
-        if (ready) {
+        int local = 0;
+        for (int w = blockIdx.x; w < P.items; w += gridDim.x, ++local) {
+            int mt, nt, split;
+            decode_item(P, w, mt, nt, split);
+            const int buf = local & 1;
+            bool ready = mbar_wait(&acc_full[buf], (local >> 1) & 1, P.err) && *(volatile int*)P.err == 0;
+            // tcgen05.ld is warp-collective: the whole warp reads or none of it does
+            ready = __all_sync(0xffffffffu, ready);
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            if (!ready) break;
+            const int m0 = mt * BM, n0 = nt * P.bn;
+            const int row = m0 + warp * 32 + lane;
+            const uint32_t acc_tmem = tmem + (uint32_t)(buf * 256) + ((uint32_t)(warp * 32) << 16);
             for (int c = 0; c < P.bn; c += 16) {
                 float v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+                tmem_ld16(acc_tmem + (uint32_t)c, v);
                 if (P.mode == 0) {
                     const int ql = row / P.npad, p = row % P.npad;
                     const int i0 = n0 + c;
@@ -282,12 +347,16 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
                     for (int j = 0; j < 16; ++j) atomicAdd(dst + j, (double)v[j]);
                 }
             }
+            // this buffer is free for the item after next
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            mbar_arrive(&acc_empty[buf]);
         }
     }
+    if (warp == 5 && lane == 0) mbar_wait(mma_done, 0, P.err);
     __syncthreads();
     if (warp == 5) {
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;\n" ::"r"(tmem));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
     }
 }
 
@@ -363,12 +432,22 @@ bool make_map(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols, 
 
 size_t smem_for(int bn, int stages) { return (size_t)stages * (2 * BM * BK * 2 + 2 * bn * BK * 2) + 1024 + 256; }
 
+int sm_count() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+        return 148;
+    return sms;
+}
+
+// One persistent CTA per SM (at most one per work item).
 cudaError_t launch_tc(const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh, const CUtensorMap& bl,
-                      const TcParams& P, int splits, cudaStream_t stream) {
+                      const TcParams& P, cudaStream_t stream) {
     const size_t smem = smem_for(P.bn, P.stages);
     cudaError_t e = cudaFuncSetAttribute(k_tc_split3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    dim3 grid(P.m_tiles * P.n_tiles, splits);
+    if (P.items < 1) return cudaSuccess;
+    const int grid = std::min(P.items, sm_count());
     k_tc_split3<<<grid, 192, smem, stream>>>(ah, al, bh, bl, P);
     return cudaGetLastError();
 }
@@ -451,6 +530,8 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         P.bn = t.bn1;
         P.k_tiles_total = (int)(npad / BK);
         P.k_tiles = P.k_tiles_total;
+        P.splits = 1;
+        P.items = P.m_tiles * P.n_tiles;
         P.mode = 0;
         P.stages = stages_for(P.bn);
         P.xh = xh;
@@ -460,7 +541,7 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         P.opad = t.opad;
         P.ocols = t.opad;
         P.err = d_err;
-        cudaError_t e = launch_tc(mAh, mAl, mCh, mCl, P, 1, stream);
+        cudaError_t e = launch_tc(mAh, mAl, mCh, mCl, P, stream);
         if (e != cudaSuccess) return e;
         // stage 2: K += X X^T over this chunk, split over k
         const int bn2 = 256 <= npad ? 256 : 128;
@@ -479,12 +560,14 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
                 if ((ntile + 1) * bn2 > mt * BM) ++upper;
         const int splits = std::max(1, std::min(Q.k_tiles_total, (2 * 148 + upper - 1) / upper));
         Q.k_tiles = (Q.k_tiles_total + splits - 1) / splits;
+        Q.splits = (Q.k_tiles_total + Q.k_tiles - 1) / Q.k_tiles;  // every split has k tiles
+        Q.items = upper * Q.splits;
         Q.mode = 1;
         Q.stages = stages_for(bn2);
         Q.kout = Kp;
         Q.ldk = npad;
         Q.err = d_err;
-        e = launch_tc(mXh, mXl, mXh2, mXl2, Q, splits, stream);
+        e = launch_tc(mXh, mXl, mXh2, mXl2, Q, stream);
         if (e != cudaSuccess) return e;
     }
     k_symmetrize_upper128<<<(unsigned)((n * n + 255) / 256), 256, 0, stream>>>(Kp, npad, n, K);

@@ -1,15 +1,16 @@
 """Train the learned initial density on converged densities from this SCF.
 
-    python -m hafnium_b200.learned.train --clusters 400 --epochs 40 --out weights.npz
+    python -m hafnium_b200.learned.train --clusters 2000 --epochs 60 --out weights.npz
 
-1. Seeded water clusters (H2O)n, n uniform in [2, 12], are converged with the
-   device DF-RHF (SAD guess, FP64, the reference's default tolerances); their
-   per-spin densities, expressed in the frames of their waters, are the targets.
+1. Seeded water clusters (H2O)n, n uniform in [2, 12], are converged together
+   by the batched device DF-RHF (SAD guess, FP64, the reference's default
+   tolerances); their per-spin densities, expressed in the frames of their
+   waters, are the targets.
 2. The network (hafnium_b200.learned.model) is trained with Adam on the device,
    forward and backward running on the hfnn kernels, several clusters per step.
 3. Held-out (H2O)16-24 clusters are converged from the SAD guess and from the
-   learned guess; the iteration counts, times and energies are recorded in the
-   weights file's metadata.
+   learned guess; iteration counts, first gradients, times (guess included)
+   and energies are recorded in the weights file's metadata.
 """
 
 from __future__ import annotations
@@ -107,36 +108,47 @@ def train(data, epochs: int, batch: int = 8, lr: float = 1e-3, seed: int = 0, de
     return params, mean_diag, history
 
 
-def evaluate(weights, sizes, seed0: int, device: int = 0):
-    """Iterations and time of the plain FP64 SCF from SAD and from the learned guess."""
+def evaluate(weights, sizes, seed0: int, device: int = 0, per_size: int = 3):
+    """Plain FP64 SCF from the SAD guess and from the learned guess on held-out
+    clusters (seeds disjoint from training): iterations, first-iteration
+    gradient, and wall time including the guess itself, after a warm-up run."""
     import torch
 
     from hafnium_b200.molecule import water_cluster
     from hafnium_b200.scf import DeviceHamiltonian, atomic_density_guess, learned_density_guess, solve_rhf
 
+    warm = water_cluster(4, seed0 + 49999)
+    wham = DeviceHamiltonian.build(warm, BASIS, AUX, device=device)
+    solve_rhf(wham, guess=learned_density_guess(warm, wham, weights=weights, device=device))
+    solve_rhf(wham, guess=atomic_density_guess(warm, BASIS, device=device))
+    del wham
     rows = []
-    for k, n in enumerate(sizes):
+    for k, n in enumerate(s for s in sizes for _ in range(per_size)):
         mol = water_cluster(n, seed0 + 50000 + k)
         ham = DeviceHamiltonian.build(mol, BASIS, AUX, device=device)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r_sad = solve_rhf(ham, guess=atomic_density_guess(mol, BASIS, device=device))
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        r_ml = solve_rhf(ham, guess=learned_density_guess(mol, ham, weights=weights, device=device))
-        torch.cuda.synchronize()
-        t2 = time.perf_counter()
-        rows.append({"n_waters": n, "sad_iterations": r_sad.n_iterations, "learned_iterations": r_ml.n_iterations,
-                     "sad_s": t1 - t0, "learned_s": t2 - t1, "dE": r_ml.energy - r_sad.energy})
+        out = {"n_waters": n}
+        for name, make in (("sad", lambda: atomic_density_guess(mol, BASIS, device=device)),
+                           ("learned", lambda: learned_density_guess(mol, ham, weights=weights, device=device))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = solve_rhf(ham, guess=make())
+            torch.cuda.synchronize()
+            out[f"{name}_iterations"] = res.n_iterations
+            out[f"{name}_first_gradient"] = res.history[0].gradient_norm
+            out[f"{name}_s"] = time.perf_counter() - t0
+            out[f"{name}_energy"] = res.energy
+        out["dE"] = out["learned_energy"] - out["sad_energy"]
+        rows.append(out)
+        del ham
     return rows
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--clusters", type=int, default=400)
-    ap.add_argument("--epochs", type=int, default=40)
-    ap.add_argument("--batch", type=int, default=8)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--clusters", type=int, default=2000)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--eval", type=str, default="16,20,24")
     ap.add_argument("--out", type=str, default=str(M.WEIGHTS))
