@@ -492,6 +492,10 @@ def run_batched(args) -> None:
                    "clusters": len(mols), "parallelism": f"replicas x{world}",
                    "l2": "per-wave tensors of tens of GB, larger than L2"},
         "converged": int(sum(s == "converged" for s in res.states)),
+        "states": {st: int(sum(s == st for s in res.states)) for st in sorted(set(res.states))},
+        "not_converged": [{"index": i, "waters": mols[i].n_atoms // 3, "state": res.states[i],
+                           "iterations": int(res.iterations[i])}
+                          for i in range(len(mols)) if res.states[i] != "converged"][:16],
         "iterations": {"mean": float(np.mean(res.iterations)), "max": int(np.max(res.iterations))},
         "timings": {k: v for k, v in res.timings.items()},
         "scf_only_clusters_per_s": len(mols) / res.timings["run_s"],

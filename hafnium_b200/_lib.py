@@ -156,6 +156,13 @@ def shell_struct(table) -> tuple[ShellTableC, tuple]:
     return s, arrays
 
 
+def torch_sync(tensor) -> None:
+    """Wait for the work torch has queued on ``tensor``'s device (its current stream)."""
+    import torch
+
+    torch.cuda.current_stream(tensor.device).synchronize()
+
+
 class Context:
     """One ``hf_ctx``: the device-resident fitted tensor and its J/K builds."""
 
@@ -241,13 +248,19 @@ class Context:
         return out
 
     # -- device entry points (torch CUDA tensors) ---------------------------
+    # The library works on its own stream and synchronises it before returning;
+    # torch's stream is synchronised first, so inputs written by torch kernels
+    # are complete and no memory torch recycles is still in use.
     def coulomb_device(self, d, out) -> None:
+        torch_sync(d)
         self.check(self.lib.hf_coulomb(self.handle, d.data_ptr(), out.data_ptr(), 1), "hf_coulomb")
 
     def exchange_device(self, d, out, precision: int = PREC_FP64) -> None:
+        torch_sync(d)
         self.check(self.lib.hf_exchange(self.handle, d.data_ptr(), out.data_ptr(), precision, 1), "hf_exchange")
 
     def exchange_factored_device(self, c, out, weights=None, precision: int = PREC_FP64) -> None:
+        torch_sync(c)
         self.check(
             self.lib.hf_exchange_factored(
                 self.handle, c.data_ptr(), c.shape[1], None if weights is None else weights.data_ptr(),

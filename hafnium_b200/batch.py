@@ -28,7 +28,7 @@ import numpy as np
 
 from hafnium_b200 import _lib
 from hafnium_b200.basis import ShellTable
-from hafnium_b200.errors import BackendError, InputError
+from hafnium_b200.errors import BackendError, ConvergenceError, InputError
 
 TILE_SHAPES = ((128, 64), (64, 64), (64, 32), (32, 32), (128, 128))
 STATE_NAMES = {0: "iterating", 1: "finishing", 2: "converged", 3: "not_converged", 4: "purification_failed"}
@@ -46,7 +46,7 @@ class BatchOptions:
     diis_size: int = 8
     energy_tolerance: float = 1e-10
     gradient_tolerance: float = 1e-6
-    purify_steps: int = 48
+    purify_steps: int = 64
     purify_tolerance: float = 1e-9
     gemm_tile: int | None = None  # None: chosen by the tile tuner
     use_graph: bool = True
@@ -126,6 +126,8 @@ class Batch:
         self.check(self.lib.hf_batch_run(self.handle, ctypes.byref(opts)), "hf_batch_run")
 
     def results(self, densities=None):
+        if densities is not None:
+            _torch().cuda.synchronize(densities.device)  # the copy runs on the batch's stream
         e = np.empty(self.count)
         it = np.empty(self.count, dtype=np.int32)
         st = np.empty(self.count, dtype=np.int32)
@@ -233,9 +235,9 @@ class _Atoms:
 
     def block(self, symbol: str):
         if symbol not in self.blocks:
-            from hafnium_b200.scf import _spherical_atom
+            from hafnium_b200.scf import atomic_block
 
-            d = _spherical_atom(symbol, self.basis, self.device)
+            d = atomic_block(symbol, self.basis, self.device)
             w = _torch().linalg.eigvalsh(0.5 * (d + d.T))
             self.blocks[symbol] = d
             self.ranks[symbol] = int((w > 1e-14 * float(w.abs().max())).sum())
@@ -265,6 +267,7 @@ def _cluster(molecule, basis: str, auxiliary: str, device: int):
     v = torch.empty_like(s)
     q = torch.as_tensor(molecule.nuclear_charges, dtype=torch.float64, device=dev)
     r = torch.as_tensor(np.ascontiguousarray(molecule.positions), dtype=torch.float64, device=dev)
+    _lib.torch_sync(s)
     for kind, out in ((0, s), (1, t), (2, v)):
         ctx.check(ctx.lib.hf_one_electron(ctx.handle, kind, q.data_ptr() if kind == 2 else None,
                                           r.data_ptr() if kind == 2 else None, q.shape[0] if kind == 2 else 0,
@@ -290,7 +293,7 @@ BATCH_FIXED_BYTES = 2 << 30  # the K chunk buffer of one batch
 def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-universal-jkfit", *, device: int = 0,
                 options: BatchOptions | None = None, tuner: TileTuner | None = None,
                 memory_fraction: float = 0.6, max_batch: int = 256, keep_densities: bool = False,
-                setup_threads: int = 8) -> BatchResult:
+                setup_threads: int = 8, retry_failed: bool = True) -> BatchResult:
     """Converge every molecule's restricted DF-RHF; energies (and, with
     ``keep_densities``, the converged per-spin densities) in input order."""
     torch = _torch()
@@ -377,6 +380,33 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
             for c in ctxs:
                 c.close()
         del keep, batches
+        if retry_failed:
+            # a cluster the batch could not converge (no gap for purification, or
+            # the iteration limit) goes through the per-cluster driver instead
+            from hafnium_b200.scf import DeviceHamiltonian, ScfOptions, atomic_density_guess, solve_rhf
+
+            for _, idx in wave:
+                for i in idx:
+                    if states[i] == "converged":
+                        continue
+                    mol = molecules[i]
+                    ham = DeviceHamiltonian.build(mol, basis, auxiliary, device=device)
+                    try:
+                        res = solve_rhf(ham, guess=atomic_density_guess(mol, basis, device=device),
+                                        options=ScfOptions(max_iterations=options.max_iterations,
+                                                           energy_tolerance=options.energy_tolerance,
+                                                           gradient_tolerance=options.gradient_tolerance,
+                                                           diis_size=options.diis_size))
+                    except ConvergenceError as error:
+                        res = getattr(error, "last", None)
+                    if res is None:
+                        continue
+                    energies[i], iterations[i] = res.energy, res.n_iterations
+                    timings.setdefault("retried", []).append({"index": i, "batch_state": states[i]})
+                    states[i] = "converged" if res.converged else "not_converged"
+                    if keep_densities:
+                        densities[i] = res.density.cpu().numpy()
+                    del ham
         timings["setup_s"] += t1 - t0
         timings["run_s"] += t2 - t1
         timings["waves"] += 1

@@ -632,7 +632,7 @@ int hf_batch_default_options(hf_batch_options* out) {
     out->diis_size = 8;
     out->energy_tolerance = 1e-10;
     out->gradient_tolerance = 1e-6;
-    out->purify_steps = 48;
+    out->purify_steps = 64;
     out->purify_tolerance = 1e-9;
     out->gemm_tile = 0;
     out->use_graph = 1;

@@ -127,6 +127,13 @@ class DeviceHamiltonian:
     def n_ao(self) -> int:
         return self.two_body.n_ao
 
+    def orthogonalizer(self, threshold: float = DEFAULT_OVERLAP_THRESHOLD):
+        """The canonical X of S (orthogonalization.py:16-42), computed once per threshold."""
+        cache = self.__dict__.setdefault("_x_cache", {})
+        if threshold not in cache:
+            cache[threshold] = canonical_orthogonalizer(self.s, threshold)
+        return cache[threshold]
+
     @classmethod
     def build(cls, molecule, basis: str, auxiliary: str, *, device: int = 0) -> "DeviceHamiltonian":
         torch = _torch()
@@ -140,9 +147,11 @@ class DeviceHamiltonian:
         s = torch.empty((n, n), dtype=torch.float64, device=dev)
         t = torch.empty_like(s)
         v = torch.empty_like(s)
-        for kind, out, args in ((0, s, ()), (1, t, ()), (2, v, (molecule.nuclear_charges, molecule.positions))):
-            q = torch.as_tensor(args[0], dtype=torch.float64, device=dev) if args else None
-            r = torch.as_tensor(np.ascontiguousarray(args[1]), dtype=torch.float64, device=dev) if args else None
+        charges = torch.as_tensor(molecule.nuclear_charges, dtype=torch.float64, device=dev)
+        positions = torch.as_tensor(np.ascontiguousarray(molecule.positions), dtype=torch.float64, device=dev)
+        _lib.torch_sync(s)  # the library reads these on its own stream
+        for kind, out, args in ((0, s, ()), (1, t, ()), (2, v, (charges, positions))):
+            q, r = args if args else (None, None)
             ctx.check(
                 ctx.lib.hf_one_electron(ctx.handle, kind, None if q is None else q.data_ptr(),
                                         None if r is None else r.data_ptr(), 0 if q is None else q.shape[0],
@@ -245,24 +254,31 @@ def _spherical_atom(symbol: str, basis: str, device: int):
     return _Rhf(ham, ScfOptions(), PrecisionSchedule(), averaged=True).run(None).density
 
 
+_ATOM_CACHE: dict[tuple, object] = {}
+
+
 def atomic_density_guess(molecule, basis: str, *, device: int = 0):
     """atoms.py:76-120: converge each distinct element once, place the per-spin
-    atomic densities on the diagonal in atom order (molecular case)."""
+    atomic densities on the diagonal in atom order (molecular case). An
+    element's atomic density depends only on the element and the basis, so it
+    is converged once per process and device and kept."""
     torch = _torch()
-    cache: dict[str, object] = {}
-    blocks = []
-    for symbol in molecule.symbols:
-        if symbol not in cache:
-            cache[symbol] = _spherical_atom(symbol, basis, device)
-        blocks.append(cache[symbol])
-    return torch.block_diag(*blocks).contiguous()
+    return torch.block_diag(*[atomic_block(symbol, basis, device) for symbol in molecule.symbols]).contiguous()
+
+
+def atomic_block(symbol: str, basis: str, device: int = 0):
+    """The converged per-spin density of one neutral atom (atoms.py:55-73), cached."""
+    key = (symbol, basis.lower(), device)
+    if key not in _ATOM_CACHE:
+        _ATOM_CACHE[key] = _spherical_atom(symbol, basis, device)
+    return _ATOM_CACHE[key]
 
 
 def project_occupied(ham: DeviceHamiltonian, density, threshold: float = DEFAULT_OVERLAP_THRESHOLD):
     """The idempotent density of the n_alpha leading natural orbitals of ``density``
     in the overlap metric: D' = C C^T with X^T S D S X = V diag(w) V^T, C = X V_top."""
     torch = _torch()
-    x = canonical_orthogonalizer(ham.s, threshold)
+    x = ham.orthogonalizer(threshold)
     d = torch.as_tensor(density, dtype=torch.float64, device=ham.s.device)
     d = 0.5 * (d + d.T)
     m = x.T @ ham.s @ d @ ham.s @ x
@@ -296,7 +312,7 @@ class _Rhf:
         self.ham = ham
         self.options = options
         self.schedule = schedule
-        self.x = canonical_orthogonalizer(ham.s, options.overlap_threshold)
+        self.x = ham.orthogonalizer(options.overlap_threshold)
         self.n = ham.n_ao
         self.anchor_k = None  # K64(D_a) of the last FP64 anchor
         self.anchor_factor = None  # C_a with D_a = C_a C_a^T
