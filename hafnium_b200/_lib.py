@@ -24,7 +24,7 @@ EXPORTS = (
     "hf_ctx_create", "hf_ctx_destroy", "hf_last_error", "hf_set_stream", "hf_shells_upload",
     "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
     "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_four_center", "hf_get_stats",
-    "hf_coulomb_static",
+    "hf_coulomb_static", "hf_mp2_energy",
 )
 
 BATCH_EXPORTS = (
@@ -117,6 +117,7 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_one_electron.argtypes = [v, i, v, v, i64, v, i]
     lib.hf_four_center.argtypes = [v, v, i]
     lib.hf_coulomb_static.argtypes = [v, v, v]
+    lib.hf_mp2_energy.argtypes = [v, v, v, i64, i64, ctypes.POINTER(ctypes.c_double), i]
     lib.hf_get_stats.argtypes = [v, p(StatsC)]
     d = ctypes.c_double
     lib.hf_batch_default_options.argtypes = [p(BatchOptionsC)]
@@ -268,6 +269,23 @@ class Context:
             ),
             "hf_exchange_factored",
         )
+
+    def mp2_energy(self, mo_coefficients, mo_energies, n_occ: int) -> float:
+        """DF-MP2 correlation energy (torch CUDA tensors or NumPy arrays)."""
+        out = ctypes.c_double()
+        if hasattr(mo_coefficients, "data_ptr"):
+            c = mo_coefficients.contiguous()
+            e = mo_energies.contiguous()
+            torch_sync(c)
+            status = self.lib.hf_mp2_energy(self.handle, c.data_ptr(), e.data_ptr(), c.shape[1], int(n_occ),
+                                            ctypes.byref(out), 1)
+        else:
+            c = np.ascontiguousarray(mo_coefficients, dtype=np.float64)
+            e = np.ascontiguousarray(mo_energies, dtype=np.float64)
+            status = self.lib.hf_mp2_energy(self.handle, c.ctypes.data, e.ctypes.data, c.shape[1], int(n_occ),
+                                            ctypes.byref(out), 0)
+        self.check(status, "hf_mp2_energy")
+        return float(out.value)
 
     # -- inspection ----------------------------------------------------------
     def metric(self) -> np.ndarray:

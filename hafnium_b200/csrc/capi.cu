@@ -16,6 +16,7 @@
 #include "jk.cuh"
 #include "linalg.cuh"
 #include "md.cuh"
+#include "mp2.cuh"
 #include "tc_exchange.cuh"
 
 using namespace hf;
@@ -999,6 +1000,34 @@ int hf_four_center(hf_ctx* ctx, double* out, int on_device) {
     if (e == cudaSuccess && !on_device) e = cudaMemcpy(out, tmp, bytes, cudaMemcpyDeviceToHost);
     release(tmp);
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("four-centre: ") + cudaGetErrorString(e));
+    return HF_OK;
+}
+
+int hf_mp2_energy(hf_ctx* ctx, const double* mo_coefficients, const double* mo_energies, int64_t n_mo, int64_t n_occ,
+                  double* correlation, int on_device) {
+    if (!ctx || !mo_coefficients || !mo_energies || !correlation || n_mo < 1 || n_occ < 1 || n_occ > n_mo)
+        return HF_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    if (n_mo > ctx->n) return fail(ctx, HF_ERR_ARG, "more orbitals than basis functions");
+    cudaSetDevice(ctx->device);
+    const JkPlan p = plan_of(ctx);
+    const double* dC = mo_coefficients;
+    const double* de = mo_energies;
+    double* staged = nullptr;
+    if (!on_device) {
+        const size_t cbytes = sizeof(double) * (size_t)ctx->n * n_mo, ebytes = sizeof(double) * (size_t)n_mo;
+        HF_CU(cudaMallocAsync((void**)&staged, cbytes + ebytes, ctx->stream));
+        HF_CU(cudaMemcpyAsync(staged, mo_coefficients, cbytes, cudaMemcpyHostToDevice, ctx->stream));
+        HF_CU(cudaMemcpyAsync(staged + (size_t)ctx->n * n_mo, mo_energies, ebytes, cudaMemcpyHostToDevice, ctx->stream));
+        dC = staged;
+        de = staged + (size_t)ctx->n * n_mo;
+    }
+    cudaError_t e = mp2_energy(p, dC, n_mo, de, n_occ, correlation, ctx->stream);
+    if (staged) cudaFreeAsync(staged, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess)
+        return fail(ctx, e == cudaErrorMemoryAllocation ? HF_ERR_OOM : HF_ERR_CUDA,
+                    std::string("hf_mp2_energy: ") + cudaGetErrorString(e));
     return HF_OK;
 }
 

@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* con
                                                              const double* __restrict__ Ct, int64_t ldc_t,
                                                              int64_t strideCt, int npad, double* __restrict__ X,
                                                              int64_t ldx, int64_t strideX, int opad,
-                                                             const int* __restrict__ active) {
+                                                             const int* __restrict__ active, int transposed) {
     const int row_tiles = (npad + XBM - 1) / XBM;
     const int cl = blockIdx.y / row_tiles;
     if (active && active[cl] == 0) return;
@@ -275,6 +275,24 @@ __global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* con
         }
     }
     asm volatile("cp.async.wait_group 0;\n" ::);
+    if (transposed) {
+        // Xt[(ql, i)][p]: row (ql opad + i), row stride npad
+        double* xt = X + (int64_t)ql * opad * npad;
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int m = m0 + wm + i * 16 + gq + h * 8;
+                    const int nn = n0 + wn + j * 8 + 2 * tq;
+                    if (m < npad) {
+                        xt[(int64_t)nn * npad + m] = acc[i][j][2 * h];
+                        xt[(int64_t)(nn + 1) * npad + m] = acc[i][j][2 * h + 1];
+                    }
+                }
+        return;
+    }
     double* xo = X + (int64_t)ql * opad;
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -498,7 +516,7 @@ cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int64_t strid
         const int64_t ldx = (int64_t)qc * opad;
         dim3 grid(opad / 64, (unsigned)(row_tiles * p.count), qc);
         k_exchange_half<<<grid, XTHREADS, smem, stream>>>(p.Btab, p.B, p.ldb, q0, p.nt, Ct, npad, strideCt, (int)npad, X,
-                                                          ldx, strideX, opad, p.active);
+                                                          ldx, strideX, opad, p.active, 0);
         const double* Xb = X;
         if (sign != nullptr) {
             const int64_t tot = npad * ldx;
@@ -557,6 +575,19 @@ cudaError_t factor_pad(const double* Lc, int64_t strideL, int64_t n, const int* 
                        int64_t npad, int64_t opad, double* sign, int count, const int* active, cudaStream_t stream) {
     k_factor_pad<<<dim3((unsigned)((opad * npad + 255) / 256), (unsigned)count), 256, 0, stream>>>(
         Lc, strideL, n, info, Ct, strideCt, npad, opad, sign, active);
+    return cudaGetLastError();
+}
+
+cudaError_t half_transform_t(const JkPlan& p, const double* Ct, int opad, int q0, int qc, double* Xt,
+                             cudaStream_t stream) {
+    if (p.count != 1) return cudaErrorInvalidValue;
+    cudaError_t e = jk_configure();
+    if (e != cudaSuccess) return e;
+    const int64_t npad = (int64_t)p.nt * 64;
+    const int smem = XST * (XBM + XBN) * XLD * (int)sizeof(double);
+    dim3 grid(opad / 64, (unsigned)((npad + XBM - 1) / XBM), qc);
+    k_exchange_half<<<grid, XTHREADS, smem, stream>>>(p.Btab, p.B, p.ldb, q0, p.nt, Ct, npad, 0, (int)npad, Xt, 0, 0,
+                                                      opad, nullptr, 1);
     return cudaGetLastError();
 }
 

@@ -61,6 +61,11 @@ cudaError_t pivoted_cholesky(const double* D, int64_t strideD, int n, double tol
 cudaError_t factor_pad(const double* Lc, int64_t strideL, int64_t n, const int* info, double* Ct, int64_t strideCt,
                        int64_t npad, int64_t opad, double* sign, int count, const int* active, cudaStream_t stream);
 
+// Xt[(ql, i)][p] = sum_r B_{q0+ql}[p][r] Ct[i][r] for ql < qc, i < opad (one
+// cluster): the half-transform with the orbital index outermost, row stride npad.
+cudaError_t half_transform_t(const JkPlan& p, const double* Ct, int opad, int q0, int qc, double* Xt,
+                             cudaStream_t stream);
+
 // Sets the kernel attributes on the current device (done lazily by the builds;
 // call it before a stream capture).
 cudaError_t jk_configure();

@@ -128,6 +128,14 @@ int hf_one_electron(hf_ctx* ctx, int kind, const double* charges, const double* 
  * with the Rust coulomb_four_center, two_electron.rs:429-935). */
 int hf_four_center(hf_ctx* ctx, double* out, int on_device);
 
+/* DF-MP2 correlation energy of a closed-shell reference from the context's
+ * fitted tensor (hafnium/mp/mp2.py:68-176, df_mp2 + second_order, restricted
+ * class, all electrons correlated): mo_coefficients [n_ao][n_mo] with the
+ * orbitals in increasing energy (the first n_occ doubly occupied),
+ * mo_energies [n_mo]; host or device arrays per on_device. */
+int hf_mp2_energy(hf_ctx* ctx, const double* mo_coefficients, const double* mo_energies, int64_t n_mo, int64_t n_occ,
+                  double* correlation, int on_device);
+
 int hf_get_stats(const hf_ctx* ctx, hf_stats* out);
 
 #ifdef __cplusplus

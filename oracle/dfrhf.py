@@ -367,3 +367,27 @@ def build_problem(orb, aux, charges, positions, e_nuc: float, n_alpha: int) -> D
     half, dropped = inverse_square_root(m)
     b = (half @ t3.reshape(t3.shape[0], -1)).reshape(t3.shape)
     return DfRhfProblem(s, h, b, e_nuc, n_alpha, m, t3, dropped)
+
+
+# ------------------------------------------------------------------ DF-MP2
+def df_mp2(b: np.ndarray, mo_energies: np.ndarray, mo_coefficients: np.ndarray, n_occ: int) -> float:
+    """hafnium/mp/mp2.py:135-176 for a restricted reference.
+
+    The reference sums ``E2 = 1/4 sum_ijab |<ij||ab>|^2 / (e_i + e_j - e_a - e_b)``
+    over spin orbitals with ``(ia|jb) = sum_P B[P,i,a] B[P,j,b]`` in the orbital
+    basis (ADR-0030); for a closed shell the spin sums reduce to
+    ``E2 = sum_ijab (ia|jb) [2 (ia|jb) - (ib|ja)] / (e_i + e_j - e_a - e_b)``
+    over spatial orbitals, all electrons correlated.
+    """
+    order = np.argsort(mo_energies, kind="stable")
+    e = mo_energies[order]
+    c = mo_coefficients[:, order]
+    co, cv = c[:, :n_occ], c[:, n_occ:]
+    eo, ev = e[:n_occ], e[n_occ:]
+    bov = np.einsum("pmn,mi,na->pia", b, co, cv, optimize=True)  # [aux, occ, vir]
+    total = 0.0
+    for i in range(n_occ):
+        iajb = np.einsum("pa,pjb->jab", bov[:, i, :], bov, optimize=True)  # (ia|jb) for all j
+        denom = eo[i] + eo[:, None, None] - ev[None, :, None] - ev[None, None, :]
+        total += float(np.sum(iajb * (2.0 * iajb - iajb.transpose(0, 2, 1)) / denom))
+    return total

@@ -56,6 +56,7 @@ def stored_pyscf(reference: pathlib.Path) -> None:
         one_kinetic=np.asarray(one["kinetic"]),
         one_nuclear=np.asarray(one["nuclear_attraction"]),
         dfrhf_energy_sto3g=np.asarray(mp2["reference_energy"]),
+        dfmp2_correlation_sto3g=np.asarray(mp2["correlation_energy"]),
         rhf_energy_sto3g=np.asarray(scf["energy"] if "energy" in scf else scf["total_energy"]),
     )
 

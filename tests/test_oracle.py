@@ -88,3 +88,18 @@ def test_planted_error_is_caught(pyscf_water):
     m[3, 5] += 1e-10
     with pytest.raises(AssertionError):
         np.testing.assert_allclose(m, pyscf_water["df_metric"], atol=INTEGRAL_TOL, rtol=0)
+
+
+def test_oracle_dfmp2_matches_the_pyscf_fixture():
+    """tests/reference/test_mp2_reference.py:37-60 (stored case): water/STO-3G with
+    def2-universal-jkfit, the reference converged with TIGHT options."""
+    g = golden("pyscf_water.npz")
+    mol = water_sto3g_pyscf_geometry(g["df_positions_bohr"])
+    orb, aux = tables(mol, "sto-3g")
+    prob = dfrhf.build_problem(orb, aux, mol.nuclear_charges, mol.positions, mol.nuclear_repulsion_energy(),
+                               mol.n_alpha)
+    res = dfrhf.solve_rhf(prob.s, prob.h, dfrhf.FittedJK(prob.b), prob.e_nuc, mol.n_alpha,
+                          energy_tolerance=1e-13, gradient_tolerance=1e-9)
+    assert abs(res.energy - float(g["dfrhf_energy_sto3g"])) < 1e-10
+    e2 = dfrhf.df_mp2(prob.b, res.mo_energies, res.mo_coefficients, mol.n_alpha)
+    assert abs(e2 - float(g["dfmp2_correlation_sto3g"])) < 1e-10
