@@ -734,8 +734,11 @@ int hf_batch_create(hf_ctx* const* clusters, int count, int64_t n_occ, hf_batch*
         tab[c] = v.B;
     }
     std::vector<int> ones(count, 1);
+    // synchronous copies from pageable memory may return before their DMA lands; the
+    // device synchronisation orders them before any kernel on the batch's stream
     if (cudaMemcpy(b->d_btab, tab.data(), sizeof(double*) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(b->act_all, ones.data(), sizeof(int) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaDeviceSynchronize() != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess) {
         hf_batch_destroy(b);
         return HF_ERR_CUDA;

@@ -282,8 +282,10 @@ int hf_ctx_create(int device, hf_ctx** out) {
         hf_ctx_destroy(ctx);
         return HF_ERR_OOM;
     }
-    cudaMemcpy(ctx->d_btable, grid.data(), sizeof(double) * grid.size(), cudaMemcpyHostToDevice);
-    if (cudaGetLastError() != cudaSuccess) {
+    // stream-ordered copies: a synchronous cudaMemcpy from pageable memory may
+    // return before its DMA lands, unordered with kernels on this non-blocking stream
+    cudaMemcpyAsync(ctx->d_btable, grid.data(), sizeof(double) * grid.size(), cudaMemcpyHostToDevice, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
         hf_ctx_destroy(ctx);
         return HF_ERR_CUDA;
     }
@@ -398,19 +400,24 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
         alloc(ctx, (void**)&ctx->d_exps, sizeof(double) * exps.size()) ||
         alloc(ctx, (void**)&ctx->d_coefs, sizeof(double) * coefs.size()))
         return HF_ERR_OOM;
-    HF_CU(cudaMemcpy(ctx->d_orb, ctx->orb.data(), sizeof(DevShell) * ctx->orb.size(), cudaMemcpyHostToDevice));
+    HF_CU(cudaMemcpyAsync(ctx->d_orb, ctx->orb.data(), sizeof(DevShell) * ctx->orb.size(), cudaMemcpyHostToDevice,
+                          ctx->stream));
     if (!ctx->aux.empty())
-        HF_CU(cudaMemcpy(ctx->d_aux, ctx->aux.data(), sizeof(DevShell) * ctx->aux.size(), cudaMemcpyHostToDevice));
-    HF_CU(cudaMemcpy(ctx->d_exps, exps.data(), sizeof(double) * exps.size(), cudaMemcpyHostToDevice));
+        HF_CU(cudaMemcpyAsync(ctx->d_aux, ctx->aux.data(), sizeof(DevShell) * ctx->aux.size(), cudaMemcpyHostToDevice,
+                              ctx->stream));
+    HF_CU(cudaMemcpyAsync(ctx->d_exps, exps.data(), sizeof(double) * exps.size(), cudaMemcpyHostToDevice, ctx->stream));
     ctx->h_exps = exps;
     ctx->h_coefs = coefs;
-    HF_CU(cudaMemcpy(ctx->d_coefs, coefs.data(), sizeof(double) * coefs.size(), cudaMemcpyHostToDevice));
+    HF_CU(cudaMemcpyAsync(ctx->d_coefs, coefs.data(), sizeof(double) * coefs.size(), cudaMemcpyHostToDevice,
+                          ctx->stream));
     for (int l = 0; l <= kMaxAuxL; ++l) {
         ctx->aux_count[l] = (int)by_l[l].size();
         if (alloc(ctx, (void**)&ctx->d_aux_by_l[l], sizeof(int) * std::max<size_t>(1, by_l[l].size()))) return HF_ERR_OOM;
         if (!by_l[l].empty())
-            HF_CU(cudaMemcpy(ctx->d_aux_by_l[l], by_l[l].data(), sizeof(int) * by_l[l].size(), cudaMemcpyHostToDevice));
+            HF_CU(cudaMemcpyAsync(ctx->d_aux_by_l[l], by_l[l].data(), sizeof(int) * by_l[l].size(),
+                                  cudaMemcpyHostToDevice, ctx->stream));
     }
+    HF_CU(cudaStreamSynchronize(ctx->stream));
     ctx->stats.n_ao = ctx->n;
     ctx->stats.n_aux = ctx->naux;
     ctx->stats.n_tiles = ctx->ntiles;
@@ -956,9 +963,10 @@ int hf_one_electron(hf_ctx* ctx, int kind, const double* charges, const double* 
     double* spos = sq + std::max<int64_t>(natoms, 1);
     int2* dt = (int2*)(spos + 3 * std::max<int64_t>(natoms, 1));
     if (kind == 2 && natoms > 0) {
-        cudaMemcpy(sq, charges, sizeof(double) * natoms, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
-        cudaMemcpy(spos, positions, sizeof(double) * 3 * natoms,
-                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+        cudaMemcpyAsync(sq, charges, sizeof(double) * natoms,
+                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync(spos, positions, sizeof(double) * 3 * natoms,
+                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream);
     }
     double* dOut = on_device ? out : sOut;
     size_t off = 0;
@@ -967,7 +975,7 @@ int hf_one_electron(hf_ctx* ctx, int kind, const double* charges, const double* 
         for (int lb = 0; lb <= 2 && e == cudaSuccess; ++lb) {
             auto& v = tasks[la][lb];
             if (v.empty()) continue;
-            cudaMemcpy(dt + off, v.data(), sizeof(int2) * v.size(), cudaMemcpyHostToDevice);
+            cudaMemcpyAsync(dt + off, v.data(), sizeof(int2) * v.size(), cudaMemcpyHostToDevice, ctx->stream);
             e = launch_one_electron(kind, la, lb, dt + off, (int)v.size(), ctx->d_orb, ctx->d_exps, ctx->d_coefs, sq,
                                     spos, (int)natoms, ctx->d_btable, dOut, n, ctx->stream);
             ++ctx->stats.kernel_launches;
