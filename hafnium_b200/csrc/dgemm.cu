@@ -26,6 +26,13 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src, const 
                  "r"(bytes));
 }
 
+// 16-byte asynchronous copy of (up to) two doubles: `bytes` of 16, 8 or 0 are
+// read and the rest of the 16 zero-filled. Both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, const double* base, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_addr(dst)), "l"(bytes ? src : base),
+                 "r"(bytes));
+}
+
 __device__ __forceinline__ void mma16x8x8(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
     asm volatile(
         "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
@@ -43,7 +50,8 @@ __host__ __device__ constexpr int smem_of() {
     return STAGES * (BM + BN) * LD * (int)sizeof(double);
 }
 
-template <int BM, int BN>
+// VEC: operands 16-byte aligned with even row strides, copied two doubles at a time.
+template <int BM, int BN, bool VEC>
 __global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN>()) < 1 ? 1 : 512 / threads_of<BM, BN>())
     k_dgemm_nt(GemmArgs g) {
     constexpr int THREADS = threads_of<BM, BN>();
@@ -84,6 +92,24 @@ __global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN
     auto load = [&](int stage, int k0) {
         double* as = As + stage * BM * LD;
         double* bs = Bs + stage * BN * LD;
+        if constexpr (VEC) {
+            auto piece = [&](int gk) { return gk < ke ? (gk + 1 < ke ? 16 : 8) : 0; };
+#pragma unroll
+            for (int i = 0; i < (BM * BK) / (2 * THREADS); ++i) {
+                const int e = tid + i * THREADS;
+                const int r = e / (BK / 2), k = (e % (BK / 2)) * 2;
+                const int gm = m0 + r, gk = k0 + k;
+                cp_async16(as + r * LD + k, A + (int64_t)gm * g.lda + gk, A, gm < g.M ? piece(gk) : 0);
+            }
+#pragma unroll
+            for (int i = 0; i < (BN * BK) / (2 * THREADS); ++i) {
+                const int e = tid + i * THREADS;
+                const int r = e / (BK / 2), k = (e % (BK / 2)) * 2;
+                const int gn = n0 + r, gk = k0 + k;
+                cp_async16(bs + r * LD + k, B + (int64_t)gn * g.ldb + gk, B, gn < g.N ? piece(gk) : 0);
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < (BM * BK) / THREADS; ++i) {
             const int e = tid + i * THREADS;
@@ -163,13 +189,27 @@ __global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN
 
 template <int BM, int BN>
 cudaError_t configure_one() {
-    return cudaFuncSetAttribute(k_dgemm_nt<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_of<BM, BN>());
+    cudaError_t e =
+        cudaFuncSetAttribute(k_dgemm_nt<BM, BN, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_of<BM, BN>());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_dgemm_nt<BM, BN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem_of<BM, BN>());
+}
+
+bool aligned16(const GemmArgs& g) {
+    auto ok = [](const void* p, int64_t ld, int64_t stride) {
+        return (reinterpret_cast<uintptr_t>(p) & 15) == 0 && (ld & 1) == 0 && (stride & 1) == 0;
+    };
+    return ok(g.A, g.lda, g.strideA) && ok(g.B, g.ldb, g.strideB);
 }
 
 template <int BM, int BN>
 cudaError_t launch(const GemmArgs& g, int batch, cudaStream_t stream) {
     dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, batch * (g.splits > 1 ? g.splits : 1));
-    k_dgemm_nt<BM, BN><<<grid, threads_of<BM, BN>(), smem_of<BM, BN>(), stream>>>(g);
+    if (aligned16(g))
+        k_dgemm_nt<BM, BN, true><<<grid, threads_of<BM, BN>(), smem_of<BM, BN>(), stream>>>(g);
+    else
+        k_dgemm_nt<BM, BN, false><<<grid, threads_of<BM, BN>(), smem_of<BM, BN>(), stream>>>(g);
     return cudaGetLastError();
 }
 

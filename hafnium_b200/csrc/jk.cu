@@ -166,16 +166,25 @@ __global__ void k_symmetrize_upper(const double* __restrict__ Kp, int64_t ldk, i
 }
 
 // X[p][ql][i] = sum_r B_q[p][r] Ct[i][r] for q = q0 + ql: 128 x 64 tiles, 8 warps,
-// mma.sync.m16n8k8 (FP64), a 3-stage cp.async pipeline. The A operand is
-// gathered from the packed tiles element by element: tile (Ip, J) when Ip <= J,
-// else the transposed tile (J, Ip); 8-byte copies make the transposition free.
+// mma.sync.m16n8k8 (FP64), a 3-stage pipeline of 16-byte cp.async copies. The A
+// operand comes from the packed tiles: tile (Ip, J) when Ip <= J, else tile
+// (J, Ip) read in its own orientation and transposed by the fragment loads.
 constexpr int XBM = 128, XBN = 64, XBK = 16, XLD = XBK + 4, XST = 3, XTHREADS = 256;
+constexpr int XLDT = 64 + 4;  // pitch of a k-major half: conflict-free fragment loads
+static_assert(XBK * XLDT <= 64 * XLD, "a k-major half fits in the p-major half's space");
 
 __device__ __forceinline__ uint32_t xsmem(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
 __device__ __forceinline__ void xcp8(double* dst, const double* src, const double* base, bool valid) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(xsmem(dst)), "l"(valid ? src : base),
                  "r"(valid ? 8 : 0));
+}
+
+// 16-byte asynchronous copy (both addresses 16-byte aligned); an invalid piece
+// copies nothing and zero-fills.
+__device__ __forceinline__ void xcp16(double* dst, const double* src, const double* base, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(xsmem(dst)), "l"(valid ? src : base),
+                 "r"(valid ? 16 : 0));
 }
 
 __device__ __forceinline__ void xmma(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
@@ -208,26 +217,43 @@ __global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* con
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
     const int nk = npad / XBK;
 
+    // Each stage holds the A rows as two 64-row halves. A half whose tile lies on
+    // or above the diagonal (Ip <= J) is stored p-major ([p][k], pitch XLD) from
+    // tile (Ip, J); a half below it reads tile (J, Ip), where k is the slow index,
+    // and is stored k-major ([k][p], pitch XLDT) so that both the global reads and
+    // the shared writes are contiguous; the fragment loads read it transposed.
+    auto tile_at = [&](int I, int Jt) -> const double* {
+        return Bq + ((int64_t)I * nt - (int64_t)I * (I - 1) / 2 + (Jt - I)) * 4096;
+    };
     auto load = [&](int stage, int k0) {
         double* as = As + stage * XBM * XLD;
         double* bs = Bs + stage * XBN * XLD;
-        const int J = k0 >> 6;
+        const int J = k0 >> 6, kin = k0 & 63;
 #pragma unroll
-        for (int i = 0; i < (XBM * XBK) / XTHREADS; ++i) {
-            const int e = tid + i * XTHREADS;
-            const int r = e / XBK, k = e % XBK;  // row r of the tile, k along the reduction
-            const int p = m0 + r, kk = k0 + k;
-            const int Ip = p >> 6;
-            const double* src = Bq;
-            if (Ip <= J) src = Bq + ((int64_t)Ip * nt - (int64_t)Ip * (Ip - 1) / 2 + (J - Ip)) * 4096 + (p & 63) * 64 + (kk & 63);
-            else src = Bq + ((int64_t)J * nt - (int64_t)J * (J - 1) / 2 + (Ip - J)) * 4096 + (kk & 63) * 64 + (p & 63);
-            xcp8(as + r * XLD + k, src, Bq, p < npad);
+        for (int h = 0; h < 2; ++h) {
+            const int p0 = m0 + 64 * h;
+            const int Ip = p0 >> 6;
+            double* ah = as + h * 64 * XLD;
+            const bool valid = p0 < npad;
+            const bool below = Ip > J;
+            const double* tile = valid ? (below ? tile_at(J, Ip) : tile_at(Ip, J)) : Bq;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int e = tid + c * XTHREADS;  // 512 16-byte pieces of a 64 x 16 half
+                if (!below) {
+                    const int r = e >> 3, kp = (e & 7) * 2;
+                    xcp16(ah + r * XLD + kp, tile + r * 64 + kin + kp, Bq, valid);
+                } else {
+                    const int k = e >> 5, pp = (e & 31) * 2;
+                    xcp16(ah + k * XLDT + pp, tile + (kin + k) * 64 + pp, Bq, valid);
+                }
+            }
         }
 #pragma unroll
-        for (int i = 0; i < (XBN * XBK) / XTHREADS; ++i) {
-            const int e = tid + i * XTHREADS;
-            const int r = e / XBK, k = e % XBK;
-            xcp8(bs + r * XLD + k, Ct + (int64_t)(n0 + r) * ldc_t + k0 + k, Ct, true);
+        for (int c = 0; c < 2; ++c) {
+            const int e = tid + c * XTHREADS;  // 512 16-byte pieces of the 64 x 16 B tile
+            const int r = e >> 3, kp = (e & 7) * 2;
+            xcp16(bs + r * XLD + kp, Ct + (int64_t)(n0 + r) * ldc_t + k0 + kp, Ct, true);
         }
     };
 
@@ -251,16 +277,29 @@ __global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* con
         asm volatile("cp.async.commit_group;\n" ::);
         const double* as = As + (it % XST) * XBM * XLD;
         const double* bs = Bs + (it % XST) * XBN * XLD;
+        // this warp's 32 rows lie in one half; that half's layout for this k tile
+        const int hh = wm >> 6, lr = wm & 63;
+        const bool below = ((m0 >> 6) + hh) > ((it * XBK) >> 6);
+        const double* ah = as + hh * 64 * XLD;
 #pragma unroll
         for (int kk = 0; kk < XBK; kk += 8) {
             double af[2][4], bf[4][2];
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
-                const double* r0 = as + (wm + i * 16 + gq) * XLD + kk + tq;
-                af[i][0] = r0[0];
-                af[i][1] = r0[8 * XLD];
-                af[i][2] = r0[4];
-                af[i][3] = r0[8 * XLD + 4];
+                const int row = lr + i * 16 + gq;
+                if (!below) {
+                    const double* r0 = ah + row * XLD + kk + tq;
+                    af[i][0] = r0[0];
+                    af[i][1] = r0[8 * XLD];
+                    af[i][2] = r0[4];
+                    af[i][3] = r0[8 * XLD + 4];
+                } else {
+                    const double* c0 = ah + (kk + tq) * XLDT + row;
+                    af[i][0] = c0[0];
+                    af[i][1] = c0[8];
+                    af[i][2] = c0[4 * XLDT];
+                    af[i][3] = c0[4 * XLDT + 8];
+                }
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
