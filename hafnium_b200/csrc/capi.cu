@@ -100,6 +100,25 @@ void release(T*& p) {
     p = nullptr;
 }
 
+// The build's stream-ordered temporaries (several GB for large molecules) come
+// from the device's default memory pool; by default the pool returns freed
+// memory to the driver at every synchronisation, so each build would map its
+// temporaries afresh. Keeping up to 8 GB in the pool makes them reusable.
+void keep_pool_memory(int device) {
+    static std::mutex mutex;
+    static bool done[64] = {};
+    if (device < 0 || device >= 64) return;
+    std::lock_guard<std::mutex> lock(mutex);
+    if (done[device]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t threshold = (uint64_t)8 << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    cudaGetLastError();
+    done[device] = true;
+}
+
 // Stream-ordered temporaries of the build: allocation and release are ordered on
 // the context's stream and, unlike cudaFree, do not synchronise the device, so
 // contexts on other streams (other clusters) keep running.
@@ -275,6 +294,7 @@ int hf_ctx_create(int device, hf_ctx** out) {
     cudaEventCreate(&ctx->ev0);
     cudaEventCreate(&ctx->ev1);
     upload_c2s(ctx->stream);
+    keep_pool_memory(device);
     auto grid = boys_grid_host();
     if (alloc(ctx, (void**)&ctx->d_btable, sizeof(double) * grid.size()) != HF_OK ||
         alloc(ctx, (void**)&ctx->d_info, 4 * sizeof(int)) != HF_OK ||
