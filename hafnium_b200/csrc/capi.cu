@@ -977,7 +977,7 @@ int hf_one_electron(hf_ctx* ctx, int kind, const double* charges, const double* 
     for (int a = 0; a < ns; ++a)
         for (int b = 0; b < ns; ++b) tasks[ctx->orb[a].l][ctx->orb[b].l].push_back(make_int2(a, b));
     const size_t need = sizeof(double) * (nn + 4 * (size_t)std::max<int64_t>(natoms, 1)) + sizeof(int2) * ns * ns + 64;
-    if (alloc(ctx, (void**)&buf, need)) return HF_ERR_OOM;
+    if (talloc(ctx, (void**)&buf, need)) return HF_ERR_OOM;
     double* sOut = buf;
     double* sq = sOut + nn;
     double* spos = sq + std::max<int64_t>(natoms, 1);
@@ -1001,9 +1001,11 @@ int hf_one_electron(hf_ctx* ctx, int kind, const double* charges, const double* 
             ++ctx->stats.kernel_launches;
             off += v.size();
         }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e == cudaSuccess && !on_device) e = cudaMemcpy(out, sOut, sizeof(double) * nn, cudaMemcpyDeviceToHost);
-    release(buf);
+    if (e == cudaSuccess && !on_device)
+        e = cudaMemcpyAsync(out, sOut, sizeof(double) * nn, cudaMemcpyDeviceToHost, ctx->stream);
+    trelease(ctx, buf);
+    const cudaError_t se = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = se;
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("one-electron: ") + cudaGetErrorString(e));
     return HF_OK;
 }
