@@ -162,7 +162,9 @@ def one_scf(torch, mol, dev, host_io=False, mode="mixed", guess_kind="sad", prob
     from hafnium_b200.scf import (DeviceHamiltonian, PrecisionSchedule, ScfOptions, atomic_density_guess,
                                   learned_density_guess, solve_rhf)
 
+    t_ham = time.perf_counter()
     ham = DeviceHamiltonian.build(mol, BASIS, AUX, device=dev.index or 0)
+    t_ham = time.perf_counter() - t_ham
     t_guess = time.perf_counter()
     if guess_kind == "learned":
         guess = learned_density_guess(mol, ham, device=dev.index or 0)
@@ -179,12 +181,15 @@ def one_scf(torch, mol, dev, host_io=False, mode="mixed", guess_kind="sad", prob
     out = {"energy": result.energy, "iterations": result.n_iterations, "converged": result.converged,
            "build": {k: ham.timings.get(k) for k in ("ms_metric", "ms_factor", "ms_three_center", "ms_fit",
                                                      "one_electron_s", "fitted_tensor_s")},
-           "scf": {**result.timings, "guess_s": t_guess, "scf_s": result.seconds},
+           "scf": {**result.timings, "guess_s": t_guess, "scf_s": result.seconds, "hamiltonian_s": t_ham},
            "launches": stats["kernel_launches"], "n_ao": ham.n_ao,
            "n_aux": ham.two_body.n_aux, "b_bytes": stats["b_bytes"],
            "precisions": [h.precision for h in result.history], "kernel_ms": kernel_ms}
+    t_free = time.perf_counter()
     del ham, result
     torch.cuda.empty_cache()
+    torch.cuda.synchronize()
+    out["scf"]["teardown_s"] = time.perf_counter() - t_free
     return out
 
 

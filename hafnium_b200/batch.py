@@ -253,11 +253,14 @@ class _Atoms:
         return sum(self.ranks[s] for s in molecule.symbols)
 
 
-def _cluster(molecule, basis: str, auxiliary: str, device: int):
-    """(context with B built, S, H) for one molecule."""
+def _cluster(molecule, basis: str, auxiliary: str, device: int, tables=None):
+    """(context with B built, S, H) for one molecule; ``tables`` = (orbital,
+    auxiliary) shell tables when the caller has them already."""
     torch = _torch()
-    orb = ShellTable.build(basis, molecule.symbols, molecule.positions)
-    aux = ShellTable.build(auxiliary, molecule.symbols, molecule.positions)
+    if tables is None:
+        tables = (ShellTable.build(basis, molecule.symbols, molecule.positions),
+                  ShellTable.build(auxiliary, molecule.symbols, molecule.positions))
+    orb, aux = tables
     ctx = _lib.Context(device)
     ctx.upload(orb, aux)
     dev = torch.device("cuda", device)
@@ -293,7 +296,7 @@ BATCH_FIXED_BYTES = 2 << 30  # the K chunk buffer of one batch
 def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-universal-jkfit", *, device: int = 0,
                 options: BatchOptions | None = None, tuner: TileTuner | None = None,
                 memory_fraction: float = 0.6, max_batch: int = 256, keep_densities: bool = False,
-                setup_threads: int = 8, retry_failed: bool = True) -> BatchResult:
+                setup_threads: int = 16, retry_failed: bool = True) -> BatchResult:
     """Converge every molecule's restricted DF-RHF; energies (and, with
     ``keep_densities``, the converged per-spin densities) in input order."""
     torch = _torch()
@@ -304,9 +307,11 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
     t_start = time.perf_counter()
     atoms = _Atoms(basis, device)
     shapes: dict[tuple, list[int]] = {}
+    tables: dict[int, tuple] = {}
     for i, mol in enumerate(molecules):
-        orb_n = ShellTable.build(basis, mol.symbols, mol.positions).n_functions
-        aux_n = ShellTable.build(auxiliary, mol.symbols, mol.positions).n_functions
+        tables[i] = (ShellTable.build(basis, mol.symbols, mol.positions),
+                     ShellTable.build(auxiliary, mol.symbols, mol.positions))
+        orb_n, aux_n = tables[i][0].n_functions, tables[i][1].n_functions
         if 2 * int(mol.n_alpha) != mol.n_electrons:
             raise InputError("the batched SCF is restricted: every molecule needs an even electron count")
         shapes.setdefault((orb_n, aux_n, int(mol.n_alpha)), []).append(i)
@@ -345,7 +350,7 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
         batches, keep = [], []
         for (n, naux, nocc), idx in wave:
             # each cluster's integrals and fitted tensor on its own stream, several at once
-            clusters = list(pool.map(lambda i: _cluster(molecules[i], basis, auxiliary, device), idx))
+            clusters = list(pool.map(lambda i: _cluster(molecules[i], basis, auxiliary, device, tables.pop(i)), idx))
             ctxs = [c[0] for c in clusters]
             s = torch.stack([c[1] for c in clusters]).contiguous()
             h = torch.stack([c[2] for c in clusters]).contiguous()
