@@ -717,8 +717,9 @@ static int exchange_from_ct(hf_ctx* ctx, const double* Ct, int opad, const doubl
     return check_async(ctx, "exchange");
 }
 
-// Split-BF16 exchange from Ct_tc ([t.opad][t.npad], FP64, zero padded) into dK (n x n).
-static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, double* dK) {
+// Split-BF16 exchange from Ct_tc ([t.opad][t.npad], FP64, zero padded) into dK (n x n);
+// sign ([t.opad], device) for a signed factor, else null.
+static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, double* dK, const double* sign = nullptr) {
     const JkPlan p = plan_of(ctx);
     if (!ctx->d_bf16_b) {
         if (alloc(ctx, &ctx->d_bf16_b, tc_b_bytes(ctx->n, ctx->naux)))
@@ -734,7 +735,7 @@ static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, doub
     size_t freeb = 0, totalb = 0;
     cudaMemGetInfo(&freeb, &totalb);
     const size_t ct_bytes = 2 * 2 * (size_t)t.opad * t.npad;
-    const size_t per_q = 2 * 2 * (size_t)t.npad * t.opad;
+    const size_t per_q = (sign ? 4 : 2) * 2 * (size_t)t.npad * t.opad;
     const size_t kp_doubles = (size_t)round_up(t.npad * t.npad, 32);
     size_t budget = std::min<size_t>((size_t)2 << 30, freeb / 3);
     size_t want = ct_bytes + per_q * std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)ctx->naux));
@@ -745,7 +746,7 @@ static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, doub
     void* work = ctx->d_tcwork + kp_doubles;
     HF_CU(cudaMemsetAsync(ctx->d_info + 2, 0, sizeof(int), ctx->stream));
     cudaError_t e = exchange_build_bf16(t, ctx->d_bf16_b, Ct_tc, t.npad, dK, Kp, work, want - sizeof(double) * kp_doubles,
-                                        ctx->d_info + 2, ctx->stream, ctx->n);
+                                        ctx->d_info + 2, ctx->stream, ctx->n, sign);
     ctx->stats.kernel_launches += 3 * ((ctx->naux + 1023) / 1024) + 3;
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("split-BF16 exchange: ") + cudaGetErrorString(e));
     int s = check_async(ctx, "split-BF16 exchange");
@@ -792,7 +793,6 @@ int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const doub
         dw = w ? sw : nullptr;
     }
     if (precision == HF_PREC_BF16X3) {
-        if (neg) return fail(ctx, HF_ERR_ARG, "the split-BF16 exchange takes non-negative weights");
         const TcPlan t = tc_plan(n, ctx->naux, ncols);
         int sc = ensure_scratch(ctx, &ctx->d_ctc, &ctx->ctc_bytes, sizeof(double) * ((size_t)t.opad * t.npad + t.opad));
         if (sc != HF_OK) return sc;
@@ -801,7 +801,7 @@ int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const doub
         k_factor_transpose<<<(unsigned)((t.opad * t.npad + 255) / 256), 256, 0, ctx->stream>>>(
             dC, n, ncols, dw, Ct_tc, t.npad, t.opad, Ct_tc + (size_t)t.opad * t.npad);
         double* dK = on_device ? K : sK;
-        int s = exchange_bf16(ctx, t, Ct_tc, dK);
+        int s = exchange_bf16(ctx, t, Ct_tc, dK, neg ? Ct_tc + (size_t)t.opad * t.npad : nullptr);
         if (s == HF_OK && !on_device) cudaMemcpyAsync(K, sK, sizeof(double) * n * n, cudaMemcpyDeviceToHost, ctx->stream);
         ctx->stats.ms_exchange = time_end(ctx);
         ctx->stats.exchange_rank = ncols;

@@ -8,8 +8,9 @@
 //   stage 1  X[(q,p)][i] = sum_r B[(q,p)][r] C[r][i]   one GEMM, M = rows (q,p),
 //            A = BF16 copies of B stored in full (both triangles, K-major),
 //            B-operand = C^T; the epilogue splits X into BF16 hi/lo, p-major.
-//   stage 2  K[p][p'] += sum_(q,i) X[p][(q,i)] X[p'][(q,i)], split over k,
-//            upper 128-row tiles only, FP64 atomics into K.
+//   stage 2  K[p][p'] += sum_(q,i) X[p][(q,i)] s_i X[p'][(q,i)], split over k,
+//            upper 128-row tiles only, FP64 atomics into K (s_i = +-1 for a
+//            signed factor, whose stage 1 also writes X diag(s)).
 //
 // A persistent CTA per SM walks 128 x BN output tiles: warp 4 drives TMA (no
 // multicast), warp 5 allocates TMEM and one thread issues tcgen05.mma
@@ -154,6 +155,10 @@ struct TcParams {
     // stage 1: output row m = q_local * npad + p, column i -> X[p][q_local * ldq + i]
     __nv_bfloat16* xh;
     __nv_bfloat16* xl;
+    // signed factor (optional): X diag(sign) written beside X for stage 2's B operand
+    __nv_bfloat16* xsh;
+    __nv_bfloat16* xsl;
+    const double* sign;  // [opad]
     int64_t ldx;  // row stride of X (= qchunk * opad)
     int npad, opad;
     int ocols;    // valid columns (the rest of the tile is padding)
@@ -340,6 +345,17 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
                             *reinterpret_cast<__nv_bfloat162*>(dh + j) = __halves2bfloat162(h0, h1);
                             *reinterpret_cast<__nv_bfloat162*>(dl + j) = __halves2bfloat162(l0, l1);
                         }
+                        if (P.xsh) {
+                            // negating both parts negates the split value exactly
+                            const int64_t off = (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) {
+                                const __nv_bfloat16 h = dh[j], l = dl[j];
+                                const bool neg = P.sign[i0 + j] < 0.0;
+                                P.xsh[off + j] = neg ? __hneg(h) : h;
+                                P.xsl[off + j] = neg ? __hneg(l) : l;
+                            }
+                        }
                     }
                 } else {
                     double* dst = P.kout + (int64_t)row * P.ldk + n0 + c;
@@ -493,7 +509,7 @@ cudaError_t tc_split_b(const JkPlan& p, int64_t npad, void* bf16_b, cudaStream_t
 
 cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const double* Ct_fp64, int64_t ct_ld,
                                 double* K, double* Kp, void* work, size_t work_bytes, int* d_err,
-                                cudaStream_t stream, int64_t n) {
+                                cudaStream_t stream, int64_t n, const double* sign) {
     (void)ct_ld;
     const int64_t npad = t.npad;
     const __nv_bfloat16* bh = static_cast<const __nv_bfloat16*>(bf16_b);
@@ -504,7 +520,7 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
     __nv_bfloat16* xbase = ctl + (int64_t)t.opad * npad;
     const size_t ct_bytes = sizeof(__nv_bfloat16) * 2 * (size_t)t.opad * npad;
     if (work_bytes <= ct_bytes) return cudaErrorInvalidValue;
-    const size_t per_q = sizeof(__nv_bfloat16) * 2 * (size_t)npad * t.opad;
+    const size_t per_q = sizeof(__nv_bfloat16) * (sign ? 4 : 2) * (size_t)npad * t.opad;
     int qchunk = (int)std::min<size_t>((work_bytes - ct_bytes) / per_q, (size_t)t.naux);
     if (qchunk < 1) return cudaErrorInvalidValue;
     const int64_t cnt = (int64_t)t.opad * npad;
@@ -518,6 +534,8 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         const int64_t ldx = (int64_t)qc * t.opad;
         __nv_bfloat16* xh = xbase;
         __nv_bfloat16* xl = xbase + npad * ldx;
+        __nv_bfloat16* xsh = sign ? xl + npad * ldx : nullptr;
+        __nv_bfloat16* xsl = sign ? xsh + npad * ldx : nullptr;
         // stage 1: rows (q, p) of the full BF16 B for q in [q0, q0 + qc)
         CUtensorMap mAh, mAl;
         const uint64_t rows = (uint64_t)qc * npad;
@@ -536,6 +554,9 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         P.stages = stages_for(P.bn);
         P.xh = xh;
         P.xl = xl;
+        P.xsh = xsh;
+        P.xsl = xsl;
+        P.sign = sign;
         P.ldx = ldx;
         P.npad = (int)npad;
         P.opad = t.opad;
@@ -546,8 +567,9 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         // stage 2: K += X X^T over this chunk, split over k
         const int bn2 = 256 <= npad ? 256 : 128;
         CUtensorMap mXh, mXl, mXh2, mXl2;
+        // B operand: X diag(sign) when the factor is signed
         if (!make_map(&mXh, xh, npad, ldx, BM) || !make_map(&mXl, xl, npad, ldx, BM) ||
-            !make_map(&mXh2, xh, npad, ldx, bn2) || !make_map(&mXl2, xl, npad, ldx, bn2))
+            !make_map(&mXh2, sign ? xsh : xh, npad, ldx, bn2) || !make_map(&mXl2, sign ? xsl : xl, npad, ldx, bn2))
             return cudaErrorInvalidValue;
         TcParams Q{};
         Q.m_tiles = (int)(npad / BM);

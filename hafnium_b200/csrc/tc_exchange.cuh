@@ -21,9 +21,11 @@ TcPlan tc_plan(int64_t n, int naux, int64_t ncols);
 size_t tc_b_bytes(int64_t n, int naux);
 // Fill the BF16 hi/lo copies ([naux][npad][npad] each, hi first) from the FP64 tiles.
 cudaError_t tc_split_b(const JkPlan& p, int64_t npad, void* bf16_b, cudaStream_t stream);
-// K = sum_q (B_q C)(B_q C)^T with split-BF16 products; Ct_fp64 is [opad][npad] (zero padded).
-// work holds the BF16 factor and one chunk of X; Kp is npad x npad scratch.
+// K = sum_q (B_q C) diag(sign) (B_q C)^T with split-BF16 products; Ct_fp64 is
+// [opad][npad] (zero padded), sign [opad] device or null for all +1. work holds
+// the BF16 factor and one chunk of X (and of X diag(sign)); Kp is npad x npad scratch.
 cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const double* Ct_fp64, int64_t ct_ld, double* K,
-                                double* Kp, void* work, size_t work_bytes, int* d_err, cudaStream_t stream, int64_t n);
+                                double* Kp, void* work, size_t work_bytes, int* d_err, cudaStream_t stream, int64_t n,
+                                const double* sign = nullptr);
 
 }  // namespace hf

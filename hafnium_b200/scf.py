@@ -353,10 +353,10 @@ class _Rhf:
         return out
 
     def difference_factors(self, factor):
-        """(P, N) with D_n - D_a = P P^T - N N^T, from a thin QR of [C_n, C_a]:
-        [C_n, C_a] = Q R, D_n - D_a = Q (R S R^T) Q^T with S = diag(I, -I), and
-        the small middle matrix diagonalised; eigenvalues below
-        ``drop_tolerance`` of the largest are dropped."""
+        """(V, s) with D_n - D_a = V diag(s) V^T, s = +-1, from a thin QR of
+        [C_n, C_a]: [C_n, C_a] = Q R, D_n - D_a = Q (R S R^T) Q^T with
+        S = diag(I, -I), and the small middle matrix diagonalised; eigenvalues
+        below ``drop_tolerance`` of the largest are dropped."""
         torch = self.torch
         m = torch.cat([factor, self.anchor_factor], dim=1)
         q, r = torch.linalg.qr(m)
@@ -367,9 +367,8 @@ class _Rhf:
         w, u = torch.linalg.eigh(0.5 * (t + t.T))
         v = q @ u
         cut = self.schedule.drop_tolerance * float(w.abs().max())
-        pos, neg = w > cut, w < -cut
-        return (v[:, pos] * torch.sqrt(w[pos])[None, :]).contiguous(), \
-            (v[:, neg] * torch.sqrt(-w[neg])[None, :]).contiguous()
+        keep = w.abs() > cut
+        return (v[:, keep] * torch.sqrt(w[keep].abs())[None, :]).contiguous(), torch.sign(w[keep]).contiguous()
 
     def exchange(self, d, factor, precision: str):
         """K for this iteration in the arithmetic ``precision`` names: ``fp64``,
@@ -387,15 +386,13 @@ class _Rhf:
             if factor is None:
                 return self._timed("bf16", lambda: two_body.context_exchange_bf16(d))
             return self._timed("bf16", lambda: two_body.exchange_factored(factor, precision=_lib.PREC_BF16X3))
-        pos, neg = self.difference_factors(factor)
+        v, sign = self.difference_factors(factor)
 
         def increment():
-            out = self.anchor_k.clone()
-            if pos.shape[1]:
-                out += two_body.exchange_factored(pos, precision=_lib.PREC_BF16X3)
-            if neg.shape[1]:
-                out -= two_body.exchange_factored(neg, precision=_lib.PREC_BF16X3)
-            return out
+            # one signed split-BF16 build over both parts of the difference density
+            if v.shape[1] == 0:
+                return self.anchor_k.clone()
+            return self.anchor_k + two_body.exchange_factored(v, sign, precision=_lib.PREC_BF16X3)
 
         return self._timed("incremental", increment)
 

@@ -106,7 +106,8 @@ int hf_coulomb_static(hf_ctx* ctx, const double* density, double* coulomb);
  * HF_ERR_NUMERIC when D is indefinite (use hf_exchange_factored then). */
 int hf_exchange(hf_ctx* ctx, const double* density, double* exchange, int precision, int on_device);
 
-/* K for D = C diag(w) C^T with C [n_ao][n_cols] row-major (w = NULL: all ones). */
+/* K for D = C diag(w) C^T with C [n_ao][n_cols] row-major (w = NULL: all ones);
+ * weights of either sign, in both precisions. */
 int hf_exchange_factored(hf_ctx* ctx, const double* factor, int64_t n_cols, const double* weights,
                          double* exchange, int precision, int on_device);
 

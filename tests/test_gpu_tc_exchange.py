@@ -49,9 +49,18 @@ def test_bf16_exchange_from_a_density(two_body):
     assert np.max(np.abs(k16 - k64)) <= REL_TOL * np.max(np.abs(k64))
 
 
-def test_bf16_rejects_negative_weights(two_body):
-    from hafnium_b200.errors import InputError
-
-    c = np.ones((two_body.n_ao, 2))
-    with pytest.raises(InputError, match="non-negative"):
-        two_body.context.exchange_factored_host(c, np.array([1.0, -1.0]), _lib.PREC_BF16X3)
+def test_bf16_signed_factor_matches_fp64(two_body):
+    """D = C diag(w) C^T with weights of both signs (the incremental builds'
+    difference densities): one split-BF16 build against the FP64 one, the error
+    relative to the larger of the positive and negative parts."""
+    rng = np.random.default_rng(11)
+    k = 20
+    c = rng.normal(size=(two_body.n_ao, 2 * k)) / np.sqrt(two_body.n_ao * k)
+    w = np.concatenate([np.full(k, 1.0), np.full(k, -0.7)])
+    ctx = two_body.context
+    k64 = ctx.exchange_factored_host(c, w, _lib.PREC_FP64)
+    k16 = ctx.exchange_factored_host(c, w, _lib.PREC_BF16X3)
+    scale = max(np.max(np.abs(ctx.exchange_factored_host(c[:, :k], None, _lib.PREC_FP64))),
+                0.7 * np.max(np.abs(ctx.exchange_factored_host(c[:, k:], None, _lib.PREC_FP64))))
+    assert np.max(np.abs(k16 - k64)) <= REL_TOL * scale
+    np.testing.assert_allclose(k16, k16.T, atol=0, rtol=0)
