@@ -11,9 +11,9 @@ the stand-in for the unavailable cc-pVDZ-JKFIT). B is tens of GB, far above
 the 126 MB L2, so no flush is needed between steps.
 
 ``value`` is the device-timed (CUDA events) time-to-converge, max over ranks;
-``e2e`` is the same SCF with every J and K going through the drop-in's host
-NumPy API (host -> device copy of D, device -> host of J and K inside the
-timed region). Several GPUs run independent replicas (no collective on the
+``e2e`` is the same learned + mixed SCF with every J and K going through the
+drop-in's host NumPy API (host -> device copy of D or of its factor, device ->
+host of J and K inside the timed region). Several GPUs run independent replicas (no collective on the
 path). ``--impl reference`` times the reference's CPU path (the oracle's
 restatement: NumPy/OpenBLAS DF-RHF over C++/OpenMP integrals) on the host cores.
 """
@@ -249,12 +249,14 @@ def run_b200(args) -> None:
     if not args.no_e2e:
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        info = one_scf(torch, mol, dev, host_io=True, mode="fp64")
+        info = one_scf(torch, mol, dev, host_io=True, mode="mixed", guess_kind=guess_kind)
         torch.cuda.synchronize(dev)
         e2e_s = time.perf_counter() - t0
         e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": info["scf"]["h2d_bytes"],
                "d2h_bytes_per_step": info["scf"]["d2h_bytes"], "energy": info["energy"],
-               "path": "reference-facing host NumPy coulomb()/exchange() calls (FP64 exchange)"}
+               "path": "learned guess + mixed schedule with every J and K through the drop-in's host NumPy "
+                       "entry points (host -> device copy of D or of the factor, device -> host of J and K)",
+               "iterations": info["iterations"]}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -300,6 +300,38 @@ def learned_density_guess(molecule, ham: DeviceHamiltonian, *, weights=None, bas
     return project_occupied(ham, predicted)
 
 
+class _HostTwoBody:
+    """The drop-in's host-array API (coulomb_exchange.py:176-190) seen from the
+    device driver: device inputs are copied to host NumPy arrays, passed to the
+    builder's host entry points, and the results copied back; the bytes each way
+    are counted on the driver."""
+
+    def __init__(self, two_body, rhf) -> None:
+        self.two_body, self.rhf = two_body, rhf
+
+    def _down(self, t):
+        a = t.detach().cpu().numpy()
+        self.rhf.h2d_bytes += a.nbytes
+        return a
+
+    def _up(self, a, device):
+        self.rhf.d2h_bytes += a.nbytes
+        return _torch().as_tensor(a, device=device)
+
+    def coulomb(self, d):
+        return self._up(self.two_body.coulomb(self._down(d)), d.device)
+
+    def exchange(self, d):
+        return self._up(self.two_body.exchange(self._down(d)), d.device)
+
+    def exchange_factored(self, factor, weights=None, precision=None):
+        w = None if weights is None else self._down(weights)
+        return self._up(self.two_body.exchange_factored(self._down(factor), w, precision), factor.device)
+
+    def context_exchange_bf16(self, d):
+        return self._up(self.two_body.context.exchange_host(self._down(d), _lib.PREC_BF16X3), d.device)
+
+
 class _Rhf:
     def __init__(self, ham: DeviceHamiltonian, options: ScfOptions, schedule: PrecisionSchedule,
                  host_io: bool = False, averaged: bool = False) -> None:
@@ -370,11 +402,11 @@ class _Rhf:
         keep = w.abs() > cut
         return (v[:, keep] * torch.sqrt(w[keep].abs())[None, :]).contiguous(), torch.sign(w[keep]).contiguous()
 
-    def exchange(self, d, factor, precision: str):
+    def exchange(self, d, factor, precision: str, two_body=None):
         """K for this iteration in the arithmetic ``precision`` names: ``fp64``,
         ``bf16`` (split-BF16 from the orbitals), ``anchor`` (FP64, kept as the
         base of the increments) or ``incremental``."""
-        two_body = self.ham.two_body
+        two_body = two_body or self.ham.two_body
         if precision in ("fp64", "anchor"):
             k = self._timed("fp64", lambda: two_body.exchange(d) if factor is None else
                             two_body.exchange_factored(factor))
@@ -402,14 +434,11 @@ class _Rhf:
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         ev[0].record()
         if self.host_io:
-            # the reference-facing call: host NumPy density in, host NumPy J/K out
-            d_host = d.cpu().numpy()
-            j = torch.as_tensor(self.ham.two_body.coulomb(2.0 * d_host), device=d.device)
+            # the reference-facing calls: host NumPy arrays in, host NumPy J/K out
+            host = _HostTwoBody(self.ham.two_body, self)
+            j = host.coulomb((2.0 * d).contiguous())
             ev[1].record()
-            k = torch.as_tensor(self.ham.two_body.exchange(d_host), device=d.device)
-            nb = d_host.nbytes
-            self.h2d_bytes += 2 * nb
-            self.d2h_bytes += 2 * nb
+            k = self.exchange(d, factor, precision, host)
         else:
             j = self.ham.two_body.coulomb((2.0 * d).contiguous())
             ev[1].record()

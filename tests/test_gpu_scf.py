@@ -52,3 +52,35 @@ def test_sad_started_scf_follows_the_reference_iterations(tag):
     assert result.n_iterations == int(ref["n_iterations"])
     np.testing.assert_allclose([h.energy for h in result.history], ref["history"], atol=1e-8, rtol=0)
     assert abs(result.energy - float(ref["energy"])) <= 1e-8
+
+
+@pytest.mark.parametrize("tag", ["h2o4_s1", "h2o8_s2"])
+def test_mixed_schedule_matches_reference(tag):
+    """Split-BF16 builds, an FP64 anchor, incremental builds on the signed difference
+    density, then FP64: the reference's converged FP64 energy and density."""
+    from hafnium_b200.scf import PrecisionSchedule, atomic_density_guess
+
+    ref = golden(f"reference_dfrhf_{tag}.npz")
+    mol = molecule(tag)
+    ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
+    result = solve_rhf(ham, guess=atomic_density_guess(mol, "cc-pvdz"),
+                       options=ScfOptions(energy_tolerance=1e-11, gradient_tolerance=1e-8),
+                       schedule=PrecisionSchedule(mode="mixed"))
+    assert result.converged
+    assert {"bf16", "incremental", "fp64"} <= {h.precision for h in result.history}
+    assert abs(result.energy - float(ref["energy"])) <= 1e-8
+    assert np.max(np.abs(result.density.cpu().numpy() - ref["density"])) <= 1e-6
+
+
+def test_host_array_path_matches_the_device_path():
+    """Every J and K through the drop-in's host NumPy entry points (what the
+    reference's driver calls) gives the device path's converged energy."""
+    from hafnium_b200.scf import PrecisionSchedule, atomic_density_guess
+
+    mol = molecule("h2o4_s1")
+    ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
+    guess = atomic_density_guess(mol, "cc-pvdz")
+    device = solve_rhf(ham, guess=guess, schedule=PrecisionSchedule(mode="mixed"))
+    host = solve_rhf(ham, guess=guess, schedule=PrecisionSchedule(mode="mixed"), host_io=True)
+    assert abs(host.energy - device.energy) <= 1e-8
+    assert host.timings["h2d_bytes"] > 0 and host.timings["d2h_bytes"] > 0
