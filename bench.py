@@ -184,7 +184,8 @@ def one_scf(torch, mol, dev, host_io=False, mode="mixed", guess_kind="sad", prob
            "scf": {**result.timings, "guess_s": t_guess, "scf_s": result.seconds, "hamiltonian_s": t_ham},
            "launches": stats["kernel_launches"], "n_ao": ham.n_ao,
            "n_aux": ham.two_body.n_aux, "b_bytes": stats["b_bytes"],
-           "precisions": [h.precision for h in result.history], "kernel_ms": kernel_ms}
+           "precisions": [h.precision for h in result.history], "kernel_ms": kernel_ms,
+           "density": result.density.detach().cpu().numpy()}
     t_free = time.perf_counter()
     del ham, result
     torch.cuda.empty_cache()
@@ -331,7 +332,8 @@ def run_b200(args) -> None:
         "step_times_s": times,
         "plain_fp64": {"value": plain_max, "step_times_s": plain_times, "energy": plain["energy"],
                        "iterations": plain["iterations"], "speedup_of_mixed": plain_max / step_max,
-                       "dE_mixed_vs_fp64": last["energy"] - plain["energy"]},
+                       "dE_mixed_vs_fp64": last["energy"] - plain["energy"],
+                       "max_abs_dD_mixed_vs_fp64": float(np.max(np.abs(last["density"] - plain["density"])))},
         "stages": {"build": last["build"], "per_build_ms": {"coulomb": j_ms, "exchange_fp64": k64_ms,
                                                              "exchange_bf16_kernel": k16_ms,
                                                              "exchange_fp64_kernel": k64_probe_ms,
