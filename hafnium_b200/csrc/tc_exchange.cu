@@ -337,6 +337,7 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
                     __nv_bfloat16* dh = P.xh + (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
                     __nv_bfloat16* dl = P.xl + (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
                     if (row < P.m_tiles * BM) {
+                        const int64_t off = (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
 #pragma unroll
                         for (int j = 0; j < 16; j += 2) {
                             const __nv_bfloat16 h0 = __float2bfloat16_rn(v[j]), h1 = __float2bfloat16_rn(v[j + 1]);
@@ -344,16 +345,13 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
                             const __nv_bfloat16 l1 = __float2bfloat16_rn(v[j + 1] - __bfloat162float(h1));
                             *reinterpret_cast<__nv_bfloat162*>(dh + j) = __halves2bfloat162(h0, h1);
                             *reinterpret_cast<__nv_bfloat162*>(dl + j) = __halves2bfloat162(l0, l1);
-                        }
-                        if (P.xsh) {
-                            // negating both parts negates the split value exactly
-                            const int64_t off = (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
-#pragma unroll
-                            for (int j = 0; j < 16; ++j) {
-                                const __nv_bfloat16 h = dh[j], l = dl[j];
-                                const bool neg = P.sign[i0 + j] < 0.0;
-                                P.xsh[off + j] = neg ? __hneg(h) : h;
-                                P.xsl[off + j] = neg ? __hneg(l) : l;
+                            if (P.xsh) {
+                                // negating both parts negates the split value exactly
+                                const bool n0 = P.sign[i0 + j] < 0.0, n1 = P.sign[i0 + j + 1] < 0.0;
+                                *reinterpret_cast<__nv_bfloat162*>(P.xsh + off + j) =
+                                    __halves2bfloat162(n0 ? __hneg(h0) : h0, n1 ? __hneg(h1) : h1);
+                                *reinterpret_cast<__nv_bfloat162*>(P.xsl + off + j) =
+                                    __halves2bfloat162(n0 ? __hneg(l0) : l0, n1 ? __hneg(l1) : l1);
                             }
                         }
                     }

@@ -421,10 +421,16 @@ class _Rhf:
         v, sign = self.difference_factors(factor)
 
         def increment():
-            # one signed split-BF16 build over both parts of the difference density
-            if v.shape[1] == 0:
-                return self.anchor_k.clone()
-            return self.anchor_k + two_body.exchange_factored(v, sign, precision=_lib.PREC_BF16X3)
+            # the positive and negative parts as two unsigned split-BF16 builds: with
+            # n_occ columns each they keep the X chunks large (a single signed build
+            # over 2 n_occ columns measured 2.6x slower at (H2O)64)
+            out = self.anchor_k.clone()
+            pos, neg = sign > 0, sign < 0
+            if bool(pos.any()):
+                out += two_body.exchange_factored(v[:, pos].contiguous(), precision=_lib.PREC_BF16X3)
+            if bool(neg.any()):
+                out -= two_body.exchange_factored(v[:, neg].contiguous(), precision=_lib.PREC_BF16X3)
+            return out
 
         return self._timed("incremental", increment)
 
