@@ -48,6 +48,7 @@ class ScfOptions:
     gradient_tolerance: float = 1e-6
     diis_size: int = 8
     overlap_threshold: float = DEFAULT_OVERLAP_THRESHOLD
+    purify: bool = True  # density by purification after the first iteration (same projector)
 
     def __post_init__(self) -> None:
         if self.max_iterations < 1:
@@ -194,6 +195,45 @@ def solve_diis(overlaps: np.ndarray) -> np.ndarray:
     keep = np.abs(w) > NULL_SPACE_TOLERANCE * np.max(np.abs(w))
     inv = np.where(keep, 1.0 / np.where(keep, w, 1.0), 0.0)
     return (v @ (inv * (v.T @ right)))[:m]
+
+
+def purify(fo, n_occ: int, tolerance: float = 1e-9, max_steps: int = 100):
+    """Canonical purification of a symmetric matrix ``fo`` (orthonormal basis) to
+    the projector onto its n_occ lowest eigenvectors (Palser and Manolopoulos,
+    PRB 58, 12704 (1998), eq. 13-16): P0 from Gershgorin bounds, then
+    P <- (P^2 ((1 + c) I - P)) / c or its c < 1/2 form, c = tr(P^2 - P^3) / tr(P - P^2),
+    until tr(P - P^2) < tolerance, plus one more (quadratic) step. Returns
+    (P, converged)."""
+    torch = _torch()
+    m = fo.shape[0]
+    diag = torch.diagonal(fo)
+    radius = fo.abs().sum(dim=1) - diag.abs()
+    lo, hi, mu = float((diag - radius).min()), float((diag + radius).max()), float(diag.sum()) / m
+    if not (hi > mu > lo) or not 0 < n_occ < m:
+        return fo, False
+    lam = min(n_occ / (hi - mu), (m - n_occ) / (mu - lo))
+    eye = torch.eye(m, dtype=fo.dtype, device=fo.device)
+    p = (lam / m) * (mu * eye - fo) + (n_occ / m) * eye
+    crossed = False
+    for _ in range(max_steps):
+        p2 = p @ p
+        t1 = float(torch.diagonal(p).sum() - torch.diagonal(p2).sum())
+        t2 = float(torch.diagonal(p2).sum() - (p2 * p).sum())
+        if crossed:
+            return 0.5 * (p + p.T), True
+        if t1 < tolerance:
+            crossed = True
+        if t1 > 0.0:
+            c = min(1.0, max(0.0, t2 / t1))
+        elif abs(t1) < tolerance:
+            c = 0.5
+        else:
+            return p, False
+        if c >= 0.5:
+            p = p2 @ (((1.0 + c) * eye - p) / c)
+        else:
+            p = p2 @ (((1.0 + c) * eye - p) / (1.0 - c)) + ((1.0 - 2.0 * c) / (1.0 - c)) * p
+    return p, False
 
 
 def fill_averaged(energies: np.ndarray, count: float, tolerance: float = 1e-6) -> np.ndarray:
@@ -346,6 +386,8 @@ class _Rhf:
         self.schedule = schedule
         self.x = ham.orthogonalizer(options.overlap_threshold)
         self.n = ham.n_ao
+        self.z = None  # occupied orbitals of the last iteration, orthonormal basis
+        self.purify = options.purify
         self.anchor_k = None  # K64(D_a) of the last FP64 anchor
         self.anchor_factor = None  # C_a with D_a = C_a C_a^T
         self.timings = {"coulomb_ms": 0.0, "exchange_ms": 0.0, "eigh_ms": 0.0, "fock_builds": 0}
@@ -360,6 +402,42 @@ class _Rhf:
         e1.synchronize()
         self.timings["eigh_ms"] += e0.elapsed_time(e1)
         return w, c
+
+    def next_density(self, f):
+        """(D, C) of the aufbau state of Fock matrix ``f``: the reference's
+        eigensolve (driver.py:307-329) on the first iteration, afterwards canonical
+        purification (Palser and Manolopoulos, PRB 58, 12704 (1998)) of X^T f X on
+        the tensor cores and the occupied orbitals as the span of P Z, Z the
+        previous occupied orbitals, orthonormalised by a Cholesky factor. With a
+        HOMO-LUMO gap both give the same projector; without one, or when P Z loses
+        rank, the eigensolve is used."""
+        torch = self.torch
+        if self.averaged or self.z is None or not self.purify:
+            w, c = self.solve(f)
+            d, factor = self.density(w, c, averaged=False)
+            self.z = self.x.T @ self.ham.s @ factor  # the occupied orbitals in the orthonormal basis
+            return d, factor
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fo = self.x.T @ f @ self.x
+        p, ok = purify(0.5 * (fo + fo.T), int(self.ham.n_alpha))
+        if ok:
+            y = p @ self.z
+            g = y.T @ y
+            low, info = torch.linalg.cholesky_ex(0.5 * (g + g.T))
+            ok = int(info) == 0 and float(torch.diagonal(low).min()) > 1e-3
+        if ok:
+            z = torch.linalg.solve_triangular(low, y.T, upper=False).T.contiguous()
+            self.z = z
+            factor = (self.x @ z).contiguous()
+        e1.record()
+        e1.synchronize()
+        self.timings["purify_ms"] = self.timings.get("purify_ms", 0.0) + e0.elapsed_time(e1)
+        if not ok:
+            self.timings["purify_fallbacks"] = self.timings.get("purify_fallbacks", 0) + 1
+            self.z = None
+            return self.next_density(f)
+        return factor @ factor.T, factor
 
     def density(self, w, c, averaged: bool):
         if averaged or self.averaged:
@@ -529,8 +607,7 @@ class _Rhf:
                 ov = torch.stack([torch.stack([2.0 * torch.sum(a * b) for b in errors]) for a in errors]).cpu().numpy()
                 coef = solve_diis(ov)
                 extrapolated = sum(float(cf) * fk for cf, fk in zip(coef, focks))
-            w, c = self.solve(extrapolated)
-            d, factor = self.density(w, c, averaged=False)
+            d, factor = self.next_density(extrapolated)
         result = self.finish(focks[-1] if focks else f, history, False, t_start)
         raise ConvergenceError(f"the SCF did not converge in {opts.max_iterations} iterations", result)
 

@@ -59,3 +59,30 @@ def test_diis_and_filling_match_the_oracle():
     np.testing.assert_allclose(solve_diis(ov), dfrhf.solve_diis(ov), atol=1e-14)
     e = np.array([-3.0, -1.0, 0.5, 0.5 + 1e-9, 0.5 - 1e-9, 2.0])
     np.testing.assert_allclose(fill_averaged(e, 3.0), dfrhf.fill_averaged(e, 3.0), atol=0)
+
+
+def test_purification_gives_the_aufbau_projector():
+    """scf.purify on the CPU: the projector onto the n_occ lowest eigenvectors."""
+    import torch
+
+    from hafnium_b200.scf import purify
+
+    rng = np.random.default_rng(5)
+    q, _ = np.linalg.qr(rng.normal(size=(60, 60)))
+    levels = np.concatenate([np.sort(rng.uniform(-20.0, -0.4, 17)), np.sort(rng.uniform(0.2, 5.0, 43))])
+    fo = (q * levels) @ q.T
+    p, ok = purify(torch.as_tensor(fo), 17)
+    assert ok
+    expected = q[:, :17] @ q[:, :17].T
+    np.testing.assert_allclose(p.numpy(), expected, atol=1e-11, rtol=0)
+
+
+def test_purification_reports_a_missing_gap():
+    import torch
+
+    from hafnium_b200.scf import purify
+
+    fo = np.diag(np.concatenate([np.full(3, -1.0), np.full(3, 0.5)]))
+    fo[2, 2] = fo[3, 3] = 0.0  # degenerate HOMO/LUMO: no projector of rank 3 is singled out
+    p, ok = purify(torch.as_tensor(fo), 3)
+    assert not ok or abs(float(torch.trace(p)) - 3.0) < 1e-8
