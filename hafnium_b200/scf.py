@@ -48,7 +48,7 @@ class ScfOptions:
     gradient_tolerance: float = 1e-6
     diis_size: int = 8
     overlap_threshold: float = DEFAULT_OVERLAP_THRESHOLD
-    purify: bool = True  # density by purification after the first iteration (same projector)
+    purify: bool = False  # density by purification after the first iteration (same projector)
 
     def __post_init__(self) -> None:
         if self.max_iterations < 1:
