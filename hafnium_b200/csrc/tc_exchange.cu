@@ -375,28 +375,53 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
 }
 
 // Full BF16 hi/lo copies of B: Bh[q][p][r] from the FP64 upper-tile packing.
-__global__ void k_split_b_full(const double* __restrict__ B, int64_t ldb, int nt, int npad, int q0, int qc,
-                               __nv_bfloat16* __restrict__ bh, __nv_bfloat16* __restrict__ bl) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t per_q = (int64_t)npad * npad;
-    if (e >= per_q * qc) return;
-    const int ql = (int)(e / per_q);
-    const int64_t rem = e % per_q;
-    int p = (int)(rem / npad), r = (int)(rem % npad);
-    int I = p >> 6, J = r >> 6, a = p & 63, b = r & 63;
-    if (I > J) {
-        const int t = I;
-        I = J;
-        J = t;
-        const int u = a;
-        a = b;
-        b = u;
+// One CTA per (packed tile (I, J), q): the 64x64 FP64 tile is read once with
+// 16-byte loads, staged in shared memory, and written as the (I, J) block and,
+// off the diagonal, the transposed (J, I) block, 128-byte rows of BF16 pairs.
+// Only the nt(nt+1)/2 packed tiles are read; rows and columns beyond nt*64
+// (when npad > nt*64) are zeroed by the host beforehand.
+__global__ void __launch_bounds__(256) k_split_b_tiles(const double* __restrict__ B, int64_t ldb, int nt,
+                                                       int npad, int q0, __nv_bfloat16* __restrict__ bh,
+                                                       __nv_bfloat16* __restrict__ bl) {
+    __shared__ double s[64][65];
+    const int tile = blockIdx.x;
+    const int ql = blockIdx.y;
+    int I = 0, rem = tile;
+    while (rem >= nt - I) {
+        rem -= nt - I;
+        ++I;
     }
-    const int64_t tile = (int64_t)I * nt - (int64_t)I * (I - 1) / 2 + (J - I);
-    const double x = B[(int64_t)(q0 + ql) * ldb + tile * 4096 + a * 64 + b];
-    const __nv_bfloat16 h = __double2bfloat16(x);
-    bh[e] = h;
-    bl[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+    const int J = I + rem;
+    const double2* src = reinterpret_cast<const double2*>(B + (int64_t)(q0 + ql) * ldb + (int64_t)tile * 4096);
+    for (int k = threadIdx.x; k < 2048; k += 256) {
+        const double2 v = src[k];
+        const int a = (2 * k) >> 6, b = (2 * k) & 63;
+        s[a][b] = v.x;
+        s[a][b + 1] = v.y;
+    }
+    __syncthreads();
+    const int64_t base = (int64_t)ql * npad * npad;
+    for (int k = threadIdx.x; k < 2048; k += 256) {
+        const int a = k >> 5, b = (k & 31) * 2;
+        const double x0 = s[a][b], x1 = s[a][b + 1];
+        const __nv_bfloat162 h = __halves2bfloat162(__double2bfloat16(x0), __double2bfloat16(x1));
+        const __nv_bfloat162 l = __halves2bfloat162(__double2bfloat16(x0 - (double)__low2float(h)),
+                                                    __double2bfloat16(x1 - (double)__high2float(h)));
+        const int64_t o = base + (int64_t)(I * 64 + a) * npad + J * 64 + b;
+        *reinterpret_cast<__nv_bfloat162*>(bh + o) = h;
+        *reinterpret_cast<__nv_bfloat162*>(bl + o) = l;
+    }
+    if (I == J) return;
+    for (int k = threadIdx.x; k < 2048; k += 256) {
+        const int a = k >> 5, b = (k & 31) * 2;
+        const double x0 = s[b][a], x1 = s[b + 1][a];
+        const __nv_bfloat162 h = __halves2bfloat162(__double2bfloat16(x0), __double2bfloat16(x1));
+        const __nv_bfloat162 l = __halves2bfloat162(__double2bfloat16(x0 - (double)__low2float(h)),
+                                                    __double2bfloat16(x1 - (double)__high2float(h)));
+        const int64_t o = base + (int64_t)(J * 64 + a) * npad + I * 64 + b;
+        *reinterpret_cast<__nv_bfloat162*>(bh + o) = h;
+        *reinterpret_cast<__nv_bfloat162*>(bl + o) = l;
+    }
 }
 
 // C^T in FP64 ([opad][npad]) -> BF16 hi/lo.
@@ -495,12 +520,16 @@ cudaError_t tc_split_b(const JkPlan& p, int64_t npad, void* bf16_b, cudaStream_t
     __nv_bfloat16* bh = static_cast<__nv_bfloat16*>(bf16_b);
     const int64_t per_q = npad * npad;
     __nv_bfloat16* bl = bh + per_q * p.naux;
-    const int qblock = 256;
+    if (npad > (int64_t)p.nt * 64) {
+        cudaError_t e = cudaMemsetAsync(bf16_b, 0, tc_b_bytes(npad, p.naux), stream);
+        if (e != cudaSuccess) return e;
+    }
+    const int ntiles = p.nt * (p.nt + 1) / 2;
+    const int qblock = 65535;
     for (int q0 = 0; q0 < p.naux; q0 += qblock) {
         const int qc = std::min(qblock, p.naux - q0);
-        const int64_t total = per_q * qc;
-        k_split_b_full<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(p.B, p.ldb, p.nt, (int)npad, q0, qc,
-                                                                             bh + per_q * q0, bl + per_q * q0);
+        k_split_b_tiles<<<dim3(ntiles, qc), 256, 0, stream>>>(p.B, p.ldb, p.nt, (int)npad, q0, bh + per_q * q0,
+                                                             bl + per_q * q0);
     }
     return cudaGetLastError();
 }

@@ -391,3 +391,95 @@ def df_mp2(b: np.ndarray, mo_energies: np.ndarray, mo_coefficients: np.ndarray, 
         denom = eo[i] + eo[:, None, None] - ev[None, :, None] - ev[None, None, :]
         total += float(np.sum(iajb * (2.0 * iajb - iajb.transpose(0, 2, 1)) / denom))
     return total
+
+
+# ------------------------------------------------------------ nuclear gradient
+def functions_by_atom(table, positions: np.ndarray) -> np.ndarray:
+    """gradient.py:158-168: ``[atom, ao]`` with one where the function sits on the atom.
+
+    The reference reads the atom from each function's label; a molecular shell
+    table carries the atom's position as the shell centre, so the atom is the
+    one at that centre.
+    """
+    rows = []
+    counts = getattr(table, "n_contractions", None)
+    if counts is None:
+        counts = table.contraction_counts
+    for sh in range(len(table.angular_momenta)):
+        dist = np.linalg.norm(np.asarray(positions) - np.asarray(table.centers[sh]), axis=1)
+        atom = int(np.argmin(dist))
+        if dist[atom] > 1e-10:
+            raise ValueError(f"shell {sh} sits on no atom")
+        rows += [atom] * (int(counts[sh]) * (2 * int(table.angular_momenta[sh]) + 1))
+    out = np.zeros((len(positions), len(rows)))
+    out[rows, np.arange(len(rows))] = 1.0
+    return out
+
+
+def _on_centers(derivative, weights, atoms):
+    """gradient.py:171-178: 2 sum_{u on K} sum_v d[x,u,v] w[v,u] as [atom, 3]."""
+    rows = 2.0 * np.einsum("xuv,vu->xu", derivative, weights)
+    return (rows @ atoms.T).T
+
+
+def _two_electron(metric_d, aux_d, orb_d, effective, metric_weights, atoms, aux_atoms):
+    """gradient.py:181-203: gradient of sum_P tr(L_P G_P) + tr(M W) at fixed G and W."""
+    symmetric = effective + np.transpose(effective, (0, 2, 1))
+    on_auxiliary = np.einsum("xPuv,Puv->xP", aux_d, effective, optimize=True)
+    on_auxiliary = on_auxiliary + 2.0 * np.einsum("xPQ,PQ->xP", metric_d, metric_weights)
+    on_orbital = np.einsum("xPuv,Puv->xu", orb_d, symmetric, optimize=True)
+    return (on_auxiliary @ aux_atoms.T + on_orbital @ atoms.T).T
+
+
+def nuclear_repulsion_gradient(charges, positions) -> np.ndarray:
+    """gradient.py:222-235: -sum_{L != K} Z_K Z_L (R_K - R_L) / |R_K - R_L|^3."""
+    pos = np.asarray(positions, dtype=np.float64)
+    z = np.asarray(charges, dtype=np.float64)
+    sep = pos[:, None, :] - pos[None, :, :]
+    dist = np.sqrt(np.sum(sep**2, axis=-1))
+    eye = np.eye(len(z)) > 0
+    w = np.where(eye, 0.0, z[:, None] * z[None, :] / np.where(eye, 1.0, dist) ** 3)
+    return -np.sum(w[:, :, None] * sep, axis=1)
+
+
+def nuclear_gradient(orb, aux, charges, positions, d_alpha, fock) -> dict:
+    """gradient.py:72-149 for a restricted state: the five terms, each [atom, 3].
+
+    ``d_alpha`` and ``fock`` are the converged alpha density and Fock matrix;
+    the spin traces are ``total = 2 D`` and ``weighted = 2 D F D``, and the
+    exchange pairs of the spin-orbital density reduce to ``T_Q = 2 D L_Q D``.
+    """
+    o, a = kernel_table(orb), kernel_table(aux)
+    z3 = np.zeros((1, 3))
+    total = 2.0 * d_alpha
+    weighted = 2.0 * d_alpha @ fock @ d_alpha
+    atoms = functions_by_atom(orb, positions)
+    aux_atoms = functions_by_atom(aux, positions)
+    by_center, by_nucleus = kernels.nuclear_attraction_derivative(o, o, z3, charges, positions)
+    one_electron = _on_centers(kernels.kinetic_derivative(o, o, z3)[0] + by_center[0], total, atoms) + np.einsum(
+        "kxuv,vu->kx", by_nucleus[0], total
+    )
+    overlap_term = -_on_centers(kernels.overlap_derivative(o, o, z3)[0], weighted, atoms)
+    m = metric(aux)
+    t3 = three_center(aux, orb)
+    metric_d = kernels.coulomb_two_center_derivative(a, a, z3)[0]
+    aux_d, orb_d = kernels.coulomb_three_center_derivative(a, o, o, np.zeros((1, 2, 3)))
+    aux_d, orb_d = aux_d[0], orb_d[0]
+    half, _ = inverse_square_root(m)
+    inverse = half @ half
+    fitted_charges = np.einsum("Puv,vu->P", t3, total)
+    c = inverse @ fitted_charges
+    coulomb_term = _two_electron(metric_d, aux_d, orb_d, c[:, None, None] * total[None, :, :],
+                                 -0.5 * c[:, None] * c[None, :], atoms, aux_atoms)
+    pairs = 2.0 * np.einsum("uv,Pvw,wx->Pux", d_alpha, t3, d_alpha, optimize=True)
+    n = total.shape[0]
+    exchange_pairs = t3.reshape(-1, n * n) @ np.transpose(pairs, (0, 2, 1)).reshape(-1, n * n).T
+    exchange_term = _two_electron(metric_d, aux_d, orb_d, -np.einsum("PQ,Quv->Puv", inverse, pairs, optimize=True),
+                                  0.5 * inverse @ exchange_pairs @ inverse, atoms, aux_atoms)
+    return {
+        "nuclear_repulsion": nuclear_repulsion_gradient(charges, positions),
+        "one_electron": one_electron,
+        "overlap": overlap_term,
+        "coulomb": coulomb_term,
+        "exchange": exchange_term,
+    }

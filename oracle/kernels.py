@@ -15,6 +15,9 @@ lib.rs:1118), computed by ``oracle/md_oracle.cpp`` through ctypes:
 - ``overlap``, ``kinetic``, ``nuclear_attraction`` (lib.rs:111-186)
 - ``coulomb_two_center``, ``coulomb_three_center`` (lib.rs:352-423)
 - ``coulomb_four_center``, ``schwarz_bounds`` (lib.rs:503-562)
+- ``overlap_derivative``, ``kinetic_derivative``, ``nuclear_attraction_derivative``,
+  ``coulomb_two_center_derivative``, ``coulomb_three_center_derivative``
+  (hafnium/_kernels.pyi:71-140; two_electron.rs:132-394)
 - ``configure_threads`` (lib.rs:1110; integrals/mod.rs:43-49)
 """
 
@@ -63,6 +66,11 @@ def library() -> ctypes.CDLL:
         lib.md_coulomb_three_center.argtypes = [p, p, p, i64, d, ctypes.c_int, ctypes.c_double, d]
         lib.md_coulomb_four_center.argtypes = [p, p, p, p, i64, d, ctypes.c_int, ctypes.c_double, ctypes.c_double, d]
         lib.md_schwarz_bounds.argtypes = [p, p, i64, d, ctypes.c_int, ctypes.c_double, d]
+        lib.md_overlap_derivative.argtypes = [p, p, i64, d, d]
+        lib.md_kinetic_derivative.argtypes = [p, p, i64, d, d]
+        lib.md_nuclear_attraction_derivative.argtypes = [p, p, i64, d, i64, d, d, ctypes.c_int, ctypes.c_double, d, d]
+        lib.md_coulomb_two_center_derivative.argtypes = [p, p, i64, d, ctypes.c_int, ctypes.c_double, d]
+        lib.md_coulomb_three_center_derivative.argtypes = [p, p, p, i64, d, ctypes.c_int, ctypes.c_double, d]
         lib.md_set_threads.argtypes = [ctypes.c_int]
         lib.md_get_threads.restype = ctypes.c_int
         _lib = lib
@@ -263,6 +271,71 @@ def coulomb_three_center(auxiliary, bra, ket, translations, omega=None, short_ra
         )
     )
     return out
+
+
+def overlap_derivative(bra: ShellTable, ket: ShellTable, translations) -> np.ndarray:
+    """``<d_A mu | nu>`` as ``[image, 3, bra, ket]``."""
+    tr = _vectors(translations, "translations")
+    out = np.empty((tr.shape[0], 3, bra.n_functions, ket.n_functions))
+    _check(library().md_overlap_derivative(ctypes.byref(bra._struct), ctypes.byref(ket._struct), tr.shape[0], _ptr(tr),
+                                           _ptr(out)))
+    return out
+
+
+def kinetic_derivative(bra: ShellTable, ket: ShellTable, translations) -> np.ndarray:
+    """``<d_A mu | -1/2 nabla^2 | nu>`` as ``[image, 3, bra, ket]``."""
+    tr = _vectors(translations, "translations")
+    out = np.empty((tr.shape[0], 3, bra.n_functions, ket.n_functions))
+    _check(library().md_kinetic_derivative(ctypes.byref(bra._struct), ctypes.byref(ket._struct), tr.shape[0], _ptr(tr),
+                                           _ptr(out)))
+    return out
+
+
+def nuclear_attraction_derivative(bra, ket, translations, charges, positions, omega=None, short_range=False):
+    """By the bra centres ``[image, 3, bra, ket]`` and by the charge positions
+    ``[image, charge, 3, bra, ket]``."""
+    tr = _vectors(translations, "translations")
+    pos = _vectors(positions, "positions")
+    q = np.ascontiguousarray(charges, dtype=np.float64)
+    if q.shape[0] != pos.shape[0]:
+        raise ValueError(f"length mismatch: {q.shape[0]} and {pos.shape[0]}")
+    kind, w = _kernel(omega, short_range)
+    by_center = np.empty((tr.shape[0], 3, bra.n_functions, ket.n_functions))
+    by_nucleus = np.empty((tr.shape[0], q.shape[0], 3, bra.n_functions, ket.n_functions))
+    _check(
+        library().md_nuclear_attraction_derivative(
+            ctypes.byref(bra._struct), ctypes.byref(ket._struct), tr.shape[0], _ptr(tr), q.shape[0], _ptr(q), _ptr(pos),
+            kind, w, _ptr(by_center), _ptr(by_nucleus),
+        )
+    )
+    return by_center, by_nucleus
+
+
+def coulomb_two_center_derivative(bra, ket, translations, omega=None, short_range=False):
+    """``(d_P P | Q)`` as ``[image, 3, bra, ket]``."""
+    tr = _vectors(translations, "translations")
+    kind, w = _kernel(omega, short_range)
+    out = np.empty((tr.shape[0], 3, bra.n_functions, ket.n_functions))
+    _check(
+        library().md_coulomb_two_center_derivative(
+            ctypes.byref(bra._struct), ctypes.byref(ket._struct), tr.shape[0], _ptr(tr), kind, w, _ptr(out)
+        )
+    )
+    return out
+
+
+def coulomb_three_center_derivative(auxiliary, bra, ket, translations, omega=None, short_range=False):
+    """``(d_P P | uv)`` and ``(P | d_A u v)``, each ``[image, 3, aux, bra, ket]``."""
+    tr = _vector_sets(translations, 2)
+    kind, w = _kernel(omega, short_range)
+    out = np.empty((tr.shape[0], 6, auxiliary.n_functions, bra.n_functions, ket.n_functions))
+    _check(
+        library().md_coulomb_three_center_derivative(
+            ctypes.byref(auxiliary._struct), ctypes.byref(bra._struct), ctypes.byref(ket._struct), tr.shape[0],
+            _ptr(tr), kind, w, _ptr(out),
+        )
+    )
+    return np.ascontiguousarray(out[:, :3]), np.ascontiguousarray(out[:, 3:])
 
 
 def coulomb_four_center(bra, ket, translations, omega=None, short_range=False, threshold=0.0):

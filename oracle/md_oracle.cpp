@@ -409,6 +409,117 @@ std::vector<double> to_spherical(const std::vector<double>& block, const int ls[
 
 int nfunc(const ShellView& s) { return s.ncontr * (2 * s.l + 1); }
 
+// ------------------------------------------------------ derivative blocks
+// Derivatives of (ab|cd) as in the reference's coulomb_block_derivative
+// (two_electron.rs:1138-1247). A Hermite centre (the centre of a lone
+// function) by the shift of the Hermite integrals: d/dP R_tuv = R_{t+1,u,v}
+// for the bra pair and the negative for the ket pair, since R_PQ = P - Q. The
+// centre of the bra's first function by raising and lowering its angular
+// momentum: d/dA_x x_A^i exp(-a x_A^2) = 2a x_A^(i+1) exp(..) - i x_A^(i-1) exp(..),
+// for which the bra pair carries one extra order on its first function.
+enum Deriv : int { kBraHermite = 0, kKetHermite = 1, kBraFunction = 2 };
+
+struct HTerm {
+    int t, u, v;
+    double c;
+};
+
+// E^{ij}_t of one axis, with the raise/lower rule applied when `raise`.
+double axis_coef(const PrimPair& P, int axis, int i, int j, int t, bool raise) {
+    if (!raise) return P.e[axis].get(i, j, t);
+    double v = 2.0 * P.ea * P.e[axis].get(i + 1, j, t);
+    if (i > 0) v -= i * P.e[axis].get(i - 1, j, t);
+    return v;
+}
+
+// Hermite terms of the Cartesian pair (a, b); the first function differentiated
+// along `axis` when `raise`.
+void pair_terms(const PrimPair& P, const std::array<int, 3>& a, const std::array<int, 3>& b, bool raise, int axis,
+                double sign_per_order, std::vector<HTerm>& out) {
+    out.clear();
+    const int ext = raise ? 1 : 0;
+    for (int t = 0; t <= a[0] + b[0] + (axis == 0 ? ext : 0); ++t) {
+        const double ex = axis_coef(P, 0, a[0], b[0], t, raise && axis == 0);
+        if (ex == 0.0) continue;
+        for (int u = 0; u <= a[1] + b[1] + (axis == 1 ? ext : 0); ++u) {
+            const double ey = ex * axis_coef(P, 1, a[1], b[1], u, raise && axis == 1);
+            if (ey == 0.0) continue;
+            for (int v = 0; v <= a[2] + b[2] + (axis == 2 ? ext : 0); ++v) {
+                const double ez = ey * axis_coef(P, 2, a[2], b[2], v, raise && axis == 2);
+                if (ez == 0.0) continue;
+                const double sg = (sign_per_order < 0.0 && ((t + u + v) & 1)) ? -1.0 : 1.0;
+                out.push_back({t, u, v, sg * ez});
+            }
+        }
+    }
+}
+
+// out[axis] (layout of coulomb_block) += d/dX (ab|cd) for the centre `mode` selects;
+// for kBraFunction the bra pair must carry one extra order on its first function.
+void coulomb_block_derivative(const Pair& bra, const Pair& ket, const Transforms& tr, int kernel, double omega,
+                              int mode, RWork& w, std::vector<double>* out) {
+    const auto& ca = tr.comps[bra.la];
+    const auto& cb = tr.comps[bra.lb];
+    const auto& cc = tr.comps[ket.la];
+    const auto& cd = tr.comps[ket.lb];
+    const int na = (int)ca.size(), nb = (int)cb.size(), nc = (int)cc.size(), nd = (int)cd.size();
+    const int L = bra.la + bra.lb + ket.la + ket.lb + 1;
+    const int s1 = L + 1;
+    std::vector<double> R(s1 * s1 * s1);
+    std::vector<std::vector<HTerm>> kterms(nc * nd);
+    std::vector<HTerm> bt;
+    std::vector<double> val(3 * na * nb * nc * nd);
+    const int sc = ket.kb * nd, sb = ket.ka * nc * sc, sa = bra.kb * nb * sb;
+    const double hsign = mode == kKetHermite ? -1.0 : 1.0;
+    for (size_t ib = 0; ib < bra.prims.size(); ++ib) {
+        const PrimPair& P = bra.prims[ib];
+        for (size_t ik = 0; ik < ket.prims.size(); ++ik) {
+            const PrimPair& Q = ket.prims[ik];
+            const double p = P.p, q = Q.p;
+            const double alpha = p * q / (p + q);
+            const double pq[3] = {P.P[0] - Q.P[0], P.P[1] - Q.P[1], P.P[2] - Q.P[2]};
+            hermite_r_kernel(L, alpha, kernel, omega, pq, w, R.data());
+            for (int ic = 0; ic < nc; ++ic)
+                for (int id = 0; id < nd; ++id) pair_terms(Q, cc[ic], cd[id], false, 0, -1.0, kterms[ic * nd + id]);
+            for (int axis = 0; axis < 3; ++axis) {
+                const int dx = (mode != kBraFunction && axis == 0) ? 1 : 0;
+                const int dy = (mode != kBraFunction && axis == 1) ? 1 : 0;
+                const int dz = (mode != kBraFunction && axis == 2) ? 1 : 0;
+                for (int ia = 0; ia < na; ++ia)
+                    for (int jb = 0; jb < nb; ++jb) {
+                        pair_terms(P, ca[ia], cb[jb], mode == kBraFunction, axis, 1.0, bt);
+                        for (int icd = 0; icd < nc * nd; ++icd) {
+                            double v = 0.0;
+                            for (const HTerm& x : bt)
+                                for (const HTerm& y : kterms[icd])
+                                    v += x.c * y.c * R[((x.t + y.t + dx) * s1 + x.u + y.u + dy) * s1 + x.v + y.v + dz];
+                            val[((axis * na + ia) * nb + jb) * nc * nd + icd] = (mode == kBraFunction ? 1.0 : hsign) * v;
+                        }
+                    }
+            }
+            const double pref = 2.0 * std::pow(kPi, 2.5) / (p * q * std::sqrt(p + q));
+            for (int axis = 0; axis < 3; ++axis)
+                for (int ka = 0; ka < bra.ka; ++ka)
+                    for (int kb = 0; kb < bra.kb; ++kb) {
+                        const double cbra = pref * bra.coef[(ib * bra.ka + ka) * bra.kb + kb];
+                        for (int kc = 0; kc < ket.ka; ++kc)
+                            for (int kd = 0; kd < ket.kb; ++kd) {
+                                const double cf = cbra * ket.coef[(ik * ket.ka + kc) * ket.kb + kd];
+                                if (cf == 0.0) continue;
+                                const int base = ka * na * sa + kb * nb * sb + kc * nc * sc + kd * nd;
+                                for (int ia = 0; ia < na; ++ia)
+                                    for (int jb = 0; jb < nb; ++jb)
+                                        for (int ic = 0; ic < nc; ++ic) {
+                                            double* o = &out[axis][base + ia * sa + jb * sb + ic * sc];
+                                            const double* s = &val[(((axis * na + ia) * nb + jb) * nc + ic) * nd];
+                                            for (int id = 0; id < nd; ++id) o[id] += cf * s[id];
+                                        }
+                            }
+                    }
+        }
+    }
+}
+
 }  // namespace
 
 // =================================================================== C ABI
@@ -777,6 +888,252 @@ int md_coulomb_four_center(const md_shells* s0, const md_shells* s1, const md_sh
                                          c.first_function + k) *
                                             n3 +
                                         d.first_function + l] = sph[((i * fb + j) * fc + k) * fd + l];
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+// <d/dA mu | O | nu> for O = 1 (kind 0), -1/2 nabla^2 (kind 1) or the point
+// charges (kind 2) -> out[image][3][bra][ket]; for kind 2 also
+// <mu | d/dC V_C | nu> -> nuclei[image][charge][3][bra][ket]
+// (one_electron.rs derivatives; the bra function by raising and lowering its
+// angular momentum, a charge position by the shift of the Hermite integrals).
+static int one_electron_derivative(int kind, const md_shells* bs, const md_shells* ks, int64_t ntr, const double* tr,
+                                   int64_t ncharge, const double* charges, const double* positions, int kernel,
+                                   double omega, double* out, double* nuclei) {
+    Table bra, ket;
+    if (!build_table(bs, bra) || !build_table(ks, ket)) return 1;
+    const int maxl = std::max(bra.maxl, ket.maxl);
+    Transforms T(maxl);
+    const long nb = bra.nfunc, nk = ket.nfunc;
+    const long plane = nb * nk;
+    for (int64_t it = 0; it < ntr; ++it) {
+        double* img = out + it * 3 * plane;
+        double* nimg = nuclei ? nuclei + it * ncharge * 3 * plane : nullptr;
+#pragma omp parallel
+        {
+            RWork w;
+#pragma omp for schedule(dynamic)
+            for (int ia = 0; ia < (int)bra.shells.size(); ++ia) {
+                const ShellView& a = bra.shells[ia];
+                for (int ib = 0; ib < (int)ket.shells.size(); ++ib) {
+                    const ShellView& b = ket.shells[ib];
+                    double cbt[3];
+                    for (int x = 0; x < 3; ++x) cbt[x] = b.center[x] + tr[3 * it + x];
+                    Pair pr = make_pair(a, a.center, b, cbt, 1, kind == 1 ? 2 : 0);
+                    const auto& ca = T.comps[a.l];
+                    const auto& cb = T.comps[b.l];
+                    const int na = (int)ca.size(), nbb = (int)cb.size();
+                    const long bsz = (long)a.ncontr * na * b.ncontr * nbb;
+                    std::vector<double> block(3 * bsz, 0.0);
+                    std::vector<double> nblock(kind == 2 ? ncharge * 3 * bsz : 0, 0.0);
+                    std::vector<double> vals(3 * na * nbb), nvals(kind == 2 ? ncharge * 3 * na * nbb : 0);
+                    const int L = a.l + b.l + 1;
+                    const int s1 = L + 1;
+                    std::vector<double> R(s1 * s1 * s1), Rs;
+                    std::vector<std::vector<double>> Rc(kind == 2 ? ncharge : 0);
+                    std::vector<HTerm> terms;
+                    for (size_t ip = 0; ip < pr.prims.size(); ++ip) {
+                        const PrimPair& P = pr.prims[ip];
+                        const double p = P.p;
+                        if (kind == 2) {
+                            Rs.assign(R.size(), 0.0);
+                            for (int64_t c = 0; c < ncharge; ++c) {
+                                const double pc[3] = {P.P[0] - positions[3 * c], P.P[1] - positions[3 * c + 1],
+                                                      P.P[2] - positions[3 * c + 2]};
+                                hermite_r_kernel(L, p, kernel, omega, pc, w, R.data());
+                                Rc[c] = R;
+                                for (size_t i = 0; i < R.size(); ++i) Rs[i] -= charges[c] * R[i];
+                            }
+                        }
+                        const double ov = std::pow(kPi / p, 1.5);
+                        const double b2 = P.eb;
+                        auto s1d = [&](int x, int i, int j) { return P.e[x].get(i, j, 0); };
+                        auto d2 = [&](int x, int i, int j) {
+                            return 4.0 * b2 * b2 * P.e[x].get(i, j + 2, 0) - 2.0 * b2 * (2 * j + 1) * P.e[x].get(i, j, 0) +
+                                   (j >= 2 ? j * (j - 1) * P.e[x].get(i, j - 2, 0) : 0.0);
+                        };
+                        auto raise = [&](auto f, int x, int i, int j) {
+                            double v = 2.0 * P.ea * f(x, i + 1, j);
+                            if (i > 0) v -= i * f(x, i - 1, j);
+                            return v;
+                        };
+                        for (int axis = 0; axis < 3; ++axis)
+                            for (int i = 0; i < na; ++i)
+                                for (int j = 0; j < nbb; ++j) {
+                                    const auto& ai = ca[i];
+                                    const auto& bj = cb[j];
+                                    double v = 0.0;
+                                    if (kind == 0) {
+                                        v = ov;
+                                        for (int x = 0; x < 3; ++x)
+                                            v *= x == axis ? raise(s1d, x, ai[x], bj[x]) : s1d(x, ai[x], bj[x]);
+                                    } else if (kind == 1) {
+                                        double s[3], t[3];
+                                        for (int x = 0; x < 3; ++x) {
+                                            s[x] = x == axis ? raise(s1d, x, ai[x], bj[x]) : s1d(x, ai[x], bj[x]);
+                                            t[x] = x == axis ? raise(d2, x, ai[x], bj[x]) : d2(x, ai[x], bj[x]);
+                                        }
+                                        v = -0.5 * ov * (t[0] * s[1] * s[2] + s[0] * t[1] * s[2] + s[0] * s[1] * t[2]);
+                                    } else {
+                                        pair_terms(P, ai, bj, true, axis, 1.0, terms);
+                                        for (const HTerm& h : terms) v += h.c * Rs[(h.t * s1 + h.u) * s1 + h.v];
+                                        v *= 2.0 * kPi / p;
+                                        pair_terms(P, ai, bj, false, 0, 1.0, terms);
+                                        const int dx = axis == 0, dy = axis == 1, dz = axis == 2;
+                                        for (int64_t c = 0; c < ncharge; ++c) {
+                                            double vc = 0.0;
+                                            for (const HTerm& h : terms)
+                                                vc += h.c * Rc[c][((h.t + dx) * s1 + h.u + dy) * s1 + h.v + dz];
+                                            nvals[((c * 3 + axis) * na + i) * nbb + j] = charges[c] * 2.0 * kPi / p * vc;
+                                        }
+                                    }
+                                    vals[(axis * na + i) * nbb + j] = v;
+                                }
+                        for (int ka = 0; ka < a.ncontr; ++ka)
+                            for (int kb = 0; kb < b.ncontr; ++kb) {
+                                const double cf = pr.coef[(ip * a.ncontr + ka) * b.ncontr + kb];
+                                for (int axis = 0; axis < 3; ++axis)
+                                    for (int i = 0; i < na; ++i)
+                                        for (int j = 0; j < nbb; ++j)
+                                            block[axis * bsz + ((ka * na + i) * b.ncontr + kb) * nbb + j] +=
+                                                cf * vals[(axis * na + i) * nbb + j];
+                                if (kind == 2)
+                                    for (int64_t c = 0; c < ncharge; ++c)
+                                        for (int axis = 0; axis < 3; ++axis)
+                                            for (int i = 0; i < na; ++i)
+                                                for (int j = 0; j < nbb; ++j)
+                                                    nblock[(c * 3 + axis) * bsz + ((ka * na + i) * b.ncontr + kb) * nbb + j] +=
+                                                        cf * nvals[((c * 3 + axis) * na + i) * nbb + j];
+                            }
+                    }
+                    const int ls[4] = {a.l, b.l, -1, -1};
+                    const int kk[4] = {a.ncontr, b.ncontr, 1, 1};
+                    const int fa = nfunc(a), fb = nfunc(b);
+                    const long nsets = kind == 2 ? 3 + 3 * ncharge : 3;
+                    for (long set = 0; set < nsets; ++set) {
+                        std::vector<double> part(set < 3 ? block.begin() + set * bsz : nblock.begin() + (set - 3) * bsz,
+                                                 set < 3 ? block.begin() + (set + 1) * bsz
+                                                         : nblock.begin() + (set - 2) * bsz);
+                        auto sph = to_spherical(part, ls, kk, T);
+                        double* tgt = set < 3 ? img + set * plane : nimg + (set - 3) * plane;
+                        for (int i = 0; i < fa; ++i)
+                            for (int j = 0; j < fb; ++j)
+                                tgt[(long)(a.first_function + i) * nk + b.first_function + j] = sph[i * fb + j];
+                    }
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+int md_overlap_derivative(const md_shells* b, const md_shells* k, int64_t ntr, const double* tr, double* out) {
+    return one_electron_derivative(0, b, k, ntr, tr, 0, nullptr, nullptr, 0, 0.0, out, nullptr);
+}
+int md_kinetic_derivative(const md_shells* b, const md_shells* k, int64_t ntr, const double* tr, double* out) {
+    return one_electron_derivative(1, b, k, ntr, tr, 0, nullptr, nullptr, 0, 0.0, out, nullptr);
+}
+int md_nuclear_attraction_derivative(const md_shells* b, const md_shells* k, int64_t ntr, const double* tr,
+                                     int64_t ncharge, const double* charges, const double* positions, int kernel,
+                                     double omega, double* by_center, double* by_nucleus) {
+    return one_electron_derivative(2, b, k, ntr, tr, ncharge, charges, positions, kernel, omega, by_center,
+                                   by_nucleus);
+}
+
+// (d/dP P | Q(r - T)) -> out[image][3][bra][ket] (two_electron.rs:132-190)
+int md_coulomb_two_center_derivative(const md_shells* bs, const md_shells* ks, int64_t ntr, const double* tr,
+                                     int kernel, double omega, double* out) {
+    Table bra, ket;
+    if (!build_table(bs, bra) || !build_table(ks, ket)) return 1;
+    Transforms T(std::max(bra.maxl, ket.maxl));
+    const long nb = bra.nfunc, nk = ket.nfunc;
+    for (int64_t it = 0; it < ntr; ++it) {
+        double* img = out + it * 3 * nb * nk;
+#pragma omp parallel
+        {
+            RWork w;
+#pragma omp for schedule(dynamic)
+            for (int ia = 0; ia < (int)bra.shells.size(); ++ia) {
+                const ShellView& a = bra.shells[ia];
+                Pair pa = single_pair(a, a.center);
+                for (int ic = 0; ic < (int)ket.shells.size(); ++ic) {
+                    const ShellView& c = ket.shells[ic];
+                    double cc[3];
+                    for (int x = 0; x < 3; ++x) cc[x] = c.center[x] + tr[3 * it + x];
+                    Pair pc = single_pair(c, cc);
+                    const long bsz = (long)a.ncontr * n_cart(a.l) * c.ncontr * n_cart(c.l);
+                    std::vector<double> blocks[3] = {std::vector<double>(bsz, 0.0), std::vector<double>(bsz, 0.0),
+                                                     std::vector<double>(bsz, 0.0)};
+                    coulomb_block_derivative(pa, pc, T, kernel, omega, kBraHermite, w, blocks);
+                    const int ls[4] = {a.l, -1, c.l, -1};
+                    const int kk[4] = {a.ncontr, 1, c.ncontr, 1};
+                    const int fa = nfunc(a), fc = nfunc(c);
+                    for (int axis = 0; axis < 3; ++axis) {
+                        auto sph = to_spherical(blocks[axis], ls, kk, T);
+                        for (int i = 0; i < fa; ++i)
+                            for (int j = 0; j < fc; ++j)
+                                img[((long)axis * nb + a.first_function + i) * nk + c.first_function + j] = sph[i * fc + j];
+                    }
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+// (d/dP P(r - T_P) | mu nu(r - T_nu)) in slots 0..2 and (P | d/dA mu nu) in slots
+// 3..5 -> out[image][6][aux][bra][ket]; tr[image][2][3] (two_electron.rs:300-394)
+int md_coulomb_three_center_derivative(const md_shells* as, const md_shells* bs, const md_shells* ks, int64_t ntr,
+                                       const double* tr, int kernel, double omega, double* out) {
+    Table aux, bra, ket;
+    if (!build_table(as, aux) || !build_table(bs, bra) || !build_table(ks, ket)) return 1;
+    Transforms T(std::max(aux.maxl, std::max(bra.maxl, ket.maxl)));
+    const long na = aux.nfunc, nb = bra.nfunc, nk = ket.nfunc;
+    const long vol = na * nb * nk;
+    for (int64_t it = 0; it < ntr; ++it) {
+        const double* tp = tr + 6 * it;
+        const double* tn = tr + 6 * it + 3;
+        double* img = out + it * 6 * vol;
+#pragma omp parallel
+        {
+            RWork w;
+#pragma omp for schedule(dynamic)
+            for (int ip = 0; ip < (int)aux.shells.size(); ++ip) {
+                const ShellView& P = aux.shells[ip];
+                double cp[3];
+                for (int x = 0; x < 3; ++x) cp[x] = P.center[x] + tp[x];
+                Pair pp = single_pair(P, cp);
+                for (int ia = 0; ia < (int)bra.shells.size(); ++ia) {
+                    const ShellView& a = bra.shells[ia];
+                    for (int ib = 0; ib < (int)ket.shells.size(); ++ib) {
+                        const ShellView& b = ket.shells[ib];
+                        double cb[3];
+                        for (int x = 0; x < 3; ++x) cb[x] = b.center[x] + tn[x];
+                        Pair pab = make_pair(a, a.center, b, cb, 1, 0);
+                        const long bsz = (long)a.ncontr * n_cart(a.l) * b.ncontr * n_cart(b.l) * P.ncontr * n_cart(P.l);
+                        const int ls[4] = {a.l, b.l, P.l, -1};
+                        const int kk[4] = {a.ncontr, b.ncontr, P.ncontr, 1};
+                        const int fa = nfunc(a), fb = nfunc(b), fp = nfunc(P);
+                        for (int which = 0; which < 2; ++which) {
+                            std::vector<double> blocks[3] = {std::vector<double>(bsz, 0.0),
+                                                             std::vector<double>(bsz, 0.0),
+                                                             std::vector<double>(bsz, 0.0)};
+                            coulomb_block_derivative(pab, pp, T, kernel, omega, which == 0 ? kKetHermite : kBraFunction,
+                                                     w, blocks);
+                            for (int axis = 0; axis < 3; ++axis) {
+                                auto sph = to_spherical(blocks[axis], ls, kk, T);
+                                double* slab = img + (long)(3 * which + axis) * vol;
+                                for (int i = 0; i < fa; ++i)
+                                    for (int j = 0; j < fb; ++j)
+                                        for (int m = 0; m < fp; ++m)
+                                            slab[((long)(P.first_function + m) * nb + a.first_function + i) * nk +
+                                                 b.first_function + j] = sph[(i * fb + j) * fp + m];
+                            }
+                        }
+                    }
                 }
             }
         }

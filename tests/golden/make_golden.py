@@ -17,6 +17,8 @@ Two kinds of fixture are written:
   its integrals supplied by the oracle's C++ restatement of the Rust kernels:
   geometry, total energy, alpha density, iteration energies. The same script
   checks the oracle's NumPy restatement (oracle/dfrhf.py) against each run.
+* ``reference_gradient_*.npz``: the reference's own DF-RHF nuclear gradient at
+  its converged state, with the state itself (see ``reference_gradients``).
 """
 
 from __future__ import annotations
@@ -109,7 +111,76 @@ def reference_runs(reference: pathlib.Path) -> None:
         )
 
 
+GRADIENT_CASES = [("water_pyscf", "def2-svp"), ("water", "cc-pvdz"), ("h2o2_s0", "cc-pvdz"), ("h2o4_s1", "cc-pvdz")]
+
+
+def reference_gradients(reference: pathlib.Path) -> None:
+    """``reference_gradient_*.npz``: the reference's own DF-RHF nuclear gradient
+    (``hafnium.properties.nuclear_gradient``, gradient.py:72-149) at its tightly
+    converged state (the options of tests/reference/test_gradient_reference.py:38),
+    with the oracle restatement checked against it term by term, and the
+    water/def2-SVP run checked against the PySCF gradient the reference stores
+    (tests/reference/data/gradient_water_def2-svp.json) at its GRADIENT_TOL 1e-7."""
+    from oracle import reference_env
+
+    reference_env.install(reference)
+    from hafnium.basis import BasisLibrary, BasisSet
+    from hafnium.integrals import RustEngine
+    from hafnium.molecule import Molecule as RefMolecule
+    from hafnium.properties import nuclear_gradient
+    from hafnium.scf import ScfOptions, hartree_fock
+
+    from hafnium_b200.basis import ShellTable
+    from hafnium_b200.molecule import Molecule
+    from oracle import dfrhf
+
+    library = BasisLibrary(offline=True)
+    engine = RustEngine()
+    options = ScfOptions(gradient_tolerance=1e-10, energy_tolerance=1e-13, max_iterations=200)
+    stored = json.loads((reference / "tests" / "reference" / "data" / "gradient_water_def2-svp.json").read_text())
+    for tag, basis_name in GRADIENT_CASES:
+        if tag == "water_pyscf":
+            mol = Molecule(("O", "H", "H"), np.asarray(stored["provenance"]["positions_bohr"], dtype=np.float64))
+        else:
+            n, seed = {"water": (1, None), "h2o2_s0": (2, 0), "h2o4_s1": (4, 1)}[tag]
+            mol = molecule_for(n, seed)
+        ref_mol = RefMolecule.from_atoms(list(zip(mol.symbols, map(tuple, mol.positions))), unit="bohr")
+        basis = BasisSet.for_atoms(ref_mol, basis_name, library=library)
+        aux = BasisSet.for_atoms(ref_mol, "def2-universal-jkfit", library=library)
+        result = hartree_fock(engine, basis, ref_mol, auxiliary=aux, options=options)
+        grad = nuclear_gradient(engine, basis, aux, ref_mol, result)
+        terms = {k: np.asarray(getattr(grad, k)) for k in
+                 ("nuclear_repulsion", "one_electron", "overlap", "coulomb", "exchange")}
+        total = np.asarray(grad.total)
+        d_alpha = np.asarray(result.density.blocks[0])
+        fock = np.asarray(result.fock.blocks[0])
+        orb = ShellTable.build(basis_name, mol.symbols, mol.positions)
+        auxt = ShellTable.build("def2-universal-jkfit", mol.symbols, mol.positions)
+        ours = dfrhf.nuclear_gradient(orb, auxt, mol.nuclear_charges, mol.positions, d_alpha, fock)
+        worst = max(float(np.max(np.abs(ours[k] - terms[k]))) for k in terms)
+        msg = f"{tag}/{basis_name}: E = {result.energy:.12f}, oracle vs reference max |dG| = {worst:.2e}"
+        if tag == "water_pyscf":
+            dp = float(np.max(np.abs(total - np.asarray(stored["gradient"]))))
+            msg += f", reference vs stored PySCF max |dG| = {dp:.2e}"
+            assert dp < 1e-7
+        print(msg)
+        assert worst < 1e-10
+        np.savez_compressed(
+            HERE / f"reference_gradient_{tag}.npz",
+            basis=np.asarray(basis_name),
+            symbols=np.asarray(mol.symbols),
+            positions_bohr=mol.positions,
+            energy=np.asarray(result.energy),
+            density=d_alpha,
+            fock=fock,
+            total=total,
+            pyscf_total=np.asarray(stored["gradient"]) if tag == "water_pyscf" else np.zeros((0, 3)),
+            **terms,
+        )
+
+
 if __name__ == "__main__":
     ref = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     stored_pyscf(ref)
     reference_runs(ref)
+    reference_gradients(ref)
