@@ -24,7 +24,7 @@ EXPORTS = (
     "hf_ctx_create", "hf_ctx_destroy", "hf_last_error", "hf_set_stream", "hf_shells_upload",
     "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
     "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_four_center", "hf_get_stats",
-    "hf_coulomb_static", "hf_mp2_energy",
+    "hf_coulomb_static", "hf_mp2_energy", "hf_nuclear_gradient",
 )
 
 BATCH_EXPORTS = (
@@ -118,6 +118,7 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_four_center.argtypes = [v, v, i]
     lib.hf_coulomb_static.argtypes = [v, v, v]
     lib.hf_mp2_energy.argtypes = [v, v, v, i64, i64, ctypes.POINTER(ctypes.c_double), i]
+    lib.hf_nuclear_gradient.argtypes = [v, v, i64, v, v, v, i64, v, i]
     lib.hf_get_stats.argtypes = [v, p(StatsC)]
     d = ctypes.c_double
     lib.hf_batch_default_options.argtypes = [p(BatchOptionsC)]
@@ -286,6 +287,27 @@ class Context:
                                             ctypes.byref(out), 0)
         self.check(status, "hf_mp2_energy")
         return float(out.value)
+
+    def nuclear_gradient(self, occupied, weighted, charges, positions) -> np.ndarray:
+        """The five DF-RHF gradient terms [5, atom, 3] (torch CUDA tensors or NumPy
+        arrays for the occupied orbitals and the energy-weighted density)."""
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        r = np.ascontiguousarray(positions, dtype=np.float64)
+        out = np.empty((5, q.shape[0], 3))
+        if hasattr(occupied, "data_ptr"):
+            c = occupied.contiguous()
+            w = weighted.contiguous()
+            torch_sync(c)
+            torch_sync(w)
+            status = self.lib.hf_nuclear_gradient(self.handle, c.data_ptr(), c.shape[1], w.data_ptr(), q.ctypes.data,
+                                                  r.ctypes.data, q.shape[0], out.ctypes.data, 0)
+        else:
+            c = np.ascontiguousarray(occupied, dtype=np.float64)
+            w = np.ascontiguousarray(weighted, dtype=np.float64)
+            status = self.lib.hf_nuclear_gradient(self.handle, c.ctypes.data, c.shape[1], w.ctypes.data, q.ctypes.data,
+                                                  r.ctypes.data, q.shape[0], out.ctypes.data, 0)
+        self.check(status, "hf_nuclear_gradient")
+        return out
 
     # -- inspection ----------------------------------------------------------
     def metric(self) -> np.ndarray:

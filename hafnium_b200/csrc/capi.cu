@@ -1061,6 +1061,274 @@ int hf_mp2_energy(hf_ctx* ctx, const double* mo_coefficients, const double* mo_e
     return HF_OK;
 }
 
+// The atom of every shell: the one at its centre.
+static int shell_atoms(hf_ctx* ctx, const std::vector<DevShell>& shells, const double* positions, int64_t natoms,
+                       std::vector<int>& out, const char* what) {
+    out.assign(shells.size(), -1);
+    for (size_t s = 0; s < shells.size(); ++s) {
+        double best = 1e300;
+        for (int64_t a = 0; a < natoms; ++a) {
+            const double dx = shells[s].x - positions[3 * a], dy = shells[s].y - positions[3 * a + 1],
+                         dz = shells[s].z - positions[3 * a + 2];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < best) {
+                best = d2;
+                out[s] = (int)a;
+            }
+        }
+        if (out[s] < 0 || best > 1e-20)
+            return fail(ctx, HF_ERR_ARG, std::string(what) + " shell " + std::to_string(s) + " sits on no atom");
+    }
+    return HF_OK;
+}
+
+int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double* W, const double* charges,
+                        const double* positions, int64_t natoms, double* terms, int on_device) {
+    if (!ctx || !C || !W || !charges || !positions || !terms || nocc < 1 || natoms < 1) return HF_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    if (nocc > ctx->n) return fail(ctx, HF_ERR_ARG, "more occupied orbitals than basis functions");
+    if ((int64_t)nocc * nocc > INT32_MAX / 2) return fail(ctx, HF_ERR_ARG, "too many occupied orbitals");
+    cudaSetDevice(ctx->device);
+    std::vector<int> orb_atom, aux_atom;
+    int st;
+    if ((st = shell_atoms(ctx, ctx->orb, positions, natoms, orb_atom, "orbital")) != HF_OK) return st;
+    if ((st = shell_atoms(ctx, ctx->aux, positions, natoms, aux_atom, "auxiliary")) != HF_OK) return st;
+    // the split-BF16 copy of B is not needed here; its room goes to the gradient
+    release(ctx->d_bf16_b);
+    upload_gradient_tables(ctx->stream);
+    const JkPlan p = plan_of(ctx);
+    const int64_t n = ctx->n, N = ctx->naux, o = nocc, oo = nocc * nocc;
+    const size_t nn = (size_t)n * n, NN = (size_t)N * N;
+    const int nso = (int)ctx->orb.size(), nsa = (int)ctx->aux.size();
+    struct Temps {
+        hf_ctx* c;
+        std::vector<void*> ptrs;
+        ~Temps() {
+            for (void* q : ptrs) cudaFreeAsync(q, c->stream);
+        }
+        double* take(size_t doubles) {
+            void* q = nullptr;
+            if (cudaMallocAsync(&q, sizeof(double) * std::max<size_t>(doubles, 1), c->stream) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            ptrs.push_back(q);
+            return static_cast<double*>(q);
+        }
+    } tmp{ctx, {}};
+    const double* dC = C;
+    const double* dW = W;
+    if (!on_device) {
+        double* sC = tmp.take((size_t)n * o);
+        double* sW = tmp.take(nn);
+        if (!sC || !sW) return fail(ctx, HF_ERR_OOM, "no room for the gradient's inputs");
+        HF_CU(cudaMemcpyAsync(sC, C, sizeof(double) * n * o, cudaMemcpyHostToDevice, ctx->stream));
+        HF_CU(cudaMemcpyAsync(sW, W, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
+        dC = sC;
+        dW = sW;
+    }
+    double* Dt = tmp.take(nn);
+    double* dfit = tmp.take(N);
+    double* cfit = tmp.take(N);
+    double* work = tmp.take((size_t)coulomb_work_doubles(p));
+    double* L = tmp.take(NN);
+    double* Linv = tmp.take(NN);
+    double* LinvT = tmp.take(NN);
+    double* wk = tmp.take((size_t)N * 64);
+    double* Gt = tmp.take((size_t)oo * N);
+    double* G = tmp.take((size_t)oo * N);
+    double* WJ = tmp.take(NN);
+    double* WK = tmp.take(NN);
+    double* acc = tmp.take((size_t)(2 * nso + nsa) * 6 + 3 * natoms);
+    double* dq = tmp.take(natoms);
+    double* dpos = tmp.take(3 * natoms);
+    if (!Dt || !dfit || !cfit || !work || !L || !Linv || !LinvT || !wk || !Gt || !G || !WJ || !WK || !acc || !dq ||
+        !dpos)
+        return fail(ctx, HF_ERR_OOM, "no room for the gradient's intermediates");
+    double* gorb = acc;
+    double* gorb1 = gorb + (size_t)nso * 6;
+    double* gaux = gorb1 + (size_t)nso * 6;
+    double* gatom = gaux + (size_t)nsa * 6;
+    HF_CU(cudaMemsetAsync(acc, 0, sizeof(double) * ((size_t)(2 * nso + nsa) * 6 + 3 * natoms), ctx->stream));
+    HF_CU(cudaMemcpyAsync(dq, charges, sizeof(double) * natoms, cudaMemcpyHostToDevice, ctx->stream));
+    HF_CU(cudaMemcpyAsync(dpos, positions, sizeof(double) * 3 * natoms, cudaMemcpyHostToDevice, ctx->stream));
+    auto gemm = [&](int M, int Ncol, int K, const double* A, int64_t lda, const double* B, int64_t ldb, double* Cm,
+                    int64_t ldc, double alpha, int kmode, int epi) {
+        GemmArgs g{};
+        g.M = M;
+        g.N = Ncol;
+        g.K = K;
+        g.A = A;
+        g.lda = lda;
+        g.B = B;
+        g.ldb = ldb;
+        g.C = Cm;
+        g.ldc = ldc;
+        g.alpha = alpha;
+        g.beta = 0.0;
+        g.kmode = kmode;
+        g.epi = epi;
+        ++ctx->stats.kernel_launches;
+        return dgemm_nt(g, 1, ctx->stream);
+    };
+    // total density D = 2 C C^T and the fitted charges d = L^-1 (P|uv) D
+    HF_CU(gemm((int)n, (int)n, (int)o, dC, o, dC, o, Dt, n, 2.0, 0, 0));
+    HF_CU(fitted_charges(p, Dt, dfit, work, ctx->stream));
+    // the metric's factor M = L L^T and its inverse
+    HF_CU(cudaMemcpyAsync(L, ctx->d_metric, NN * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    HF_CU(cudaMemsetAsync(ctx->d_info, 0, sizeof(int), ctx->stream));
+    const double big = 1e300;
+    HF_CU(cudaMemcpyAsync(ctx->d_scalar, &big, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    HF_CU(cholesky_lower(L, N, N, ctx->d_info, ctx->d_scalar, ctx->stream));
+    int info = 0;
+    HF_CU(cudaMemcpyAsync(&info, ctx->d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    HF_CU(cudaStreamSynchronize(ctx->stream));
+    if (info != 0) return fail(ctx, HF_ERR_NUMERIC, "the Coulomb metric is not positive definite");
+    HF_CU(triangular_inverse(L, N, N, Linv, LinvT, wk, ctx->stream));
+    // c = M^-1 q = L^-T d
+    HF_CU(gemm(1, (int)N, (int)N, dfit, N, LinvT, N, cfit, N, 1.0, 1, 0));
+    // Gamma_P = C^T (sum_Q M^-1_PQ (Q|uv)) C = L^-T applied to C^T B_Q C
+    HF_CU(occupied_pair_tensor_t(p, dC, o, o, Gt, ctx->stream));
+    HF_CU(gemm((int)oo, (int)N, (int)N, Gt, N, LinvT, N, G, oo, 1.0, 1, 1));
+    // metric weights: W^J = -c c^T / 2, W^K = Gamma Gamma^T (gradient.py:127-145)
+    HF_CU(gemm((int)N, (int)N, 1, cfit, 1, cfit, 1, WJ, N, -0.5, 0, 0));
+    HF_CU(gemm((int)N, (int)N, (int)oo, G, oo, G, oo, WK, N, 1.0, 0, 0));
+    HF_CU(launch_metric_grad(ctx->d_aux, ctx->d_exps, ctx->d_coefs, ctx->d_aux_by_l, ctx->aux_count, ctx->d_btable,
+                             WJ, WK, N, gaux, ctx->stream));
+    ctx->stats.kernel_launches += 25;
+    // three-centre derivatives over blocks of auxiliary functions, with the
+    // exchange weight GK_P = -2 C Gamma_P C^T of the block formed by two GEMMs
+    std::vector<PairTask> tasks[3][3];
+    int max_npp[3][3];
+    chunk_tasks(ctx, 0, ctx->nt, tasks, max_npp);
+    size_t ntask = 0;
+    for (int la = 0; la <= 2; ++la)
+        for (int lb = la; lb <= 2; ++lb) {
+            ntask += tasks[la][lb].size();
+            if (!tasks[la][lb].empty() && three_center_grad_smem(la, lb, max_npp[la][lb]) > 200 * 1024)
+                return fail(ctx, HF_ERR_ARG, "a shell pair has too many primitive pairs for the gradient kernel");
+        }
+    PairTask* d_tasks = reinterpret_cast<PairTask*>(tmp.take((ntask * sizeof(PairTask) + 7) / 8 + 1));
+    if (!d_tasks) return fail(ctx, HF_ERR_OOM, "no room for the gradient's pair list");
+    {
+        size_t off = 0;
+        for (int la = 0; la <= 2; ++la)
+            for (int lb = la; lb <= 2; ++lb) {
+                auto& v = tasks[la][lb];
+                if (v.empty()) continue;
+                HF_CU(cudaMemcpyAsync(d_tasks + off, v.data(), sizeof(PairTask) * v.size(), cudaMemcpyHostToDevice,
+                                      ctx->stream));
+                off += v.size();
+            }
+    }
+    size_t freeb = 0, totalb = 0;
+    cudaMemGetInfo(&freeb, &totalb);
+    const size_t per_p = sizeof(double) * (nn + (size_t)n * o);
+    const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 3);
+    const int64_t pb_max = std::max<int64_t>(16, (int64_t)(budget / per_p));
+    double* Zt = tmp.take((size_t)n * o * (pb_max + 8));
+    double* GK = tmp.take(nn * (pb_max + 8));
+    if (!Zt || !GK) return fail(ctx, HF_ERR_OOM, "no room for the exchange weights of a block");
+    int class_start[kMaxAuxL + 1];
+    for (int l = 0, c = 0; l <= kMaxAuxL; ++l) {
+        class_start[l] = c;
+        c += ctx->aux_count[l];
+    }
+    auto nfun = [&](int s) { return ctx->aux[s].ncontr * nsph(ctx->aux[s].l); };
+    for (int s0 = 0; s0 < nsa;) {
+        const int P0 = ctx->aux[s0].fn;
+        int s1 = s0 + 1;
+        while (s1 < nsa && ctx->aux[s1].fn + nfun(s1) - P0 <= pb_max) ++s1;
+        const int64_t Pb = ctx->aux[s1 - 1].fn + nfun(s1 - 1) - P0;
+        HF_CU(gemm((int)n, (int)(Pb * o), (int)o, dC, o, G + (size_t)P0 * oo, o, Zt, Pb * o, 1.0, 0, 0));
+        HF_CU(gemm((int)n, (int)(n * Pb), (int)o, dC, o, Zt, o, GK, n * Pb, -2.0, 0, 0));
+        const int* alist[kMaxAuxL + 1];
+        int count[kMaxAuxL + 1];
+        for (int l = 0; l <= kMaxAuxL; ++l) {
+            const int lo = std::max(s0, class_start[l]), hi = std::min(s1, class_start[l] + ctx->aux_count[l]);
+            alist[l] = ctx->d_aux_by_l[l] + std::max(0, lo - class_start[l]);
+            count[l] = std::max(0, hi - lo);
+        }
+        const GradWeights gw{Dt, cfit, GK, n, P0, Pb};
+        size_t off = 0;
+        for (int la = 0; la <= 2; ++la)
+            for (int lb = la; lb <= 2; ++lb) {
+                const auto& v = tasks[la][lb];
+                if (v.empty()) continue;
+                HF_CU(launch_three_center_grad(la, lb, d_tasks + off, (int)v.size(), max_npp[la][lb], ctx->d_orb,
+                                               ctx->d_aux, ctx->d_exps, ctx->d_coefs, alist, count, ctx->d_btable, gw,
+                                               gorb, gaux, ctx->stream));
+                ctx->stats.kernel_launches += 5;
+                off += v.size();
+            }
+        s0 = s1;
+    }
+    // one-electron terms over all ordered shell pairs
+    std::vector<int2> pairs1[3][3];
+    for (int a = 0; a < nso; ++a)
+        for (int b = 0; b < nso; ++b) pairs1[ctx->orb[a].l][ctx->orb[b].l].push_back(make_int2(a, b));
+    int2* d_pairs1 = reinterpret_cast<int2*>(tmp.take(((size_t)nso * nso * sizeof(int2) + 7) / 8 + 1));
+    if (!d_pairs1) return fail(ctx, HF_ERR_OOM, "no room for the one-electron pair list");
+    {
+        size_t off = 0;
+        for (int la = 0; la <= 2; ++la)
+            for (int lb = 0; lb <= 2; ++lb) {
+                auto& v = pairs1[la][lb];
+                if (v.empty()) continue;
+                HF_CU(cudaMemcpyAsync(d_pairs1 + off, v.data(), sizeof(int2) * v.size(), cudaMemcpyHostToDevice,
+                                      ctx->stream));
+                HF_CU(launch_one_electron_grad(la, lb, d_pairs1 + off, (int)v.size(), ctx->d_orb, ctx->d_exps,
+                                               ctx->d_coefs, dq, dpos, (int)natoms, ctx->d_btable, Dt, dW, n, gorb1,
+                                               gatom, ctx->stream));
+                ctx->stats.kernel_launches += 2;
+                off += v.size();
+            }
+    }
+    std::vector<double> h((size_t)(2 * nso + nsa) * 6 + 3 * natoms);
+    HF_CU(cudaMemcpyAsync(h.data(), acc, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    HF_CU(cudaStreamSynchronize(ctx->stream));
+    if ((st = check_async(ctx, "hf_nuclear_gradient")) != HF_OK) return st;
+    // per-shell sums to atoms in a fixed order; the nuclear repulsion on the host
+    std::vector<double> out((size_t)5 * natoms * 3, 0.0);
+    auto at = [&](int term, int atom, int d) -> double& { return out[((size_t)term * natoms + atom) * 3 + d]; };
+    for (int64_t k = 0; k < natoms; ++k)
+        for (int64_t l = 0; l < natoms; ++l) {
+            if (k == l) continue;
+            double r[3], r2 = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                r[d] = positions[3 * k + d] - positions[3 * l + d];
+                r2 += r[d] * r[d];
+            }
+            const double w = charges[k] * charges[l] / (r2 * std::sqrt(r2));
+            for (int d = 0; d < 3; ++d) at(0, (int)k, d) -= w * r[d];
+        }
+    const double* hg = h.data();
+    const double* hg1 = hg + (size_t)nso * 6;
+    const double* hga = hg1 + (size_t)nso * 6;
+    const double* hat = hga + (size_t)nsa * 6;
+    for (int s = 0; s < nso; ++s)
+        for (int d = 0; d < 3; ++d) {
+            at(1, orb_atom[s], d) += hg1[s * 6 + d];
+            at(2, orb_atom[s], d) += hg1[s * 6 + 3 + d];
+            at(3, orb_atom[s], d) += hg[s * 6 + d];
+            at(4, orb_atom[s], d) += hg[s * 6 + 3 + d];
+        }
+    for (int s = 0; s < nsa; ++s)
+        for (int d = 0; d < 3; ++d) {
+            at(3, aux_atom[s], d) += hga[s * 6 + d];
+            at(4, aux_atom[s], d) += hga[s * 6 + 3 + d];
+        }
+    for (int64_t c = 0; c < natoms; ++c)
+        for (int d = 0; d < 3; ++d) at(1, (int)c, d) += hat[c * 3 + d];
+    if (on_device) {
+        HF_CU(cudaMemcpyAsync(terms, out.data(), sizeof(double) * out.size(), cudaMemcpyHostToDevice, ctx->stream));
+        HF_CU(cudaStreamSynchronize(ctx->stream));
+    } else {
+        std::memcpy(terms, out.data(), sizeof(double) * out.size());
+    }
+    return HF_OK;
+}
+
 int hf_get_stats(const hf_ctx* ctx, hf_stats* out) {
     if (!ctx || !out) return HF_ERR_ARG;
     *out = ctx->stats;

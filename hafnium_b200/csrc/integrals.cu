@@ -25,8 +25,6 @@ __constant__ int c_tet_v[ntet(8)];
 __constant__ int c_cart[kMaxAuxL + 1][15][3];
 
 namespace {
-constexpr double kPi = 3.14159265358979323846;
-constexpr double kTwoPi52 = 34.98683665524972;  // 2 pi^(5/2)
 
 double fact(int n) {
     double v = 1.0;
@@ -73,6 +71,31 @@ std::vector<double> c2s_host(int l) {
 }
 }  // namespace
 
+ConstantTables constant_tables_host() {
+    ConstantTables t{};
+    std::vector<double> all;
+    for (int l = 0; l <= kMaxAuxL; ++l) {
+        auto m = c2s_host(l);
+        all.insert(all.end(), m.begin(), m.end());
+    }
+    for (size_t k = 0; k < all.size() && k < (size_t)kC2sSize; ++k) t.c2s[k] = all[k];
+    for (int s = 0; s <= 8; ++s)
+        for (int tt = 0; tt <= s; ++tt)
+            for (int u = 0; u <= s - tt; ++u) {
+                const int v = s - tt - u;
+                t.tet_t[tet(tt, u, v)] = tt;
+                t.tet_u[tet(tt, u, v)] = u;
+                t.tet_v[tet(tt, u, v)] = v;
+            }
+    for (int l = 0; l <= kMaxAuxL; ++l)
+        for (int c = 0; c < ncart(l); ++c) {
+            t.cart[l][c][0] = cart_x(l, c);
+            t.cart[l][c][1] = cart_y(l, c);
+            t.cart[l][c][2] = cart_z(l, c);
+        }
+    return t;
+}
+
 void upload_c2s(cudaStream_t stream) {
     // the tables are constants of the library: written once per device
     static std::mutex mutex;
@@ -81,32 +104,12 @@ void upload_c2s(cudaStream_t stream) {
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
     std::lock_guard<std::mutex> lock(mutex);
     if (done[dev]) return;
-    std::vector<double> all;
-    for (int l = 0; l <= kMaxAuxL; ++l) {
-        auto m = c2s_host(l);
-        all.insert(all.end(), m.begin(), m.end());
-    }
-    cudaMemcpyToSymbolAsync(c_c2s, all.data(), sizeof(double) * all.size(), 0, cudaMemcpyHostToDevice, stream);
-    int tt[ntet(8)], tu[ntet(8)], tv[ntet(8)];
-    for (int s = 0; s <= 8; ++s)
-        for (int t = 0; t <= s; ++t)
-            for (int u = 0; u <= s - t; ++u) {
-                const int v = s - t - u;
-                tt[tet(t, u, v)] = t;
-                tu[tet(t, u, v)] = u;
-                tv[tet(t, u, v)] = v;
-            }
-    int cc[kMaxAuxL + 1][15][3] = {};
-    for (int l = 0; l <= kMaxAuxL; ++l)
-        for (int c = 0; c < ncart(l); ++c) {
-            cc[l][c][0] = cart_x(l, c);
-            cc[l][c][1] = cart_y(l, c);
-            cc[l][c][2] = cart_z(l, c);
-        }
-    cudaMemcpyToSymbolAsync(c_tet_t, tt, sizeof(tt), 0, cudaMemcpyHostToDevice, stream);
-    cudaMemcpyToSymbolAsync(c_tet_u, tu, sizeof(tu), 0, cudaMemcpyHostToDevice, stream);
-    cudaMemcpyToSymbolAsync(c_tet_v, tv, sizeof(tv), 0, cudaMemcpyHostToDevice, stream);
-    cudaMemcpyToSymbolAsync(c_cart, cc, sizeof(cc), 0, cudaMemcpyHostToDevice, stream);
+    const ConstantTables t = constant_tables_host();
+    cudaMemcpyToSymbolAsync(c_c2s, t.c2s, sizeof(t.c2s), 0, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyToSymbolAsync(c_tet_t, t.tet_t, sizeof(t.tet_t), 0, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyToSymbolAsync(c_tet_u, t.tet_u, sizeof(t.tet_u), 0, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyToSymbolAsync(c_tet_v, t.tet_v, sizeof(t.tet_v), 0, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyToSymbolAsync(c_cart, t.cart, sizeof(t.cart), 0, cudaMemcpyHostToDevice, stream);
     done[dev] = cudaStreamSynchronize(stream) == cudaSuccess;
 }
 
@@ -239,12 +242,6 @@ struct PairLayout {
     static constexpr int STRIDE = 4 + KK + NSAB * NH;
 };
 
-// Primitive pairs whose |c_a c_b| exp(-mu R_AB^2) falls below this contribute
-// less than ~1e-15 to any (P|ab) and are skipped (the reference evaluates every
-// primitive triple; the difference is far below its 1e-12 integral tolerance).
-constexpr double kPairScreen = 1e-22;
-
-constexpr int kMaxPrimPairs = 256;
 
 template <int LA, int LB>
 __device__ int pair_prologue(const DevShell& A, const DevShell& B, const double* __restrict__ exps,

@@ -5,6 +5,8 @@
 
 #include <vector>
 
+#include "md.cuh"
+
 namespace hf {
 
 // One shell on the device. `fn` is the first orbital function (AO order) for
@@ -39,7 +41,18 @@ struct ShellClassLists {
     int max_npp[3][3] = {};
 };
 
+// The constant tables every integral kernel reads (each translation unit with
+// such kernels holds its own __constant__ copy): Cartesian-to-spherical
+// matrices, the (t, u, v) of each tetrahedral index up to order 8 and the
+// Cartesian exponents per l.
+struct ConstantTables {
+    double c2s[kC2sSize];
+    int tet_t[ntet(8)], tet_u[ntet(8)], tet_v[ntet(8)];
+    int cart[kMaxAuxL + 1][15][3];
+};
+ConstantTables constant_tables_host();
 void upload_c2s(cudaStream_t stream);
+void upload_gradient_tables(cudaStream_t stream);
 std::vector<double> boys_grid_host();
 
 // (P|Q) for all aux shells into M[N][N] (internal order, row-major, ld = ldm).
@@ -59,6 +72,36 @@ cudaError_t launch_one_electron(int kind, int la, int lb, const int2* tasks, int
                                 const double* exps, const double* coefs, const double* charges,
                                 const double* positions, int natoms, const double* btable, double* out,
                                 int64_t n, cudaStream_t stream);
+
+// Weights the contracted three-centre derivative kernels read: the total density
+// D [n][n], the fitted Coulomb coefficients cfit [naux] (internal order) and the
+// exchange weight GK [n][n][Pb] of the auxiliary functions [P0, P0 + Pb).
+struct GradWeights {
+    const double* D;
+    const double* cfit;
+    const double* GK;
+    int64_t n;
+    int P0;
+    int64_t Pb;
+};
+
+// DF-RHF gradient pieces, contracted on the fly (gradient_kernels.cuh). Force
+// sums per shell: gorb/gaux [shell][6] (Coulomb x y z, exchange x y z) for the
+// fitted terms, gorb1 [shell][6] (one-electron, overlap) and gatom [atom][3]
+// (the attraction's dependence on the nuclei).
+cudaError_t launch_three_center_grad(int la, int lb, const PairTask* tasks, int ntasks, int max_npp,
+                                     const DevShell* orb, const DevShell* aux, const double* exps,
+                                     const double* coefs, const int* const* alist_by_l, const int* count_by_l,
+                                     const double* btable, GradWeights g, double* gorb, double* gaux,
+                                     cudaStream_t stream);
+size_t three_center_grad_smem(int la, int lb, int max_npp);
+cudaError_t launch_metric_grad(const DevShell* aux, const double* exps, const double* coefs,
+                               const int* const* aux_by_l, const int* count, const double* btable, const double* WJ,
+                               const double* WK, int64_t ldw, double* gaux, cudaStream_t stream);
+cudaError_t launch_one_electron_grad(int la, int lb, const int2* tasks, int ntasks, const DevShell* orb,
+                                     const double* exps, const double* coefs, const double* charges,
+                                     const double* positions, int natoms, const double* btable, const double* D,
+                                     const double* W, int64_t n, double* gorb1, double* gatom, cudaStream_t stream);
 
 // Exact (ab|cd) over all shell quartets of a small table into out[n][n][n][n].
 cudaError_t launch_four_center(const DevShell* shells, int ns, const double* exps, const double* coefs,

@@ -521,6 +521,14 @@ cudaError_t coulomb_build(const JkPlan& p, const double* D, int64_t strideD, dou
 
 int64_t coulomb_work_doubles(const JkPlan& p) { return 2 * p.ntiles * 4096 + ((p.naux + 1) / 2) * 2; }
 
+cudaError_t fitted_charges(const JkPlan& p, const double* D, double* d, double* work, cudaStream_t stream) {
+    const int64_t nelem = p.ntiles * 4096;
+    k_pack_density<<<dim3((unsigned)((nelem + 255) / 256), 1), 256, 0, stream>>>(D, 0, 1.0, p.n, p.nt, work, 0,
+                                                                                 nullptr);
+    k_coulomb_charges<<<dim3(p.naux, 1), 512, 0, stream>>>(nullptr, p.B, p.ldb, nelem, work, d, 0, nullptr);
+    return cudaGetLastError();
+}
+
 int syrk_splits(int64_t npad, int count) {
     const int64_t mt = (npad + 127) / 128, nt = (npad + 63) / 64;
     int64_t upper = 0;

@@ -28,6 +28,11 @@ inline cudaError_t coulomb_build(const JkPlan& p, const double* D, double* J, do
 }
 int64_t coulomb_work_doubles(const JkPlan& p);  // per cluster
 
+// d[q] = sum_{mu nu} B_q[mu][nu] D[mu][nu] for a full symmetric n x n D (one
+// cluster): the fitted charges, the first half of the J build; work holds
+// coulomb_work_doubles(p) doubles.
+cudaError_t fitted_charges(const JkPlan& p, const double* D, double* d, double* work, cudaStream_t stream);
+
 // K = sum_q (B_q C) diag(sign) (B_q C)^T. Ct: [opad][npad] (C^T, zero padded,
 // opad a multiple of 64). sign: [opad] or null for all +1 (single cluster only).
 // Kp: npad x npad scratch; X, Xs: npad x (qchunk * opad) scratch (Xs only when

@@ -26,7 +26,8 @@ constexpr int kMaxOrbL = 2;   // cc-pVDZ / def2-SVP / STO-3G for H-Ne
 constexpr int kMaxAuxL = 4;   // def2-universal-jkfit for H-Ne
 constexpr int kMaxOrbContr[3] = {3, 2, 1};  // general contractions per l (cc-pVDZ O)
 constexpr int kBoysTerms = 8;
-constexpr int kBoysOrders = 2 * kMaxOrbL + kMaxAuxL + kBoysTerms;  // 16
+// one order more than the integrals need, for their first derivatives
+constexpr int kBoysOrders = 2 * kMaxOrbL + kMaxAuxL + 1 + kBoysTerms;  // 17
 constexpr double kBoysStep = 0.05;
 constexpr double kBoysTmax = 36.0;
 constexpr int kBoysGrid = 721;  // T = 0 .. 36 inclusive
@@ -66,6 +67,14 @@ __host__ __device__ constexpr int c2s_offset(int l) {
     return o;
 }
 constexpr int kC2sSize = 1 + 9 + 30 + 70 + 135;
+
+// Primitive pairs whose |c_a c_b| exp(-mu R_AB^2) falls below this contribute
+// less than ~1e-15 to any (P|ab) and are skipped (the reference evaluates every
+// primitive triple; the difference is far below its 1e-12 integral tolerance).
+constexpr double kPairScreen = 1e-22;
+constexpr int kMaxPrimPairs = 256;
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTwoPi52 = 34.98683665524972;  // 2 pi^(5/2)
 // The matrices live in __constant__ memory of the translation unit that uses them.
 
 // F_0..F_L at T. `table` is [kBoysGrid][kBoysOrders].

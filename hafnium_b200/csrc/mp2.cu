@@ -86,6 +86,51 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 }  // namespace
 
+cudaError_t occupied_pair_tensor_t(const JkPlan& p, const double* C, int64_t ncol, int64_t nocc, double* Gt,
+                                   cudaStream_t stream) {
+    const int64_t n = p.n, npad = (int64_t)p.nt * 64, naux = p.naux;
+    if (nocc < 1) return cudaSuccess;
+    const int opad = (int)std::max<int64_t>(64, round_up(nocc, 64));
+    const int64_t per_q = (int64_t)opad * (npad + opad) * 8;
+    const int qc_max = (int)std::max<int64_t>(1, std::min<int64_t>(naux, ((int64_t)1 << 30) / per_q));
+    double *Cot = nullptr, *Xt = nullptr, *W = nullptr;
+    cudaError_t e;
+    if ((e = cudaMallocAsync((void**)&Cot, sizeof(double) * (size_t)opad * npad, stream)) != cudaSuccess) return e;
+    if ((e = cudaMallocAsync((void**)&Xt, sizeof(double) * (size_t)qc_max * opad * npad, stream)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&W, sizeof(double) * (size_t)qc_max * opad * opad, stream)) != cudaSuccess) {
+        cudaFreeAsync(Cot, stream);
+        if (Xt) cudaFreeAsync(Xt, stream);
+        return e;
+    }
+    k_columns_t<<<(unsigned)((opad * npad + 255) / 256), 256, 0, stream>>>(C, n, ncol, 0, nocc, Cot, opad, npad);
+    for (int q0 = 0; q0 < naux && e == cudaSuccess; q0 += qc_max) {
+        const int qc = (int)std::min<int64_t>(qc_max, naux - q0);
+        e = half_transform_t(p, Cot, opad, q0, qc, Xt, stream);
+        if (e != cudaSuccess) break;
+        GemmArgs g{};
+        g.M = qc * opad;
+        g.N = (int)nocc;
+        g.K = (int)npad;
+        g.A = Xt;
+        g.lda = npad;
+        g.B = Cot;
+        g.ldb = npad;
+        g.C = W;
+        g.ldc = opad;
+        g.alpha = 1.0;
+        g.beta = 0.0;
+        e = dgemm_nt(g, 1, stream);
+        if (e != cudaSuccess) break;
+        dim3 grid((unsigned)((nocc * nocc + 31) / 32), (unsigned)((qc + 31) / 32));
+        k_transpose_ov<<<grid, dim3(32, 8), 0, stream>>>(W, opad, opad, qc, (int)nocc, (int)nocc, naux, q0, Gt);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(Cot, stream);
+    cudaFreeAsync(Xt, stream);
+    cudaFreeAsync(W, stream);
+    return e;
+}
+
 cudaError_t mp2_energy(const JkPlan& p, const double* C, int64_t nmo, const double* eps, int64_t nocc,
                        double* correlation, cudaStream_t stream) {
     const int64_t n = p.n, npad = (int64_t)p.nt * 64, naux = p.naux;

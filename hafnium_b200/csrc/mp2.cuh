@@ -12,4 +12,10 @@ namespace hf {
 cudaError_t mp2_energy(const JkPlan& p, const double* C, int64_t nmo, const double* eps, int64_t nocc,
                        double* correlation, cudaStream_t stream);
 
+// The fitted tensor in the occupied orbital basis with the auxiliary index
+// contiguous: Gt[(i * nocc + j)][Q] = sum_{pq} C[p][i] B_Q[p][q] C[q][j] for
+// the first nocc columns of C [n][ncol] (device). Temporaries are stream-ordered.
+cudaError_t occupied_pair_tensor_t(const JkPlan& p, const double* C, int64_t ncol, int64_t nocc, double* Gt,
+                                   cudaStream_t stream);
+
 }  // namespace hf

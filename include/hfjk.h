@@ -137,6 +137,20 @@ int hf_four_center(hf_ctx* ctx, double* out, int on_device);
 int hf_mp2_energy(hf_ctx* ctx, const double* mo_coefficients, const double* mo_energies, int64_t n_mo, int64_t n_occ,
                   double* correlation, int on_device);
 
+/* Analytic nuclear gradient of the DF-RHF energy of a converged closed-shell
+ * state (hafnium/properties/gradient.py:72-149, nuclear_gradient, restricted
+ * class): terms [5][natoms][3] in Hartree/Bohr, in the order nuclear
+ * repulsion, one-electron, overlap, Coulomb, exchange (NuclearGradient,
+ * gradient.py:44-69; their sum is the gradient). C: the occupied orbitals
+ * [n_ao][nocc] (D = C C^T per spin); W: the energy-weighted density 2 D F D
+ * [n_ao][n_ao]; charges [natoms] and positions [natoms][3] (Bohr) are host
+ * arrays, and every shell must sit on one of those atoms. The derivative
+ * integrals are contracted with their weights as they are formed, never
+ * stored. C, W and terms are device pointers when on_device, else host.
+ * Frees the context's split-BF16 copy of B (rebuilt on its next use). */
+int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double* W, const double* charges,
+                        const double* positions, int64_t natoms, double* terms, int on_device);
+
 int hf_get_stats(const hf_ctx* ctx, hf_stats* out);
 
 #ifdef __cplusplus
