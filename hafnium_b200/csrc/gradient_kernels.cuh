@@ -386,7 +386,9 @@ static cudaError_t three_center_grad_one(const PairTask* tasks, int ntasks, int 
     constexpr int SPB = 128 / nsph(LP);
     const size_t smem = sizeof(double) * (size_t)max_npp * GradPairLayout<LA, LB>::STRIDE;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
-    if (smem > 48 * 1024) {
+    // the attribute covers the dynamic part; the static part (pair list, reduction)
+    // counts against the 48 KB default too
+    if (smem > 40 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_three_center_grad<LA, LB, LP>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;

@@ -442,7 +442,9 @@ static cudaError_t three_center_one(const PairTask* tasks, int ntasks, int max_n
     if (ntasks == 0 || nalist == 0) return cudaSuccess;
     constexpr int SPB = 128 / nsph(LP);
     const size_t smem = sizeof(double) * (size_t)max_npp * PairLayout<LA, LB>::STRIDE;
-    if (smem > 48 * 1024) {
+    // the attribute covers the dynamic part; the static pair list counts against
+    // the 48 KB default too
+    if (smem > 40 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_three_center<LA, LB, LP>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
