@@ -75,6 +75,10 @@ class StatsC(ctypes.Structure):
         ("b_bytes", ctypes.c_int64),
         ("exchange_rank", ctypes.c_int64),
         ("kernel_launches", ctypes.c_int64),
+        ("ms_gradient_weights", ctypes.c_double),
+        ("ms_gradient_metric", ctypes.c_double),
+        ("ms_gradient_three_center", ctypes.c_double),
+        ("ms_gradient_one_electron", ctypes.c_double),
     ]
 
 

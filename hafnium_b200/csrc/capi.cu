@@ -1172,6 +1172,8 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
         return dgemm_nt(g, 1, ctx->stream);
     };
     // total density D = 2 C C^T and the fitted charges d = L^-1 (P|uv) D
+    ctx->stats.ms_gradient_weights = 0.0;
+    time_begin(ctx);
     HF_CU(gemm((int)n, (int)n, (int)o, dC, o, dC, o, Dt, n, 2.0, 0, 0));
     HF_CU(fitted_charges(p, Dt, dfit, work, ctx->stream));
     // the metric's factor M = L L^T and its inverse
@@ -1193,9 +1195,12 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
     // metric weights: W^J = -c c^T / 2, W^K = Gamma Gamma^T (gradient.py:127-145)
     HF_CU(gemm((int)N, (int)N, 1, cfit, 1, cfit, 1, WJ, N, -0.5, 0, 0));
     HF_CU(gemm((int)N, (int)N, (int)oo, G, oo, G, oo, WK, N, 1.0, 0, 0));
+    ctx->stats.ms_gradient_weights += time_end(ctx);
+    time_begin(ctx);
     HF_CU(launch_metric_grad(ctx->d_aux, ctx->d_exps, ctx->d_coefs, ctx->d_aux_by_l, ctx->aux_count, ctx->d_btable,
                              WJ, WK, N, gaux, ctx->stream));
     ctx->stats.kernel_launches += 25;
+    ctx->stats.ms_gradient_metric = time_end(ctx);
     // three-centre derivatives over blocks of auxiliary functions, with the
     // exchange weight GK_P = -2 C Gamma_P C^T of the block formed by two GEMMs
     std::vector<PairTask> tasks[3][3];
@@ -1229,6 +1234,7 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
     double* Zt = tmp.take((size_t)n * o * (pb_max + 8));
     double* GK = tmp.take(nn * (pb_max + 8));
     if (!Zt || !GK) return fail(ctx, HF_ERR_OOM, "no room for the exchange weights of a block");
+    time_begin(ctx);
     int class_start[kMaxAuxL + 1];
     for (int l = 0, c = 0; l <= kMaxAuxL; ++l) {
         class_start[l] = c;
@@ -1263,7 +1269,9 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
             }
         s0 = s1;
     }
+    ctx->stats.ms_gradient_three_center = time_end(ctx);
     // one-electron terms over all ordered shell pairs
+    time_begin(ctx);
     std::vector<int2> pairs1[3][3];
     for (int a = 0; a < nso; ++a)
         for (int b = 0; b < nso; ++b) pairs1[ctx->orb[a].l][ctx->orb[b].l].push_back(make_int2(a, b));
@@ -1284,6 +1292,7 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
                 off += v.size();
             }
     }
+    ctx->stats.ms_gradient_one_electron = time_end(ctx);
     std::vector<double> h((size_t)(2 * nso + nsa) * 6 + 3 * natoms);
     HF_CU(cudaMemcpyAsync(h.data(), acc, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
     HF_CU(cudaStreamSynchronize(ctx->stream));

@@ -1,13 +1,14 @@
 """A small, fixed workload for kernel profiling (ncu) and kernel timing.
 
-    python -m hafnium_b200.profile_case [--waters 16] [--repeats 1] [--batched 0]
+    python -m hafnium_b200.profile_case [--waters 16] [--repeats 1] [--batched 0] [--gradient]
 
 Builds one seeded (H2O)n (one-electron integrals, metric, factor, three-centre
 integrals, fitted tensor), then runs ``repeats`` of each build on the
 occupied orbitals of a converged-looking density (the core-Hamiltonian
 orbitals; the kernels do not depend on the values): J, FP64 K, split-BF16 K.
 With ``--batched C`` it also converges C seeded (H2O)2 clusters through the
-batched graph-resident SCF. Prints one JSON line with the device time of each
+batched graph-resident SCF; with ``--gradient`` it times the DF-RHF nuclear
+gradient of the same orbitals (the kernels do not depend on the values). Prints one JSON line with the device time of each
 step (CUDA events), so the same command gives both the timing and, under
 ``ncu``, the launch list of a bounded number of kernels.
 """
@@ -24,6 +25,7 @@ def main() -> None:
     ap.add_argument("--repeats", type=int, default=1)
     ap.add_argument("--batched", type=int, default=0)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--gradient", action="store_true", help="also time the DF-RHF nuclear gradient")
     args = ap.parse_args()
 
     import torch
@@ -64,6 +66,17 @@ def main() -> None:
     out["exchange_fp64_tflops"] = 4.0 * naux * n * n * o / (out["exchange_fp64_ms"] / 1e3) / 1e12
     out["exchange_bf16_exec_tflops"] = 3 * 4.0 * naux * n * n * o / (out["exchange_bf16_ms"] / 1e3) / 1e12
     out["coulomb_gbs"] = 2.0 * two_body.stats()["b_bytes"] / (out["coulomb_ms"] / 1e3) / 1e9
+    if args.gradient:
+        from hafnium_b200.gradient import gradient_from_state
+
+        e0.record()
+        gradient_from_state(two_body, occ, ham.h, mol)
+        e1.record()
+        e1.synchronize()
+        out["gradient_ms"] = e0.elapsed_time(e1)
+        st = two_body.stats()
+        out["gradient_stages_ms"] = {k: st[f"ms_gradient_{k}"] for k in
+                                     ("weights", "metric", "three_center", "one_electron")}
     del ham, two_body
     torch.cuda.empty_cache()
     if args.batched:

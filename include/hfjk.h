@@ -65,6 +65,10 @@ typedef struct hf_stats {
     int64_t b_bytes;        /* bytes of the packed fitted tensor */
     int64_t exchange_rank;  /* columns of the last exchange factor */
     int64_t kernel_launches;/* launches issued by this context so far */
+    double ms_gradient_weights; /* last gradient: densities, metric factor, Gamma, metric weights */
+    double ms_gradient_metric;  /* last gradient: (dP P|Q) against the metric weights */
+    double ms_gradient_three_center; /* last gradient: exchange weights and (dP P|uv), (P|dA uv) */
+    double ms_gradient_one_electron; /* last gradient: S, T, V derivatives */
 } hf_stats;
 
 /* Context lifetime (no reference counterpart: the reference's kernels are
