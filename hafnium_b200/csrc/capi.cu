@@ -1093,12 +1093,18 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
     int st;
     if ((st = shell_atoms(ctx, ctx->orb, positions, natoms, orb_atom, "orbital")) != HF_OK) return st;
     if ((st = shell_atoms(ctx, ctx->aux, positions, natoms, aux_atom, "auxiliary")) != HF_OK) return st;
-    // the split-BF16 copy of B is not needed here; its room goes to the gradient
-    release(ctx->d_bf16_b);
     upload_gradient_tables(ctx->stream);
     const JkPlan p = plan_of(ctx);
     const int64_t n = ctx->n, N = ctx->naux, o = nocc, oo = nocc * nocc;
     const size_t nn = (size_t)n * n, NN = (size_t)N * N;
+    {
+        // the split-BF16 copy of B is not needed here: its room goes to the
+        // gradient when the intermediates (and 2 GB of exchange weights) do not fit
+        size_t freeb = 0, totalb = 0;
+        cudaMemGetInfo(&freeb, &totalb);
+        const size_t need = sizeof(double) * (2 * (size_t)oo * N + 5 * NN + 4 * nn) + ((size_t)2 << 30);
+        if (ctx->d_bf16_b && freeb < need) release(ctx->d_bf16_b);
+    }
     const int nso = (int)ctx->orb.size(), nsa = (int)ctx->aux.size();
     struct Temps {
         hf_ctx* c;

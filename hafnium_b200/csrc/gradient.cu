@@ -1,6 +1,7 @@
 // The DF-RHF nuclear gradient's derivative-integral kernels
 // (gradient_kernels.cuh), in their own translation unit with their own copy of
 // the constant tables the integral kernels read.
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <vector>

@@ -210,13 +210,19 @@ __device__ __forceinline__ void cta_sum12(double* v, double* red) {
     }
 }
 
-// One CTA per orbital shell pair of class (LA <= LB) and slab of auxiliary shells
-// of class LP from this block's list; one thread per (auxiliary shell, m_P).
+// One CTA per orbital shell pair of class (LA <= LB) and group of slabs of
+// auxiliary shells of class LP from this block's list (slab blockIdx.y, then
+// every gridDim.y-th); one thread per (auxiliary shell, m_P) of a slab.
 // Accumulates, for the Coulomb (slot 0..2) and exchange (slot 3..5) weights,
 // the auxiliary-centre derivative into gaux[aux shell][6] and the two orbital
 // centres' derivatives into gorb[orbital shell][6].
+// Threads per CTA of the three-centre derivative kernel: with the pair data of
+// the larger classes at 50-90 KB of shared memory, two CTAs fit an SM, so the
+// CTA is made wide to keep 16 warps resident.
+constexpr int kGradThreads = 256;
+
 template <int LA, int LB, int LP>
-__global__ void __launch_bounds__(128) k_three_center_grad(const PairTask* __restrict__ tasks,
+__global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTask* __restrict__ tasks,
                                                            const DevShell* __restrict__ orb,
                                                            const DevShell* __restrict__ aux,
                                                            const double* __restrict__ exps,
@@ -228,10 +234,10 @@ __global__ void __launch_bounds__(128) k_three_center_grad(const PairTask* __res
     constexpr int L = LA + LB + LP + 1;
     constexpr int LAB = LA + LB;
     constexpr int NCP = ncart(LP), NSP = nsph(LP);
-    constexpr int SPB = 128 / NSP;
+    constexpr int SPB = kGradThreads / NSP;
     extern __shared__ double smem[];
     __shared__ int s_pos[kMaxPrimPairs + 1];
-    __shared__ double red[4 * 12];
+    __shared__ double red[kGradThreads / 32 * 12];
     const PairTask task = tasks[blockIdx.x];
     const int ia_shell = task.swap ? task.second : task.first;
     const int ib_shell = task.swap ? task.first : task.second;
@@ -241,19 +247,25 @@ __global__ void __launch_bounds__(128) k_three_center_grad(const PairTask* __res
     if (npp == 0) return;
 
     const int slot = threadIdx.x / NSP, mp = threadIdx.x % NSP;
-    const int ia = blockIdx.y * SPB + slot;
-    const bool active = slot < SPB && ia < nalist;
-    // acc: Q_J[3] Q_K[3] A_J[3] A_K[3] (J parts without the factor c_P)
-    double acc[12];
+    const int nslabs = (nalist + SPB - 1) / SPB;
+    const double fac = task.first == task.second ? 1.0 : 2.0;
+    // per-thread sums over the slabs for the two orbital centres:
+    // A_J[3] A_K[3] B_J[3] B_K[3] (J parts with the factor c_P applied)
+    double v[12];
 #pragma unroll
-    for (int k = 0; k < 12; ++k) acc[k] = 0.0;
-    double cP = 0.0;
-    int pshell = 0;
-    if (active) {
-        pshell = alist[ia];
+    for (int k = 0; k < 12; ++k) v[k] = 0.0;
+    // this CTA's pair data stays in shared memory while it walks over slabs
+    for (int slab = blockIdx.y; slab < nslabs; slab += gridDim.y) {
+        const int ia = slab * SPB + slot;
+        if (slot >= SPB || ia >= nalist) continue;
+        // acc: Q_J[3] Q_K[3] A_J[3] A_K[3] (J parts without the factor c_P)
+        double acc[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) acc[k] = 0.0;
+        const int pshell = alist[ia];
         const DevShell P = aux[pshell];
         const int pf = P.fn + mp;
-        cP = g.cfit[pf];
+        const double cP = g.cfit[pf];
         double gk[PL::KK][PL::NSAB];
 #pragma unroll
         for (int ka = 0; ka < PL::KA; ++ka)
@@ -263,12 +275,12 @@ __global__ void __launch_bounds__(128) k_three_center_grad(const PairTask* __res
                 for (int ma = 0; ma < PL::NSA; ++ma)
 #pragma unroll
                     for (int mb = 0; mb < PL::NSB; ++mb) {
-                        double v = 0.0;
+                        double val = 0.0;
                         if (ka < A.ncontr && kb < B.ncontr) {
                             const int64_t mu = A.fn + ka * PL::NSA + ma, nu = B.fn + kb * PL::NSB + mb;
-                            v = g.GK[(mu * g.n + nu) * g.Pb + (pf - g.P0)];
+                            val = g.GK[(mu * g.n + nu) * g.Pb + (pf - g.P0)];
                         }
-                        gk[ka * PL::KB + kb][ma * PL::NSB + mb] = v;
+                        gk[ka * PL::KB + kb][ma * PL::NSB + mb] = val;
                     }
         double crow[NCP];
 #pragma unroll
@@ -314,10 +326,10 @@ __global__ void __launch_bounds__(128) k_three_center_grad(const PairTask* __res
                 double w[PL::NSAB];
 #pragma unroll
                 for (int m = 0; m < PL::NSAB; ++m) {
-                    double v = 0.0;
+                    double x = 0.0;
 #pragma unroll
-                    for (int k = 0; k < PL::KK; ++k) v += s[4 + k] * gk[k][m];
-                    w[m] = v;
+                    for (int k = 0; k < PL::KK; ++k) x += s[4 + k] * gk[k][m];
+                    w[m] = x;
                 }
                 const double* et = s + PL::OFF_E;
                 const double* ea = s + PL::OFF_EA;
@@ -350,23 +362,16 @@ __global__ void __launch_bounds__(128) k_three_center_grad(const PairTask* __res
                 }
             }
         }
-    }
-    const double fac = task.first == task.second ? 1.0 : 2.0;
-    if (active) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             atomicAdd(gaux + (int64_t)pshell * 6 + d, fac * cP * acc[d]);
             atomicAdd(gaux + (int64_t)pshell * 6 + 3 + d, fac * acc[3 + d]);
+            // first centre: A; second: B = -(Q + A)
+            v[d] += cP * acc[6 + d];
+            v[3 + d] += acc[9 + d];
+            v[6 + d] -= cP * (acc[d] + acc[6 + d]);
+            v[9 + d] -= acc[3 + d] + acc[9 + d];
         }
-    }
-    // first centre: A; second: B = -(Q + A)
-    double v[12];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        v[d] = cP * acc[6 + d];
-        v[3 + d] = acc[9 + d];
-        v[6 + d] = -cP * (acc[d] + acc[6 + d]);
-        v[9 + d] = -(acc[3 + d] + acc[9 + d]);
     }
     cta_sum12(v, red);
     if (threadIdx.x == 0) {
@@ -383,7 +388,7 @@ static cudaError_t three_center_grad_one(const PairTask* tasks, int ntasks, int 
                                          const int* alist, int nalist, const double* btable, GradWeights g,
                                          double* gorb, double* gaux, cudaStream_t stream) {
     if (ntasks == 0 || nalist == 0) return cudaSuccess;
-    constexpr int SPB = 128 / nsph(LP);
+    constexpr int SPB = kGradThreads / nsph(LP);
     const size_t smem = sizeof(double) * (size_t)max_npp * GradPairLayout<LA, LB>::STRIDE;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     // the attribute covers the dynamic part; the static part (pair list, reduction)
@@ -393,8 +398,11 @@ static cudaError_t three_center_grad_one(const PairTask* tasks, int ntasks, int 
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    dim3 grid(ntasks, (nalist + SPB - 1) / SPB);
-    k_three_center_grad<LA, LB, LP><<<grid, 128, smem, stream>>>(tasks, orb, aux, exps, coefs, alist, nalist, btable,
+    // one slab per CTA: walking several slabs with one CTA (to build the pair
+    // data once) measured slower, the CTAs' costs being too uneven
+    const int nslabs = (nalist + SPB - 1) / SPB;
+    dim3 grid(ntasks, nslabs);
+    k_three_center_grad<LA, LB, LP><<<grid, kGradThreads, smem, stream>>>(tasks, orb, aux, exps, coefs, alist, nalist, btable,
                                                                  g, gorb, gaux);
     return cudaGetLastError();
 }

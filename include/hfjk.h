@@ -151,7 +151,8 @@ int hf_mp2_energy(hf_ctx* ctx, const double* mo_coefficients, const double* mo_e
  * arrays, and every shell must sit on one of those atoms. The derivative
  * integrals are contracted with their weights as they are formed, never
  * stored. C, W and terms are device pointers when on_device, else host.
- * Frees the context's split-BF16 copy of B (rebuilt on its next use). */
+ * Frees the context's split-BF16 copy of B when the intermediates would not
+ * fit beside it (it is rebuilt on its next use). */
 int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double* W, const double* charges,
                         const double* positions, int64_t natoms, double* terms, int on_device);
 
