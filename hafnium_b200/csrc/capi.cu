@@ -1207,6 +1207,7 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
                              WJ, WK, N, gaux, ctx->stream));
     ctx->stats.kernel_launches += 25;
     ctx->stats.ms_gradient_metric = time_end(ctx);
+    time_begin(ctx);
     // three-centre derivatives over blocks of auxiliary functions, with the
     // exchange weight GK_P = -2 C Gamma_P C^T of the block formed by two GEMMs
     std::vector<PairTask> tasks[3][3];
@@ -1220,7 +1221,26 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
                 return fail(ctx, HF_ERR_ARG, "a shell pair has too many primitive pairs for the gradient kernel");
         }
     PairTask* d_tasks = reinterpret_cast<PairTask*>(tmp.take((ntask * sizeof(PairTask) + 7) / 8 + 1));
-    if (!d_tasks) return fail(ctx, HF_ERR_OOM, "no room for the gradient's pair list");
+    // every pair's Hermite data, built once for all auxiliary classes and blocks
+    std::vector<int64_t> pair_off(ntask + 1, 0);
+    {
+        size_t t = 0;
+        for (int la = 0; la <= 2; ++la)
+            for (int lb = la; lb <= 2; ++lb) {
+                const int64_t stride = (int64_t)(three_center_grad_smem(la, lb, 1) / sizeof(double));
+                for (const PairTask& pt : tasks[la][lb]) {
+                    pair_off[t + 1] = pair_off[t] + (int64_t)ctx->orb[pt.first].nprim * ctx->orb[pt.second].nprim * stride;
+                    ++t;
+                }
+            }
+    }
+    int64_t* d_pair_off = reinterpret_cast<int64_t*>(tmp.take(ntask + 1));
+    int* d_npps = reinterpret_cast<int*>(tmp.take(ntask / 2 + 1));
+    double* pair_data = tmp.take((size_t)pair_off[ntask]);
+    if (!d_tasks || !d_pair_off || !d_npps || !pair_data)
+        return fail(ctx, HF_ERR_OOM, "no room for the gradient's pair list and pair data");
+    HF_CU(cudaMemcpyAsync(d_pair_off, pair_off.data(), sizeof(int64_t) * (ntask + 1), cudaMemcpyHostToDevice,
+                          ctx->stream));
     {
         size_t off = 0;
         for (int la = 0; la <= 2; ++la)
@@ -1229,6 +1249,10 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
                 if (v.empty()) continue;
                 HF_CU(cudaMemcpyAsync(d_tasks + off, v.data(), sizeof(PairTask) * v.size(), cudaMemcpyHostToDevice,
                                       ctx->stream));
+                HF_CU(launch_grad_pair_data(la, lb, d_tasks + off, (int)v.size(), max_npp[la][lb], ctx->d_orb,
+                                            ctx->d_exps, ctx->d_coefs, Dt, n,
+                                            GradPairData{d_pair_off + off, pair_data, d_npps + off}, ctx->stream));
+                ++ctx->stats.kernel_launches;
                 off += v.size();
             }
     }
@@ -1240,7 +1264,6 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
     double* Zt = tmp.take((size_t)n * o * (pb_max + 8));
     double* GK = tmp.take(nn * (pb_max + 8));
     if (!Zt || !GK) return fail(ctx, HF_ERR_OOM, "no room for the exchange weights of a block");
-    time_begin(ctx);
     int class_start[kMaxAuxL + 1];
     for (int l = 0, c = 0; l <= kMaxAuxL; ++l) {
         class_start[l] = c;
@@ -1269,7 +1292,8 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
                 if (v.empty()) continue;
                 HF_CU(launch_three_center_grad(la, lb, d_tasks + off, (int)v.size(), max_npp[la][lb], ctx->d_orb,
                                                ctx->d_aux, ctx->d_exps, ctx->d_coefs, alist, count, ctx->d_btable, gw,
-                                               gorb, gaux, ctx->stream));
+                                               GradPairData{d_pair_off + off, pair_data, d_npps + off}, gorb, gaux,
+                                               ctx->stream));
                 ctx->stats.kernel_launches += 5;
                 off += v.size();
             }

@@ -210,17 +210,41 @@ __device__ __forceinline__ void cta_sum12(double* v, double* red) {
     }
 }
 
+// Threads per CTA of the three-centre derivative kernel: with the pair data of
+// the larger classes at 50-90 KB of shared memory, two CTAs fit an SM, so the
+// CTA is made wide to keep 16 warps resident.
+constexpr int kGradThreads = 256;
+
+// The pair data of grad_pair_prologue, built once per shell pair into global
+// memory (data + offsets[task], npp * STRIDE doubles; npps[task] = the primitive
+// pairs kept) for every auxiliary class and block to copy.
+template <int LA, int LB>
+__global__ void __launch_bounds__(kGradThreads) k_grad_pair_data(const PairTask* __restrict__ tasks,
+                                                                 const DevShell* __restrict__ orb,
+                                                                 const double* __restrict__ exps,
+                                                                 const double* __restrict__ coefs,
+                                                                 const double* __restrict__ D, int64_t n,
+                                                                 const int64_t* __restrict__ offsets,
+                                                                 double* __restrict__ data, int* __restrict__ npps) {
+    using PL = GradPairLayout<LA, LB>;
+    extern __shared__ double smem[];
+    __shared__ int s_pos[kMaxPrimPairs + 1];
+    const PairTask task = tasks[blockIdx.x];
+    const DevShell A = orb[task.swap ? task.second : task.first];
+    const DevShell B = orb[task.swap ? task.first : task.second];
+    const int npp = grad_pair_prologue<LA, LB>(A, B, exps, coefs, D, n, smem, s_pos);
+    double* dst = data + offsets[blockIdx.x];
+    const int total = npp * PL::STRIDE;
+    for (int k = threadIdx.x; k < total; k += blockDim.x) dst[k] = smem[k];
+    if (threadIdx.x == 0) npps[blockIdx.x] = npp;
+}
+
 // One CTA per orbital shell pair of class (LA <= LB) and group of slabs of
 // auxiliary shells of class LP from this block's list (slab blockIdx.y, then
 // every gridDim.y-th); one thread per (auxiliary shell, m_P) of a slab.
 // Accumulates, for the Coulomb (slot 0..2) and exchange (slot 3..5) weights,
 // the auxiliary-centre derivative into gaux[aux shell][6] and the two orbital
 // centres' derivatives into gorb[orbital shell][6].
-// Threads per CTA of the three-centre derivative kernel: with the pair data of
-// the larger classes at 50-90 KB of shared memory, two CTAs fit an SM, so the
-// CTA is made wide to keep 16 warps resident.
-constexpr int kGradThreads = 256;
-
 template <int LA, int LB, int LP>
 __global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTask* __restrict__ tasks,
                                                            const DevShell* __restrict__ orb,
@@ -229,6 +253,9 @@ __global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTa
                                                            const double* __restrict__ coefs,
                                                            const int* __restrict__ alist, int nalist,
                                                            const double* __restrict__ btable, GradWeights g,
+                                                           const int64_t* __restrict__ offsets,
+                                                           const double* __restrict__ pdata,
+                                                           const int* __restrict__ npps,
                                                            double* __restrict__ gorb, double* __restrict__ gaux) {
     using PL = GradPairLayout<LA, LB>;
     constexpr int L = LA + LB + LP + 1;
@@ -236,15 +263,20 @@ __global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTa
     constexpr int NCP = ncart(LP), NSP = nsph(LP);
     constexpr int SPB = kGradThreads / NSP;
     extern __shared__ double smem[];
-    __shared__ int s_pos[kMaxPrimPairs + 1];
     __shared__ double red[kGradThreads / 32 * 12];
     const PairTask task = tasks[blockIdx.x];
     const int ia_shell = task.swap ? task.second : task.first;
     const int ib_shell = task.swap ? task.first : task.second;
     const DevShell A = orb[ia_shell];
     const DevShell B = orb[ib_shell];
-    const int npp = grad_pair_prologue<LA, LB>(A, B, exps, coefs, g.D, g.n, smem, s_pos);
-    if (npp == 0) return;
+    const int npp = npps[blockIdx.x];
+    if (npp == 0) return;  // nothing survives screening
+    {
+        const double* src = pdata + offsets[blockIdx.x];
+        const int total = npp * PL::STRIDE;
+        for (int k = threadIdx.x; k < total; k += blockDim.x) smem[k] = src[k];
+    }
+    __syncthreads();
 
     const int slot = threadIdx.x / NSP, mp = threadIdx.x % NSP;
     const int nslabs = (nalist + SPB - 1) / SPB;
@@ -386,7 +418,7 @@ template <int LA, int LB, int LP>
 static cudaError_t three_center_grad_one(const PairTask* tasks, int ntasks, int max_npp, const DevShell* orb,
                                          const DevShell* aux, const double* exps, const double* coefs,
                                          const int* alist, int nalist, const double* btable, GradWeights g,
-                                         double* gorb, double* gaux, cudaStream_t stream) {
+                                         GradPairData pd, double* gorb, double* gaux, cudaStream_t stream) {
     if (ntasks == 0 || nalist == 0) return cudaSuccess;
     constexpr int SPB = kGradThreads / nsph(LP);
     const size_t smem = sizeof(double) * (size_t)max_npp * GradPairLayout<LA, LB>::STRIDE;
@@ -402,21 +434,22 @@ static cudaError_t three_center_grad_one(const PairTask* tasks, int ntasks, int 
     // data once) measured slower, the CTAs' costs being too uneven
     const int nslabs = (nalist + SPB - 1) / SPB;
     dim3 grid(ntasks, nslabs);
-    k_three_center_grad<LA, LB, LP><<<grid, kGradThreads, smem, stream>>>(tasks, orb, aux, exps, coefs, alist, nalist, btable,
-                                                                 g, gorb, gaux);
+    k_three_center_grad<LA, LB, LP><<<grid, kGradThreads, smem, stream>>>(tasks, orb, aux, exps, coefs, alist, nalist,
+                                                                         btable, g, pd.offsets, pd.data, pd.npps,
+                                                                         gorb, gaux);
     return cudaGetLastError();
 }
 
 cudaError_t launch_three_center_grad(int la, int lb, const PairTask* tasks, int ntasks, int max_npp,
                                      const DevShell* orb, const DevShell* aux, const double* exps,
                                      const double* coefs, const int* const* alist_by_l, const int* count_by_l,
-                                     const double* btable, GradWeights g, double* gorb, double* gaux,
-                                     cudaStream_t stream) {
+                                     const double* btable, GradWeights g, GradPairData pd, double* gorb,
+                                     double* gaux, cudaStream_t stream) {
     cudaError_t e = cudaSuccess;
 #define HF_3CG(LA, LB, LP)                                                                                        \
     if (e == cudaSuccess && la == LA && lb == LB)                                                                 \
         e = three_center_grad_one<LA, LB, LP>(tasks, ntasks, max_npp, orb, aux, exps, coefs, alist_by_l[LP],       \
-                                              count_by_l[LP], btable, g, gorb, gaux, stream);
+                                              count_by_l[LP], btable, g, pd, gorb, gaux, stream);
 #define HF_3CG_P(LA, LB) HF_3CG(LA, LB, 0) HF_3CG(LA, LB, 1) HF_3CG(LA, LB, 2) HF_3CG(LA, LB, 3) HF_3CG(LA, LB, 4)
     HF_3CG_P(0, 0)
     HF_3CG_P(0, 1)
@@ -426,6 +459,34 @@ cudaError_t launch_three_center_grad(int la, int lb, const PairTask* tasks, int 
     HF_3CG_P(2, 2)
 #undef HF_3CG_P
 #undef HF_3CG
+    return e;
+}
+
+template <int LA, int LB>
+static cudaError_t grad_pair_data_one(const PairTask* tasks, int ntasks, int max_npp, const DevShell* orb,
+                                      const double* exps, const double* coefs, const double* D, int64_t n,
+                                      GradPairData pd, cudaStream_t stream) {
+    if (ntasks == 0) return cudaSuccess;
+    const size_t smem = sizeof(double) * (size_t)max_npp * GradPairLayout<LA, LB>::STRIDE;
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    if (smem > 40 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_grad_pair_data<LA, LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    k_grad_pair_data<LA, LB><<<ntasks, kGradThreads, smem, stream>>>(tasks, orb, exps, coefs, D, n, pd.offsets,
+                                                                     pd.data, pd.npps);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grad_pair_data(int la, int lb, const PairTask* tasks, int ntasks, int max_npp,
+                                  const DevShell* orb, const double* exps, const double* coefs, const double* D,
+                                  int64_t n, GradPairData pd, cudaStream_t stream) {
+    cudaError_t e = cudaSuccess;
+#define HF_GPD(LA, LB) \
+    if (la == LA && lb == LB) e = grad_pair_data_one<LA, LB>(tasks, ntasks, max_npp, orb, exps, coefs, D, n, pd, stream);
+    HF_GPD(0, 0) HF_GPD(0, 1) HF_GPD(0, 2) HF_GPD(1, 1) HF_GPD(1, 2) HF_GPD(2, 2)
+#undef HF_GPD
     return e;
 }
 

@@ -89,11 +89,22 @@ struct GradWeights {
 // sums per shell: gorb/gaux [shell][6] (Coulomb x y z, exchange x y z) for the
 // fitted terms, gorb1 [shell][6] (one-electron, overlap) and gatom [atom][3]
 // (the attraction's dependence on the nuclei).
+// Per shell pair of a class: offsets[task] (doubles) into data of its Hermite
+// data, npps[task] its primitive pairs kept (filled by launch_grad_pair_data).
+struct GradPairData {
+    const int64_t* offsets;
+    double* data;
+    int* npps;
+};
+cudaError_t launch_grad_pair_data(int la, int lb, const PairTask* tasks, int ntasks, int max_npp,
+                                  const DevShell* orb, const double* exps, const double* coefs, const double* D,
+                                  int64_t n, GradPairData pd, cudaStream_t stream);
 cudaError_t launch_three_center_grad(int la, int lb, const PairTask* tasks, int ntasks, int max_npp,
                                      const DevShell* orb, const DevShell* aux, const double* exps,
                                      const double* coefs, const int* const* alist_by_l, const int* count_by_l,
-                                     const double* btable, GradWeights g, double* gorb, double* gaux,
-                                     cudaStream_t stream);
+                                     const double* btable, GradWeights g, GradPairData pd, double* gorb,
+                                     double* gaux, cudaStream_t stream);
+// Shared memory of one pair's data: max_npp primitive pairs of class (la, lb).
 size_t three_center_grad_smem(int la, int lb, int max_npp);
 cudaError_t launch_metric_grad(const DevShell* aux, const double* exps, const double* coefs,
                                const int* const* aux_by_l, const int* count, const double* btable, const double* WJ,
