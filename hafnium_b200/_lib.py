@@ -24,7 +24,7 @@ EXPORTS = (
     "hf_ctx_create", "hf_ctx_destroy", "hf_last_error", "hf_set_stream", "hf_shells_upload",
     "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
     "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_four_center", "hf_get_stats",
-    "hf_coulomb_static", "hf_mp2_energy", "hf_nuclear_gradient",
+    "hf_coulomb_static", "hf_mp2_energy", "hf_nuclear_gradient", "hf_mo_fitted_tensor",
 )
 
 BATCH_EXPORTS = (
@@ -123,6 +123,7 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_coulomb_static.argtypes = [v, v, v]
     lib.hf_mp2_energy.argtypes = [v, v, v, i64, i64, ctypes.POINTER(ctypes.c_double), i]
     lib.hf_nuclear_gradient.argtypes = [v, v, i64, v, v, v, i64, v, i]
+    lib.hf_mo_fitted_tensor.argtypes = [v, v, i64, v, i64, v, i]
     lib.hf_get_stats.argtypes = [v, p(StatsC)]
     d = ctypes.c_double
     lib.hf_batch_default_options.argtypes = [p(BatchOptionsC)]
@@ -291,6 +292,29 @@ class Context:
                                             ctypes.byref(out), 0)
         self.check(status, "hf_mp2_energy")
         return float(out.value)
+
+    def mo_fitted_tensor(self, c_bra, c_ket):
+        """B[P, p, q] in an orbital basis, [aux, n_bra, n_ket] (torch CUDA tensors in,
+        a torch CUDA tensor out; or NumPy in and out)."""
+        _, naux = self.dims()
+        if hasattr(c_bra, "data_ptr"):
+            import torch
+
+            cb = c_bra.contiguous()
+            ck = c_ket.contiguous()
+            out = torch.empty((naux, cb.shape[1], ck.shape[1]), dtype=torch.float64, device=cb.device)
+            torch_sync(cb)
+            torch_sync(ck)
+            status = self.lib.hf_mo_fitted_tensor(self.handle, cb.data_ptr(), cb.shape[1], ck.data_ptr(), ck.shape[1],
+                                                  out.data_ptr(), 1)
+        else:
+            cb = np.ascontiguousarray(c_bra, dtype=np.float64)
+            ck = np.ascontiguousarray(c_ket, dtype=np.float64)
+            out = np.empty((naux, cb.shape[1], ck.shape[1]))
+            status = self.lib.hf_mo_fitted_tensor(self.handle, cb.ctypes.data, cb.shape[1], ck.ctypes.data, ck.shape[1],
+                                                  out.ctypes.data, 0)
+        self.check(status, "hf_mo_fitted_tensor")
+        return out
 
     def nuclear_gradient(self, occupied, weighted, charges, positions) -> np.ndarray:
         """The five DF-RHF gradient terms [5, atom, 3] (torch CUDA tensors or NumPy

@@ -1061,6 +1061,40 @@ int hf_mp2_energy(hf_ctx* ctx, const double* mo_coefficients, const double* mo_e
     return HF_OK;
 }
 
+int hf_mo_fitted_tensor(hf_ctx* ctx, const double* c_bra, int64_t n_bra, const double* c_ket, int64_t n_ket,
+                        double* out, int on_device) {
+    if (!ctx || !c_bra || !c_ket || !out || n_bra < 1 || n_ket < 1) return HF_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    cudaSetDevice(ctx->device);
+    const JkPlan p = plan_of(ctx);
+    const int64_t n = ctx->n, N = ctx->naux;
+    const size_t out_doubles = (size_t)N * n_bra * n_ket;
+    double *staged = nullptr, *dout = out;
+    const double *db = c_bra, *dk = c_ket;
+    if (!on_device) {
+        const size_t cb = (size_t)n * n_bra, ck = (size_t)n * n_ket;
+        if (cudaMallocAsync((void**)&staged, sizeof(double) * (cb + ck + out_doubles), ctx->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, HF_ERR_OOM, "no room to stage the orbital-basis tensor");
+        }
+        HF_CU(cudaMemcpyAsync(staged, c_bra, sizeof(double) * cb, cudaMemcpyHostToDevice, ctx->stream));
+        HF_CU(cudaMemcpyAsync(staged + cb, c_ket, sizeof(double) * ck, cudaMemcpyHostToDevice, ctx->stream));
+        db = staged;
+        dk = staged + cb;
+        dout = staged + cb + ck;
+    }
+    cudaError_t e = mo_fitted_tensor(p, db, n_bra, dk, n_ket, nullptr, dout, ctx->stream);
+    ctx->stats.kernel_launches += 2 + 3 * ((N + 63) / 64);
+    if (e == cudaSuccess && !on_device)
+        e = cudaMemcpyAsync(out, dout, sizeof(double) * out_doubles, cudaMemcpyDeviceToHost, ctx->stream);
+    if (staged) cudaFreeAsync(staged, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess)
+        return fail(ctx, e == cudaErrorMemoryAllocation ? HF_ERR_OOM : HF_ERR_CUDA,
+                    std::string("hf_mo_fitted_tensor: ") + cudaGetErrorString(e));
+    return HF_OK;
+}
+
 // The atom of every shell: the one at its centre.
 static int shell_atoms(hf_ctx* ctx, const std::vector<DevShell>& shells, const double* positions, int64_t natoms,
                        std::vector<int>& out, const char* what) {

@@ -131,6 +131,69 @@ cudaError_t occupied_pair_tensor_t(const JkPlan& p, const double* C, int64_t nco
     return e;
 }
 
+// out[Q'][i][a] = W[(ql * bpad + i) * kpad + a] for Q = q0 + ql, Q' = ref[Q] (or Q).
+__global__ void k_scatter_mo(const double* __restrict__ W, int bpad, int64_t kpad, int qc, int q0, int64_t nb,
+                             int64_t nk, const int* __restrict__ ref, double* __restrict__ out) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t per_q = nb * nk;
+    if (e >= per_q * qc) return;
+    const int ql = (int)(e / per_q);
+    const int64_t r = e % per_q;
+    const int64_t i = r / nk, a = r % nk;
+    const int64_t q = ref ? ref[q0 + ql] : q0 + ql;
+    out[q * per_q + r] = W[((int64_t)ql * bpad + i) * kpad + a];
+}
+
+cudaError_t mo_fitted_tensor(const JkPlan& p, const double* Cb, int64_t nb, const double* Ck, int64_t nk,
+                             const int* ref, double* out, cudaStream_t stream) {
+    const int64_t n = p.n, npad = (int64_t)p.nt * 64, naux = p.naux;
+    if (nb < 1 || nk < 1) return cudaSuccess;
+    const int bpad = (int)std::max<int64_t>(64, round_up(nb, 64));
+    const int64_t kpad = round_up(nk, 64);
+    const int64_t per_q = (int64_t)bpad * (npad + kpad) * 8;
+    const int qc_max = (int)std::max<int64_t>(1, std::min<int64_t>(naux, ((int64_t)1 << 30) / per_q));
+    double *Cbt = nullptr, *Ckt = nullptr, *Xt = nullptr, *W = nullptr;
+    cudaError_t e;
+    if ((e = cudaMallocAsync((void**)&Cbt, sizeof(double) * (size_t)bpad * npad, stream)) != cudaSuccess) return e;
+    if ((e = cudaMallocAsync((void**)&Ckt, sizeof(double) * (size_t)kpad * npad, stream)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&Xt, sizeof(double) * (size_t)qc_max * bpad * npad, stream)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&W, sizeof(double) * (size_t)qc_max * bpad * kpad, stream)) != cudaSuccess) {
+        cudaFreeAsync(Cbt, stream);
+        if (Ckt) cudaFreeAsync(Ckt, stream);
+        if (Xt) cudaFreeAsync(Xt, stream);
+        return e;
+    }
+    k_columns_t<<<(unsigned)((bpad * npad + 255) / 256), 256, 0, stream>>>(Cb, n, nb, 0, nb, Cbt, bpad, npad);
+    k_columns_t<<<(unsigned)((kpad * npad + 255) / 256), 256, 0, stream>>>(Ck, n, nk, 0, nk, Ckt, kpad, npad);
+    for (int q0 = 0; q0 < naux && e == cudaSuccess; q0 += qc_max) {
+        const int qc = (int)std::min<int64_t>(qc_max, naux - q0);
+        e = half_transform_t(p, Cbt, bpad, q0, qc, Xt, stream);
+        if (e != cudaSuccess) break;
+        GemmArgs g{};
+        g.M = qc * bpad;
+        g.N = (int)nk;
+        g.K = (int)npad;
+        g.A = Xt;
+        g.lda = npad;
+        g.B = Ckt;
+        g.ldb = npad;
+        g.C = W;
+        g.ldc = kpad;
+        g.alpha = 1.0;
+        g.beta = 0.0;
+        e = dgemm_nt(g, 1, stream);
+        if (e != cudaSuccess) break;
+        const int64_t cnt = nb * nk * qc;
+        k_scatter_mo<<<(unsigned)((cnt + 255) / 256), 256, 0, stream>>>(W, bpad, kpad, qc, q0, nb, nk, ref, out);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(Cbt, stream);
+    cudaFreeAsync(Ckt, stream);
+    cudaFreeAsync(Xt, stream);
+    cudaFreeAsync(W, stream);
+    return e;
+}
+
 cudaError_t mp2_energy(const JkPlan& p, const double* C, int64_t nmo, const double* eps, int64_t nocc,
                        double* correlation, cudaStream_t stream) {
     const int64_t n = p.n, npad = (int64_t)p.nt * 64, naux = p.naux;

@@ -130,6 +130,14 @@ class B200DensityFittedCoulombExchange:
         self.context.exchange_factored_device(c, out, sign, self.precision)
         return out if on_device else out.cpu().numpy()
 
+    def orbital_tensor(self, c_bra, c_ket):
+        """``B[P, p, q]`` in an orbital basis (hafnium/orbitals/integrals.py:73-157,
+        ``transform_df_tensor`` for restricted real orbitals): ``[aux, n_bra, n_ket]``
+        from ``C`` blocks ``[n_ao, n_bra]`` and ``[n_ao, n_ket]``. The auxiliary index
+        is the Cholesky gauge of this fitting; contractions over it are the
+        reference's."""
+        return self.context.mo_fitted_tensor(c_bra, c_ket)
+
     def exchange_factored(self, factor, weights=None, precision: int | None = None):
         """``K`` for ``D = C diag(w) C^T`` with ``C`` of shape ``[n_ao, k]``."""
         prec = self.precision if precision is None else precision

@@ -141,6 +141,17 @@ int hf_four_center(hf_ctx* ctx, double* out, int on_device);
 int hf_mp2_energy(hf_ctx* ctx, const double* mo_coefficients, const double* mo_energies, int64_t n_mo, int64_t n_occ,
                   double* correlation, int on_device);
 
+/* The fitted tensor in an orbital basis (hafnium/orbitals/integrals.py:73-157,
+ * transform_df_tensor for restricted real orbitals without irrep sectors):
+ * out[P][p][q] = sum_uv c_bra[u][p] B[P][u][v] c_ket[v][q], with c_bra
+ * [n_ao][n_bra], c_ket [n_ao][n_ket]; host or device arrays per on_device.
+ * B is the context's Cholesky-fitted tensor L^-1 (P|uv), whose auxiliary index
+ * is an orthogonal rotation of the reference's M^-1/2 (P|uv): every contraction
+ * over P (what the tensor's consumers form) is the reference's, the single
+ * elements are not. */
+int hf_mo_fitted_tensor(hf_ctx* ctx, const double* c_bra, int64_t n_bra, const double* c_ket, int64_t n_ket,
+                        double* out, int on_device);
+
 /* Analytic nuclear gradient of the DF-RHF energy of a converged closed-shell
  * state (hafnium/properties/gradient.py:72-149, nuclear_gradient, restricted
  * class): terms [5][natoms][3] in Hartree/Bohr, in the order nuclear

@@ -2,11 +2,13 @@
 
 Mirrors tests/reference/test_mp2_reference.py:37-80 (stored case: water/STO-3G,
 def2-universal-jkfit, reference converged with TIGHT options) and adds a
-cc-pVDZ water dimer against the oracle's restatement of hafnium/mp/mp2.py.
+cc-pVDZ water dimer against the oracle's restatement of hafnium/mp/mp2.py, and
+the orbital-basis fitted tensor (hf_mo_fitted_tensor) the same consumers read.
 """
 
 from __future__ import annotations
 
+import numpy as np
 import pytest
 
 from oracle import dfrhf
@@ -45,3 +47,26 @@ def test_dfmp2_matches_the_oracle_on_a_dimer():
     result = device_mp2(mol, "cc-pvdz")
     assert abs(result.reference_energy - ref.energy) < 1e-9
     assert abs(result.correlation_energy - expected) < 1e-9
+
+
+def test_orbital_basis_tensor_contractions_match_the_oracle():
+    """transform_df_tensor (orbitals/integrals.py:73-157) on the device: the
+    orbital-basis four-index products sum_P B[P,p,q] B[P,r,s] against the
+    oracle's tensor M^-1/2 (P|uv) (the auxiliary gauges differ by a rotation)."""
+    from hafnium_b200.jk import B200DensityFittedCoulombExchange
+    from oracle import dfrhf
+    from tests.helpers import molecule, tables
+
+    mol = molecule("h2o2_s0")
+    orb, aux = tables(mol)
+    two_body = B200DensityFittedCoulombExchange.from_tables(orb, aux)
+    b = dfrhf.df_tensor(dfrhf.metric(aux), dfrhf.three_center(aux, orb))
+    rng = np.random.default_rng(4)
+    cb = rng.normal(size=(two_body.n_ao, 5)) / np.sqrt(two_body.n_ao)
+    ck = rng.normal(size=(two_body.n_ao, 7)) / np.sqrt(two_body.n_ao)
+    got = two_body.orbital_tensor(cb, ck)
+    want = np.einsum("up,Puv,vq->Ppq", cb, b, ck)
+    assert got.shape == want.shape
+    g = got.reshape(got.shape[0], -1)
+    w = want.reshape(want.shape[0], -1)
+    np.testing.assert_allclose(g.T @ g, w.T @ w, atol=1e-10, rtol=0)
