@@ -327,32 +327,6 @@ __global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTa
                 const double alpha = p * q / (p + q);
                 double R[ntet(L)];
                 hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, R);
-                // G1[h] = sum_c crow[c] R[h + c] (h up to LAB + 1) for the orbital-centre
-                // derivative; GQ[d][h] = -sum_c crow[c] R[h + c + e_d] for the auxiliary centre
-                double G1[PL::NH1];
-                double GQ[3][PL::NH];
-#pragma unroll 1
-                for (int h = 0; h < PL::NH1; ++h) {
-                    const int tu = c_tet_t[h], uu = c_tet_u[h], vu = c_tet_v[h];
-                    double v1 = 0.0;
-#pragma unroll 1
-                    for (int c = 0; c < NCP; ++c)
-                        v1 += crow[c] * R[tet(tu + c_cart[LP][c][0], uu + c_cart[LP][c][1], vu + c_cart[LP][c][2])];
-                    G1[h] = v1;
-                    if (h < PL::NH) {
-                        double gx = 0.0, gy = 0.0, gz = 0.0;
-#pragma unroll 1
-                        for (int c = 0; c < NCP; ++c) {
-                            const int t0 = tu + c_cart[LP][c][0], u0 = uu + c_cart[LP][c][1], v0 = vu + c_cart[LP][c][2];
-                            gx += crow[c] * R[tet(t0 + 1, u0, v0)];
-                            gy += crow[c] * R[tet(t0, u0 + 1, v0)];
-                            gz += crow[c] * R[tet(t0, u0, v0 + 1)];
-                        }
-                        GQ[0][h] = -gx;
-                        GQ[1][h] = -gy;
-                        GQ[2][h] = -gz;
-                    }
-                }
                 const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * cq;
                 // exchange weight of this primitive pair: w[m] = sum_k cc[k] gk[k][m]
                 double w[PL::NSAB];
@@ -367,29 +341,46 @@ __global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTa
                 const double* ea = s + PL::OFF_EA;
                 const double* ej = s + PL::OFF_EJ;
                 const double* eja = s + PL::OFF_EJA;
-                // auxiliary centre
+                // auxiliary centre: -sum_c crow[c] R[h + c + e_d], formed as it is used
 #pragma unroll 1
                 for (int h = 0; h < PL::NH; ++h) {
+                    const int tu = c_tet_t[h], uu = c_tet_u[h], vu = c_tet_v[h];
+                    double gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll 1
+                    for (int c = 0; c < NCP; ++c) {
+                        const int t0 = tu + c_cart[LP][c][0], u0 = uu + c_cart[LP][c][1], v0 = vu + c_cart[LP][c][2];
+                        gx += crow[c] * R[tet(t0 + 1, u0, v0)];
+                        gy += crow[c] * R[tet(t0, u0 + 1, v0)];
+                        gz += crow[c] * R[tet(t0, u0, v0 + 1)];
+                    }
                     double wk = 0.0;
 #pragma unroll
                     for (int m = 0; m < PL::NSAB; ++m) wk += w[m] * et[m * PL::NH + h];
-                    const double wj = ej[h];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        acc[d] += pref * wj * GQ[d][h];
-                        acc[3 + d] += pref * wk * GQ[d][h];
-                    }
+                    const double wj = pref * ej[h];
+                    wk *= pref;
+                    acc[0] -= wj * gx;
+                    acc[1] -= wj * gy;
+                    acc[2] -= wj * gz;
+                    acc[3] -= wk * gx;
+                    acc[4] -= wk * gy;
+                    acc[5] -= wk * gz;
                 }
-                // centre of the first orbital function
+                // centre of the first orbital function: sum_c crow[c] R[h + c], h up to LAB + 1
 #pragma unroll 1
                 for (int h = 0; h < PL::NH1; ++h) {
+                    const int tu = c_tet_t[h], uu = c_tet_u[h], vu = c_tet_v[h];
+                    double g1 = 0.0;
+#pragma unroll 1
+                    for (int c = 0; c < NCP; ++c)
+                        g1 += crow[c] * R[tet(tu + c_cart[LP][c][0], uu + c_cart[LP][c][1], vu + c_cart[LP][c][2])];
+                    g1 *= pref;
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         double wk = 0.0;
 #pragma unroll
                         for (int m = 0; m < PL::NSAB; ++m) wk += w[m] * ea[(d * PL::NSAB + m) * PL::NH1 + h];
-                        acc[6 + d] += pref * eja[d * PL::NH1 + h] * G1[h];
-                        acc[9 + d] += pref * wk * G1[h];
+                        acc[6 + d] += eja[d * PL::NH1 + h] * g1;
+                        acc[9 + d] += wk * g1;
                     }
                 }
             }
