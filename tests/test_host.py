@@ -86,3 +86,25 @@ def test_purification_reports_a_missing_gap():
     fo[2, 2] = fo[3, 3] = 0.0  # degenerate HOMO/LUMO: no projector of rank 3 is singled out
     p, ok = purify(torch.as_tensor(fo), 3)
     assert not ok or abs(float(torch.trace(p)) - 3.0) < 1e-8
+
+
+def test_occupied_factor_reproduces_an_idempotent_density():
+    """hafnium_b200.gradient.occupied_factor: C C^T = D for D S D = D (the form in
+    which the reference's ScfResult gives a state), and the five gradient terms
+    add up to NuclearGradient.total."""
+    from hafnium_b200.gradient import NuclearGradient, occupied_factor
+
+    rng = np.random.default_rng(5)
+    n, k = 12, 4
+    a = rng.normal(size=(n, n))
+    s = a @ a.T / n + np.eye(n)
+    w, v = np.linalg.eigh(s)
+    inv_half = (v / np.sqrt(w)) @ v.T
+    q, _ = np.linalg.qr(rng.normal(size=(n, k)))
+    c = inv_half @ q  # orthonormal in the S metric
+    d = c @ c.T
+    np.testing.assert_allclose(d @ s @ d, d, atol=1e-12)
+    got = occupied_factor(d, s, k)
+    np.testing.assert_allclose(got @ got.T, d, atol=1e-12)
+    terms = [rng.normal(size=(3, 3)) for _ in range(5)]
+    np.testing.assert_allclose(NuclearGradient(*terms).total, sum(terms), atol=0)
