@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ablation", action="store_true",
+                    help="also run SAD+mixed and learned+plain once each (outside the timed steps)")
     ap.add_argument("--batched", type=int, default=0,
                     help="run the batched workload instead: this many seeded (H2O)n, n uniform in [2, 16]")
     return ap.parse_args()
@@ -243,6 +245,21 @@ def run_b200(args) -> None:
     clocks = sampler.stop()
     # kernel-only timing of the exchange builds for the roofline, outside the timed steps
     probe = one_scf(torch, mol, dev, mode="mixed", guess_kind=guess_kind, probe_kernels=True)["kernel_ms"]
+    ablation = None
+    if args.ablation:
+        # which part of the gain is the guess and which the precision schedule, one
+        # untimed-by-the-contract run each (CUDA events around the whole SCF as above)
+        ablation = {}
+        for label, mode, kind in (("sad_mixed", "mixed", "sad"), ("learned_fp64", "fp64", guess_kind)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record()
+            info = one_scf(torch, mol, dev, mode=mode, guess_kind=kind)
+            e1.record()
+            e1.synchronize()
+            ablation[label] = {"seconds": e0.elapsed_time(e1) / 1e3, "iterations": info["iterations"],
+                               "energy": info["energy"], "precisions": info["precisions"],
+                               "scf_s": info["scf"]["scf_s"], "hamiltonian_s": info["scf"]["hamiltonian_s"]}
     step_max, plain_max = max_over_ranks([max(times), max(plain_times)], dev)
     if world > 1:
         dist.barrier()
@@ -336,6 +353,7 @@ def run_b200(args) -> None:
                        "build": plain["build"],
                        "dE_mixed_vs_fp64": last["energy"] - plain["energy"],
                        "max_abs_dD_mixed_vs_fp64": float(np.max(np.abs(last["density"] - plain["density"])))},
+        "ablation": ablation,
         "stages": {"build": last["build"], "per_build_ms": {"coulomb": j_ms, "exchange_fp64": k64_ms,
                                                              "exchange_bf16_kernel": k16_ms,
                                                              "exchange_fp64_kernel": k64_probe_ms,
