@@ -1077,8 +1077,13 @@ int hf_mo_fitted_tensor(hf_ctx* ctx, const double* c_bra, int64_t n_bra, const d
             cudaGetLastError();
             return fail(ctx, HF_ERR_OOM, "no room to stage the orbital-basis tensor");
         }
-        HF_CU(cudaMemcpyAsync(staged, c_bra, sizeof(double) * cb, cudaMemcpyHostToDevice, ctx->stream));
-        HF_CU(cudaMemcpyAsync(staged + cb, c_ket, sizeof(double) * ck, cudaMemcpyHostToDevice, ctx->stream));
+        cudaError_t ec = cudaMemcpyAsync(staged, c_bra, sizeof(double) * cb, cudaMemcpyHostToDevice, ctx->stream);
+        if (ec == cudaSuccess)
+            ec = cudaMemcpyAsync(staged + cb, c_ket, sizeof(double) * ck, cudaMemcpyHostToDevice, ctx->stream);
+        if (ec != cudaSuccess) {
+            cudaFreeAsync(staged, ctx->stream);
+            return fail(ctx, HF_ERR_CUDA, std::string("hf_mo_fitted_tensor: ") + cudaGetErrorString(ec));
+        }
         db = staged;
         dk = staged + cb;
         dout = staged + cb + ck;
