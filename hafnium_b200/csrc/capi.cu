@@ -1239,7 +1239,7 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
     HF_CU(gemm((int)oo, (int)N, (int)N, Gt, N, LinvT, N, G, oo, 1.0, 1, 1));
     // metric weights: W^J = -c c^T / 2, W^K = Gamma Gamma^T (gradient.py:127-145)
     HF_CU(gemm((int)N, (int)N, 1, cfit, 1, cfit, 1, WJ, N, -0.5, 0, 0));
-    HF_CU(gemm((int)N, (int)N, (int)oo, G, oo, G, oo, WK, N, 1.0, 0, 0));
+    HF_CU(gemm((int)N, (int)N, (int)oo, G, oo, G, oo, WK, N, 1.0, 0, 3));  // upper tiles only
     ctx->stats.ms_gradient_weights += time_end(ctx);
     time_begin(ctx);
     HF_CU(launch_metric_grad(ctx->d_aux, ctx->d_exps, ctx->d_coefs, ctx->d_aux_by_l, ctx->aux_count, ctx->d_btable,

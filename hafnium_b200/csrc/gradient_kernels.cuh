@@ -12,7 +12,8 @@
 //                        of auxiliary functions; the derivative for the second
 //                        orbital centre follows from translational invariance,
 //                        d_A + d_B + d_P = 0 (two_electron.rs:300-394).
-//   k_metric_grad        (d_P P|Q) against the metric weights W^J, W^K.
+//   k_metric_grad        (d_P P|Q) against the metric weights W^J, W^K (of W^K only
+//                        the upper triangle is read).
 //   k_one_electron_grad  <d_A u|O|v> for S, T and V against W and D.
 //   k_attraction_nucleus_grad
 //                        <u|d_C V_C|v> against D, one nucleus per grid row.
@@ -556,10 +557,13 @@ __global__ void __launch_bounds__(128) k_metric_grad(const DevShell* __restrict_
                 }
             }
         }
-        const int64_t row = (int64_t)(P.fn + mp) * ldw + Q.fn;
+        const int64_t pr = P.fn + mp;
+        const int64_t row = pr * ldw + Q.fn;
 #pragma unroll
         for (int m = 0; m < NSQ; ++m) {
-            const double wj = WJ[row + m], wk = WK[row + m];
+            // W^K is symmetric and only its upper triangle (row <= column) is formed
+            const int64_t qc = Q.fn + m;
+            const double wj = WJ[row + m], wk = pr <= qc ? WK[row + m] : WK[qc * ldw + pr];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 acc[d] += val[d][m] * wj;

@@ -106,6 +106,7 @@ cudaError_t launch_three_center_grad(int la, int lb, const PairTask* tasks, int 
                                      double* gaux, cudaStream_t stream);
 // Shared memory of one pair's data: max_npp primitive pairs of class (la, lb).
 size_t three_center_grad_smem(int la, int lb, int max_npp);
+// WK: only entries with row <= column are read (its upper triangle).
 cudaError_t launch_metric_grad(const DevShell* aux, const double* exps, const double* coefs,
                                const int* const* aux_by_l, const int* count, const double* btable, const double* WJ,
                                const double* WK, int64_t ldw, double* gaux, cudaStream_t stream);
