@@ -1,6 +1,7 @@
 """A small, fixed workload for kernel profiling (ncu) and kernel timing.
 
     python -m hafnium_b200.profile_case [--waters 16] [--repeats 1] [--batched 0] [--gradient]
+                                        [--columns 0]
 
 Builds one seeded (H2O)n (one-electron integrals, metric, factor, three-centre
 integrals, fitted tensor), then runs ``repeats`` of each build on the
@@ -8,9 +9,11 @@ occupied orbitals of a converged-looking density (the core-Hamiltonian
 orbitals; the kernels do not depend on the values): J, FP64 K, split-BF16 K.
 With ``--batched C`` it also converges C seeded (H2O)2 clusters through the
 batched graph-resident SCF; with ``--gradient`` it times the DF-RHF nuclear
-gradient of the same orbitals (the kernels do not depend on the values). Prints one JSON line with the device time of each
-step (CUDA events), so the same command gives both the timing and, under
-``ncu``, the launch list of a bounded number of kernels.
+gradient of the same orbitals (the kernels do not depend on the values). With
+``--columns W`` the K builds use a random factor of W columns instead of the
+occupied orbitals. Prints one JSON line with the device time of each step (CUDA
+events), so the same command gives both the timing and, under ``ncu``, the
+launch list of a bounded number of kernels.
 """
 
 from __future__ import annotations
@@ -26,6 +29,9 @@ def main() -> None:
     ap.add_argument("--batched", type=int, default=0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--gradient", action="store_true", help="also time the DF-RHF nuclear gradient")
+    ap.add_argument("--columns", type=int, default=0,
+                    help="factor width of the K builds (default: the occupied orbitals), e.g. 320 to give a "
+                         "smaller cluster the (H2O)64 tile shape")
     args = ap.parse_args()
 
     import torch
@@ -48,11 +54,17 @@ def main() -> None:
     x = v / torch.sqrt(w)[None, :]
     _, c = torch.linalg.eigh(x.T @ ham.h @ x)
     occ = (x @ c[:, : int(mol.n_alpha)]).contiguous()
+    if args.columns:
+        gen = torch.Generator(device=occ.device).manual_seed(args.seed)
+        kfac = torch.randn((occ.shape[0], args.columns), generator=gen, dtype=torch.float64, device=occ.device)
+        kfac = (kfac / (occ.shape[0] * args.columns) ** 0.5).contiguous()
+    else:
+        kfac = occ
     d = (occ @ occ.T).contiguous()
     two_body = ham.two_body
     steps = (("coulomb", lambda: two_body.coulomb(2.0 * d)),
-             ("exchange_fp64", lambda: two_body.exchange_factored(occ)),
-             ("exchange_bf16", lambda: two_body.exchange_factored(occ, precision=_lib.PREC_BF16X3)))
+             ("exchange_fp64", lambda: two_body.exchange_factored(kfac)),
+             ("exchange_bf16", lambda: two_body.exchange_factored(kfac, precision=_lib.PREC_BF16X3)))
     for name, fn in steps:
         fn()  # first call allocates scratch (and the BF16 copy of B)
         torch.cuda.synchronize(dev)
@@ -62,7 +74,7 @@ def main() -> None:
         e1.record()
         e1.synchronize()
         out[f"{name}_ms"] = e0.elapsed_time(e1) / args.repeats
-    n, naux, o = ham.n_ao, two_body.n_aux, int(mol.n_alpha)
+    n, naux, o = ham.n_ao, two_body.n_aux, int(kfac.shape[1])
     out["exchange_fp64_tflops"] = 4.0 * naux * n * n * o / (out["exchange_fp64_ms"] / 1e3) / 1e12
     out["exchange_bf16_exec_tflops"] = 3 * 4.0 * naux * n * n * o / (out["exchange_bf16_ms"] / 1e3) / 1e12
     out["coulomb_gbs"] = 2.0 * two_body.stats()["b_bytes"] / (out["coulomb_ms"] / 1e3) / 1e9
