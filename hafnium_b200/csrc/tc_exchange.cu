@@ -334,25 +334,41 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
                 if (P.mode == 0) {
                     const int ql = row / P.npad, p = row % P.npad;
                     const int i0 = n0 + c;
-                    __nv_bfloat16* dh = P.xh + (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
-                    __nv_bfloat16* dl = P.xl + (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
                     if (row < P.m_tiles * BM) {
+                        // 16 columns of one row: 32 contiguous bytes per part, stored as two
+                        // 16-byte vectors (the row stride, opad and i0 are multiples of 16)
                         const int64_t off = (int64_t)p * P.ldx + (int64_t)ql * P.opad + i0;
+                        alignas(16) __nv_bfloat162 hv[8], lv[8];
 #pragma unroll
-                        for (int j = 0; j < 16; j += 2) {
-                            const __nv_bfloat16 h0 = __float2bfloat16_rn(v[j]), h1 = __float2bfloat16_rn(v[j + 1]);
-                            const __nv_bfloat16 l0 = __float2bfloat16_rn(v[j] - __bfloat162float(h0));
-                            const __nv_bfloat16 l1 = __float2bfloat16_rn(v[j + 1] - __bfloat162float(h1));
-                            *reinterpret_cast<__nv_bfloat162*>(dh + j) = __halves2bfloat162(h0, h1);
-                            *reinterpret_cast<__nv_bfloat162*>(dl + j) = __halves2bfloat162(l0, l1);
-                            if (P.xsh) {
-                                // negating both parts negates the split value exactly
-                                const bool n0 = P.sign[i0 + j] < 0.0, n1 = P.sign[i0 + j + 1] < 0.0;
-                                *reinterpret_cast<__nv_bfloat162*>(P.xsh + off + j) =
-                                    __halves2bfloat162(n0 ? __hneg(h0) : h0, n1 ? __hneg(h1) : h1);
-                                *reinterpret_cast<__nv_bfloat162*>(P.xsl + off + j) =
-                                    __halves2bfloat162(n0 ? __hneg(l0) : l0, n1 ? __hneg(l1) : l1);
+                        for (int j = 0; j < 8; ++j) {
+                            const __nv_bfloat16 h0 = __float2bfloat16_rn(v[2 * j]), h1 = __float2bfloat16_rn(v[2 * j + 1]);
+                            const __nv_bfloat16 l0 = __float2bfloat16_rn(v[2 * j] - __bfloat162float(h0));
+                            const __nv_bfloat16 l1 = __float2bfloat16_rn(v[2 * j + 1] - __bfloat162float(h1));
+                            hv[j] = __halves2bfloat162(h0, h1);
+                            lv[j] = __halves2bfloat162(l0, l1);
+                        }
+                        uint4* dh = reinterpret_cast<uint4*>(P.xh + off);
+                        uint4* dl = reinterpret_cast<uint4*>(P.xl + off);
+                        dh[0] = reinterpret_cast<const uint4*>(hv)[0];
+                        dh[1] = reinterpret_cast<const uint4*>(hv)[1];
+                        dl[0] = reinterpret_cast<const uint4*>(lv)[0];
+                        dl[1] = reinterpret_cast<const uint4*>(lv)[1];
+                        if (P.xsh) {
+                            // negating both parts negates the split value exactly
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) {
+                                const bool m0 = P.sign[i0 + 2 * j] < 0.0, m1 = P.sign[i0 + 2 * j + 1] < 0.0;
+                                const __nv_bfloat16 h0 = __low2bfloat16(hv[j]), h1 = __high2bfloat16(hv[j]);
+                                const __nv_bfloat16 l0 = __low2bfloat16(lv[j]), l1 = __high2bfloat16(lv[j]);
+                                hv[j] = __halves2bfloat162(m0 ? __hneg(h0) : h0, m1 ? __hneg(h1) : h1);
+                                lv[j] = __halves2bfloat162(m0 ? __hneg(l0) : l0, m1 ? __hneg(l1) : l1);
                             }
+                            uint4* sh = reinterpret_cast<uint4*>(P.xsh + off);
+                            uint4* sl = reinterpret_cast<uint4*>(P.xsl + off);
+                            sh[0] = reinterpret_cast<const uint4*>(hv)[0];
+                            sh[1] = reinterpret_cast<const uint4*>(hv)[1];
+                            sl[0] = reinterpret_cast<const uint4*>(lv)[0];
+                            sl[1] = reinterpret_cast<const uint4*>(lv)[1];
                         }
                     }
                 } else {
