@@ -608,7 +608,8 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         cudaError_t e = launch_tc(mAh, mAl, mCh, mCl, P, stream);
         if (e != cudaSuccess) return e;
         // stage 2: K += X X^T over this chunk, split over k
-        const int bn2 = 256 <= npad ? 256 : 128;
+        // the n tiles must cover npad exactly (an odd multiple of 128 takes 128-wide tiles)
+        const int bn2 = npad % 256 == 0 ? 256 : 128;
         CUtensorMap mXh, mXl, mXh2, mXl2;
         // B operand: X diag(sign) when the factor is signed
         if (!make_map(&mXh, xh, npad, ldx, BM) || !make_map(&mXl, xl, npad, ldx, BM) ||

@@ -84,3 +84,21 @@ def test_host_array_path_matches_the_device_path():
     host = solve_rhf(ham, guess=guess, schedule=PrecisionSchedule(mode="mixed"), host_io=True)
     assert abs(host.energy - device.energy) <= 1e-8
     assert host.timings["h2d_bytes"] > 0 and host.timings["d2h_bytes"] > 0
+
+
+def test_mixed_schedule_matches_plain_fp64_at_an_odd_padding():
+    """(H2O)12: n = 288, padded to 384 for the split-BF16 builds (an odd multiple of
+    128). The mixed schedule reaches the plain FP64 path's energy and density."""
+    from hafnium_b200.molecule import water_cluster
+    from hafnium_b200.scf import PrecisionSchedule, atomic_density_guess
+
+    mol = water_cluster(12, 3)
+    ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
+    guess = atomic_density_guess(mol, "cc-pvdz")
+    options = ScfOptions(energy_tolerance=1e-11, gradient_tolerance=1e-8)
+    plain = solve_rhf(ham, guess=guess, options=options)
+    mixed = solve_rhf(ham, guess=guess, options=options, schedule=PrecisionSchedule(mode="mixed"))
+    assert plain.converged and mixed.converged
+    assert {"bf16", "incremental", "fp64"} <= {h.precision for h in mixed.history}
+    assert abs(mixed.energy - plain.energy) <= 1e-8
+    assert float((mixed.density - plain.density).abs().max()) <= 1e-6
