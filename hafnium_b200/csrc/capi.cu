@@ -738,7 +738,8 @@ static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, doub
     const size_t per_q = (sign ? 4 : 2) * 2 * (size_t)t.npad * t.opad;
     const size_t kp_doubles = (size_t)round_up(t.npad * t.npad, 32);
     size_t budget = std::min<size_t>((size_t)2 << 30, freeb / 3);
-    size_t want = ct_bytes + per_q * std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)ctx->naux));
+    size_t want = round_up((int64_t)ct_bytes, 256) + tc_partial_bytes(t.npad) +
+                  per_q * std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)ctx->naux));
     want = round_up((int64_t)want, 256) + sizeof(double) * kp_doubles;
     int st = ensure_scratch(ctx, &ctx->d_tcwork, &ctx->tcwork_bytes, want);
     if (st != HF_OK) return st;

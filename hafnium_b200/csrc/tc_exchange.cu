@@ -9,8 +9,10 @@
 //            A = BF16 copies of B stored in full (both triangles, K-major),
 //            B-operand = C^T; the epilogue splits X into BF16 hi/lo, p-major.
 //   stage 2  K[p][p'] += sum_(q,i) X[p][(q,i)] s_i X[p'][(q,i)], split over k,
-//            upper 128-row tiles only, FP64 atomics into K (s_i = +-1 for a
-//            signed factor, whose stage 1 also writes X diag(s)).
+//            upper 128-row tiles only; every (tile, split) writes its FP32 sum
+//            to its own slice of a partial buffer, which a second kernel adds
+//            into K in FP64 in a fixed order (s_i = +-1 for a signed factor,
+//            whose stage 1 also writes X diag(s)).
 //
 // A persistent CTA per SM walks 128 x BN output tiles: warp 4 drives TMA (no
 // multicast), warp 5 allocates TMEM and one thread issues tcgen05.mma
@@ -165,6 +167,9 @@ struct TcParams {
     // stage 2: K[p][p'] += acc (upper tiles only)
     double* kout;
     int64_t ldk;
+    // stage 2 with per-split partial sums: kpart[split][p][p'] (FP32, row stride ldk) instead
+    // of FP64 atomics into kout; summed into kout by k_reduce_partials
+    float* kpart;
     int* err;
 };
 
@@ -371,6 +376,14 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
                             sl[1] = reinterpret_cast<const uint4*>(lv)[1];
                         }
                     }
+                } else if (P.kpart) {
+                    // 16 columns of this row's partial sum: four 16-byte vectors (ldk is a
+                    // multiple of 128 and n0 + c of 16, so they are aligned)
+                    float4* d4 = reinterpret_cast<float4*>(P.kpart + ((int64_t)split * P.ldk + row) * P.ldk + n0 + c);
+                    d4[0] = make_float4(v[0], v[1], v[2], v[3]);
+                    d4[1] = make_float4(v[4], v[5], v[6], v[7]);
+                    d4[2] = make_float4(v[8], v[9], v[10], v[11]);
+                    d4[3] = make_float4(v[12], v[13], v[14], v[15]);
                 } else {
                     double* dst = P.kout + (int64_t)row * P.ldk + n0 + c;
 #pragma unroll
@@ -451,6 +464,19 @@ __global__ void k_split_ct(const double* __restrict__ ct, int64_t count, __nv_bf
     l[e] = __double2bfloat16(x - (double)__bfloat162float(hi));
 }
 
+// Kp[p][p'] += sum_s part[s][p][p'] over the elements of the stage-2 tiles that
+// touch the upper triangle ((p' / bn + 1) bn > (p / 128) 128), in a fixed order.
+__global__ void k_reduce_partials(const float* __restrict__ part, int splits, int64_t npad, int bn,
+                                  double* __restrict__ Kp) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= npad * npad) return;
+    const int64_t row = e / npad, col = e % npad;
+    if ((col / bn + 1) * bn <= (row / BM) * BM) return;
+    double sum = 0.0;
+    for (int k = 0; k < splits; ++k) sum += (double)part[(int64_t)k * npad * npad + e];
+    Kp[e] += sum;
+}
+
 __global__ void k_symmetrize_upper128(const double* __restrict__ Kp, int64_t ldk, int64_t n, double* __restrict__ K) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n * n) return;
@@ -527,6 +553,27 @@ TcPlan tc_plan(int64_t n, int naux, int64_t ncols) {
     return t;
 }
 
+namespace {
+// Stage 2's column tile width, its tiles touching the upper triangle, and the
+// largest k split it uses (two CTAs' worth of items per SM).
+void stage2_shape(int64_t npad, int& bn2, int& upper, int& splits_max) {
+    // the n tiles must cover npad exactly (an odd multiple of 128 takes 128-wide tiles)
+    bn2 = npad % 256 == 0 ? 256 : 128;
+    const int m_tiles = (int)(npad / BM), n_tiles = (int)(npad / bn2);
+    upper = 0;
+    for (int mt = 0; mt < m_tiles; ++mt)
+        for (int nt = 0; nt < n_tiles; ++nt)
+            if ((nt + 1) * bn2 > mt * BM) ++upper;
+    splits_max = std::max(1, (2 * 148 + upper - 1) / upper);
+}
+}  // namespace
+
+size_t tc_partial_bytes(int64_t npad) {
+    int bn2, upper, splits_max;
+    stage2_shape(npad, bn2, upper, splits_max);
+    return ((size_t)splits_max * npad * npad * sizeof(float) + 255) / 256 * 256;
+}
+
 size_t tc_b_bytes(int64_t n, int naux) {
     const int64_t npad = (n + 127) / 128 * 128;
     return sizeof(__nv_bfloat16) * 2 * (size_t)npad * npad * naux;
@@ -557,14 +604,17 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
     const int64_t npad = t.npad;
     const __nv_bfloat16* bh = static_cast<const __nv_bfloat16*>(bf16_b);
     const __nv_bfloat16* bl = bh + npad * npad * t.naux;
-    // work: Ct hi/lo [opad][npad] | X hi/lo [npad][qchunk*opad]
+    // work: Ct hi/lo [opad][npad] | stage-2 partial sums | X hi/lo [npad][qchunk*opad]
     __nv_bfloat16* cth = static_cast<__nv_bfloat16*>(work);
     __nv_bfloat16* ctl = cth + (int64_t)t.opad * npad;
-    __nv_bfloat16* xbase = ctl + (int64_t)t.opad * npad;
     const size_t ct_bytes = sizeof(__nv_bfloat16) * 2 * (size_t)t.opad * npad;
-    if (work_bytes <= ct_bytes) return cudaErrorInvalidValue;
+    const size_t part_bytes = tc_partial_bytes(npad);
+    const size_t head = (ct_bytes + 255) / 256 * 256 + part_bytes;
+    float* kpart = reinterpret_cast<float*>(static_cast<uint8_t*>(work) + (ct_bytes + 255) / 256 * 256);
+    __nv_bfloat16* xbase = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(work) + head);
+    if (work_bytes <= head) return cudaErrorInvalidValue;
     const size_t per_q = sizeof(__nv_bfloat16) * (sign ? 4 : 2) * (size_t)npad * t.opad;
-    int qchunk = (int)std::min<size_t>((work_bytes - ct_bytes) / per_q, (size_t)t.naux);
+    int qchunk = (int)std::min<size_t>((work_bytes - head) / per_q, (size_t)t.naux);
     if (qchunk < 1) return cudaErrorInvalidValue;
     const int64_t cnt = (int64_t)t.opad * npad;
     k_split_ct<<<(unsigned)((cnt + 255) / 256), 256, 0, stream>>>(Ct_fp64, cnt, cth, ctl);
@@ -608,8 +658,8 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         cudaError_t e = launch_tc(mAh, mAl, mCh, mCl, P, stream);
         if (e != cudaSuccess) return e;
         // stage 2: K += X X^T over this chunk, split over k
-        // the n tiles must cover npad exactly (an odd multiple of 128 takes 128-wide tiles)
-        const int bn2 = npad % 256 == 0 ? 256 : 128;
+        int bn2, upper, splits_max;
+        stage2_shape(npad, bn2, upper, splits_max);
         CUtensorMap mXh, mXl, mXh2, mXl2;
         // B operand: X diag(sign) when the factor is signed
         if (!make_map(&mXh, xh, npad, ldx, BM) || !make_map(&mXl, xl, npad, ldx, BM) ||
@@ -620,11 +670,7 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         Q.n_tiles = (int)(npad / bn2);
         Q.bn = bn2;
         Q.k_tiles_total = (int)((ldx + BK - 1) / BK);  // the ragged last tile reads zeros past ldx
-        int upper = 0;
-        for (int mt = 0; mt < Q.m_tiles; ++mt)
-            for (int ntile = 0; ntile < Q.n_tiles; ++ntile)
-                if ((ntile + 1) * bn2 > mt * BM) ++upper;
-        const int splits = std::max(1, std::min(Q.k_tiles_total, (2 * 148 + upper - 1) / upper));
+        const int splits = std::max(1, std::min(Q.k_tiles_total, splits_max));
         Q.k_tiles = (Q.k_tiles_total + splits - 1) / splits;
         Q.splits = (Q.k_tiles_total + Q.k_tiles - 1) / Q.k_tiles;  // every split has k tiles
         Q.items = upper * Q.splits;
@@ -632,9 +678,11 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         Q.stages = stages_for(bn2);
         Q.kout = Kp;
         Q.ldk = npad;
+        Q.kpart = kpart;
         Q.err = d_err;
         e = launch_tc(mXh, mXl, mXh2, mXl2, Q, stream);
         if (e != cudaSuccess) return e;
+        k_reduce_partials<<<(unsigned)((npad * npad + 255) / 256), 256, 0, stream>>>(kpart, Q.splits, npad, bn2, Kp);
     }
     k_symmetrize_upper128<<<(unsigned)((n * n + 255) / 256), 256, 0, stream>>>(Kp, npad, n, K);
     return cudaGetLastError();
