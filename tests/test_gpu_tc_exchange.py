@@ -69,3 +69,13 @@ def test_bf16_signed_factor_matches_fp64(two_body):
                 0.7 * np.max(np.abs(ctx.exchange_factored_host(c[:, k:], None, _lib.PREC_FP64))))
     assert np.max(np.abs(k16 - k64)) <= REL_TOL * scale
     np.testing.assert_allclose(k16, k16.T, atol=0, rtol=0)
+
+
+def test_bf16_exchange_is_reproducible(two_body):
+    """Stage 2 sums its k splits in a fixed order: two builds give the same bits."""
+    rng = np.random.default_rng(7)
+    c = rng.normal(size=(two_body.n_ao, 50)) / np.sqrt(two_body.n_ao * 50)
+    ctx = two_body.context
+    first = ctx.exchange_factored_host(c, None, _lib.PREC_BF16X3)
+    second = ctx.exchange_factored_host(c, None, _lib.PREC_BF16X3)
+    assert np.array_equal(first, second)
