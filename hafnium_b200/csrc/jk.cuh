@@ -49,7 +49,8 @@ inline cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int op
 }
 
 // Split-K factor of the K = X X^T product for `count` clusters of padded size
-// npad (enough CTAs for two per SM), and the partial-product scratch it needs.
+// npad (enough CTAs for about twelve per SM, at most 32 splits), and the
+// partial-product scratch it needs.
 int syrk_splits(int64_t npad, int count);
 int64_t syrk_partial_doubles(int64_t npad, int count);
 
