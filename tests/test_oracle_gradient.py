@@ -117,3 +117,23 @@ def test_planted_gradient_error_is_caught():
     _, _, orb, aux = _tables(mol, str(ref["basis"]))
     got = dfrhf.nuclear_gradient(orb, aux, mol.nuclear_charges, mol.positions, ref["density"], -ref["fock"])
     assert np.max(np.abs(got["overlap"] - ref["overlap"])) > 1e-3
+
+
+def test_derivative_integrals_are_translationally_invariant():
+    """Moving every centre together changes no integral: the bra, ket and
+    auxiliary (or nuclear) derivatives sum to zero. This is the identity the
+    device kernels use for the second orbital centre."""
+    mol = water()
+    o, a, _, _ = _tables(mol, "cc-pvdz")
+    s_x = kernels.overlap_derivative(o, o, Z3)[0]
+    t_x = kernels.kinetic_derivative(o, o, Z3)[0]
+    v_x, v_nuc = kernels.nuclear_attraction_derivative(o, o, Z3, mol.nuclear_charges, mol.positions)
+    m_x = kernels.coulomb_two_center_derivative(a, a, Z3)[0]
+    by_aux, by_orb = kernels.coulomb_three_center_derivative(a, o, o, np.zeros((1, 2, 3)))
+    for axis in range(3):
+        np.testing.assert_allclose(s_x[axis] + s_x[axis].T, 0.0, atol=1e-12)
+        np.testing.assert_allclose(t_x[axis] + t_x[axis].T, 0.0, atol=1e-11)
+        np.testing.assert_allclose(v_x[0][axis] + v_x[0][axis].T + v_nuc[0][:, axis].sum(axis=0), 0.0, atol=1e-10)
+        np.testing.assert_allclose(m_x[axis] + m_x[axis].T, 0.0, atol=1e-11)
+        total = by_aux[0][axis] + by_orb[0][axis] + np.transpose(by_orb[0][axis], (0, 2, 1))
+        np.testing.assert_allclose(total, 0.0, atol=1e-11)
