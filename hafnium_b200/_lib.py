@@ -24,7 +24,8 @@ EXPORTS = (
     "hf_ctx_create", "hf_ctx_destroy", "hf_last_error", "hf_set_stream", "hf_shells_upload",
     "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
     "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_four_center", "hf_get_stats",
-    "hf_coulomb_static", "hf_mp2_energy", "hf_nuclear_gradient", "hf_mo_fitted_tensor",
+    "hf_coulomb_static", "hf_mp2_energy", "hf_nuclear_gradient", "hf_mo_fitted_tensor", "hf_set_wait_limit",
+    "hf_boys",
 )
 
 BATCH_EXPORTS = (
@@ -79,6 +80,7 @@ class StatsC(ctypes.Structure):
         ("ms_gradient_metric", ctypes.c_double),
         ("ms_gradient_three_center", ctypes.c_double),
         ("ms_gradient_one_electron", ctypes.c_double),
+        ("device_allocations", ctypes.c_int64),
     ]
 
 
@@ -121,6 +123,8 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_one_electron.argtypes = [v, i, v, v, i64, v, i]
     lib.hf_four_center.argtypes = [v, v, i]
     lib.hf_coulomb_static.argtypes = [v, v, v]
+    lib.hf_set_wait_limit.argtypes = [v, i64, i]
+    lib.hf_boys.argtypes = [v, v, i64, i, v]
     lib.hf_mp2_energy.argtypes = [v, v, v, i64, i64, ctypes.POINTER(ctypes.c_double), i]
     lib.hf_nuclear_gradient.argtypes = [v, v, i64, v, v, v, i64, v, i]
     lib.hf_mo_fitted_tensor.argtypes = [v, v, i64, v, i64, v, i]
@@ -261,6 +265,30 @@ class Context:
     def coulomb_device(self, d, out) -> None:
         torch_sync(d)
         self.check(self.lib.hf_coulomb(self.handle, d.data_ptr(), out.data_ptr(), 1), "hf_coulomb")
+
+    def boys(self, t, n_max: int) -> np.ndarray:
+        """F_0..F_n_max at each argument in ``t`` from the device evaluation:
+        ``[len(t), n_max + 1]``."""
+        t = np.ascontiguousarray(np.atleast_1d(np.asarray(t, dtype=np.float64)))
+        out = np.empty((t.shape[0], n_max + 1))
+        self.check(self.lib.hf_boys(self.handle, t.ctypes.data, t.shape[0], int(n_max), out.ctypes.data), "hf_boys")
+        return out
+
+    def set_wait_limit(self, seconds: float, stall_next_build: bool = False) -> None:
+        """Limit of the split-BF16 exchange's device waits; ``stall_next_build``
+        makes the next split-BF16 build wait once on a barrier that nothing
+        completes (it then returns HF_ERR_TIMEOUT, raised as BackendError)."""
+        self.check(self.lib.hf_set_wait_limit(self.handle, int(round(seconds * 1e9)), int(stall_next_build)),
+                   "hf_set_wait_limit")
+
+    def coulomb_static_device(self, d, out) -> None:
+        """J into ``out`` through hf_coulomb_static, the build that allocates no
+        device memory (its scratch is a static device array). Torch's pending
+        work on ``d`` and ``out`` is waited for first: the library runs on its
+        own stream."""
+        torch_sync(d)
+        torch_sync(out)
+        self.check(self.lib.hf_coulomb_static(self.handle, d.data_ptr(), out.data_ptr()), "hf_coulomb_static")
 
     def exchange_device(self, d, out, precision: int = PREC_FP64) -> None:
         torch_sync(d)

@@ -154,8 +154,15 @@ class ShellTable:
         """Lay out a reference ``BasisSet`` on a reference ``Molecule``.
 
         Mirrors ``ShellTable.from_basis`` (hafnium/integrals/shell_table.py:84-116)
-        by duck typing, so the drop-in accepts the caller's own objects.
+        by duck typing, so the drop-in accepts the caller's own objects. A basis
+        laid out for other elements than the molecule's is refused, as the
+        reference's ``require_basis_for_atoms`` (shell_table.py:141-154) does.
         """
+        basis_symbols = tuple(getattr(basis, "atom_symbols", ()))
+        molecule_symbols = tuple(molecule.symbols)
+        if basis_symbols != molecule_symbols:
+            raise InputError(f"the basis belongs to atoms {list(basis_symbols)}, the molecule has "
+                             f"{list(molecule_symbols)}; lay the basis out for this molecule's atoms")
         positions = np.asarray(molecule.positions_array(), dtype=np.float64)
         ls, centers, offsets, exps, coefs, ks, atoms = [], [], [0], [], [], [], []
         for shell, atom in zip(basis.shells, basis.shell_atoms):

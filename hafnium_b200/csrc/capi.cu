@@ -66,6 +66,9 @@ struct hf_ctx {
     int* d_info = nullptr;
     double* d_scalar = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // bounded device waits of the split-BF16 exchange (hf_set_wait_limit)
+    uint64_t wait_ns = 2000000000ull;  // 2 s: far above any legitimate wait there
+    int stall_next = 0;                // the next split-BF16 build runs the stall self-test
 };
 
 namespace {
@@ -84,6 +87,7 @@ int fail(hf_ctx* c, int code, const std::string& msg) {
     } while (0)
 
 int alloc(hf_ctx* ctx, void** p, size_t bytes) {
+    ctx->stats.device_allocations++;
     cudaError_t e = cudaMalloc(p, bytes ? bytes : 8);
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -123,6 +127,7 @@ void keep_pool_memory(int device) {
 // the context's stream and, unlike cudaFree, do not synchronise the device, so
 // contexts on other streams (other clusters) keep running.
 int talloc(hf_ctx* ctx, void** p, size_t bytes) {
+    ctx->stats.device_allocations++;
     cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 8, ctx->stream);
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -350,6 +355,15 @@ const char* hf_last_error(const hf_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 int hf_set_stream(hf_ctx* ctx, void* stream) {
     if (!ctx) return HF_ERR_ARG;
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+    return HF_OK;
+}
+
+int hf_set_wait_limit(hf_ctx* ctx, int64_t wait_ns, int stall_next_build) {
+    if (!ctx) return HF_ERR_ARG;
+    if (wait_ns < 1000 || wait_ns > 60000000000ll)
+        return fail(ctx, HF_ERR_ARG, "the wait limit lies between 1 us and 60 s (got " + std::to_string(wait_ns) + " ns)");
+    ctx->wait_ns = (uint64_t)wait_ns;
+    ctx->stall_next = stall_next_build ? 1 : 0;
     return HF_OK;
 }
 
@@ -746,8 +760,10 @@ static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, doub
     double* Kp = ctx->d_tcwork;
     void* work = ctx->d_tcwork + kp_doubles;
     HF_CU(cudaMemsetAsync(ctx->d_info + 2, 0, sizeof(int), ctx->stream));
+    const TcWait wait{ctx->d_info + 2, ctx->wait_ns, ctx->stall_next};
+    ctx->stall_next = 0;
     cudaError_t e = exchange_build_bf16(t, ctx->d_bf16_b, Ct_tc, t.npad, dK, Kp, work, want - sizeof(double) * kp_doubles,
-                                        ctx->d_info + 2, ctx->stream, ctx->n, sign);
+                                        wait, ctx->stream, ctx->n, sign);
     ctx->stats.kernel_launches += 3 * ((ctx->naux + 1023) / 1024) + 3;
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("split-BF16 exchange: ") + cudaGetErrorString(e));
     int s = check_async(ctx, "split-BF16 exchange");
@@ -1414,6 +1430,28 @@ int hf_get_stats(const hf_ctx* ctx, hf_stats* out) {
     return HF_OK;
 }
 
+int hf_boys(hf_ctx* ctx, const double* t, int64_t count, int n_max, double* out) {
+    if (!ctx || count < 0 || (count > 0 && (!t || !out))) return HF_ERR_ARG;
+    if (n_max < 0 || n_max > kBoysMaxOrder)
+        return fail(ctx, HF_ERR_ARG, "the device Boys function covers orders 0.." + std::to_string(kBoysMaxOrder) +
+                                         " (got " + std::to_string(n_max) + ")");
+    for (int64_t i = 0; i < count; ++i)
+        if (!(t[i] >= 0.0) || !std::isfinite(t[i])) return fail(ctx, HF_ERR_ARG, "the Boys function argument is non-negative");
+    if (count == 0) return HF_OK;
+    cudaSetDevice(ctx->device);
+    const size_t in_bytes = sizeof(double) * (size_t)count, out_bytes = in_bytes * (size_t)(n_max + 1);
+    double* dt = nullptr;
+    if (talloc(ctx, (void**)&dt, in_bytes + out_bytes)) return HF_ERR_OOM;
+    double* dout = dt + count;
+    cudaError_t e = cudaMemcpyAsync(dt, t, in_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_boys_values(dt, count, n_max, ctx->d_btable, dout, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    trelease(ctx, dt);
+    ctx->stats.kernel_launches += 1;
+    if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("hf_boys: ") + cudaGetErrorString(e));
+    return check_async(ctx, "hf_boys");
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -1435,7 +1473,9 @@ int hf_get_stats(const hf_ctx* ctx, hf_stats* out) {
 // contexts at the same time) race on it and must be serialised by the caller.
 // The first call on a device resolves the array's device address
 // (cudaGetSymbolAddress, with that device current); make that first call before
-// any stream capture.
+// any stream capture. The address is kept for the life of the process: after a
+// reset of the device (cudaDeviceReset) it is stale, so no call may follow one.
+// The call returns once J is complete (it waits for the context's stream).
 namespace {
 constexpr int64_t kStaticMaxAo = 1536;
 constexpr int64_t kStaticMaxAux = 8192;

@@ -139,6 +139,44 @@ std::vector<double> boys_grid_host() {
     return g;
 }
 
+// F_0..F_L(T) of the device evaluation the integral kernels use, one argument
+// per thread, into out[i][0..L] (the values special.rs:34-51 fill_boys gives).
+template <int L>
+__global__ void k_boys_values(const double* __restrict__ t, int64_t count, const double* __restrict__ btable,
+                              double* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    double F[L + 1];
+    boys<L>(t[i], btable, F);
+#pragma unroll
+    for (int n = 0; n <= L; ++n) out[i * (L + 1) + n] = F[n];
+}
+
+template <int L>
+cudaError_t boys_values_l(const double* t, int64_t count, const double* btable, double* out, cudaStream_t stream) {
+    k_boys_values<L><<<(unsigned)((count + 127) / 128), 128, 0, stream>>>(t, count, btable, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_boys_values(const double* t, int64_t count, int n_max, const double* btable, double* out,
+                               cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    switch (n_max) {
+        case 0: return boys_values_l<0>(t, count, btable, out, stream);
+        case 1: return boys_values_l<1>(t, count, btable, out, stream);
+        case 2: return boys_values_l<2>(t, count, btable, out, stream);
+        case 3: return boys_values_l<3>(t, count, btable, out, stream);
+        case 4: return boys_values_l<4>(t, count, btable, out, stream);
+        case 5: return boys_values_l<5>(t, count, btable, out, stream);
+        case 6: return boys_values_l<6>(t, count, btable, out, stream);
+        case 7: return boys_values_l<7>(t, count, btable, out, stream);
+        case 8: return boys_values_l<8>(t, count, btable, out, stream);
+        case 9: return boys_values_l<9>(t, count, btable, out, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+static_assert(kBoysOrders - kBoysTerms == 9, "launch_boys_values covers orders 0..9");
+
 // ------------------------------------------------------------- (P|Q) metric
 template <int LP, int LQ>
 __global__ void __launch_bounds__(128) k_metric(const DevShell* __restrict__ aux, const double* __restrict__ exps,

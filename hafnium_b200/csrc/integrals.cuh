@@ -54,6 +54,12 @@ ConstantTables constant_tables_host();
 void upload_c2s(cudaStream_t stream);
 void upload_gradient_tables(cudaStream_t stream);
 std::vector<double> boys_grid_host();
+// The highest Boys order the device evaluation supports (the Taylor grid holds
+// kBoysTerms orders above it).
+constexpr int kBoysMaxOrder = kBoysOrders - kBoysTerms;
+// F_0..F_n_max at count arguments t (device arrays) into out[count][n_max + 1].
+cudaError_t launch_boys_values(const double* t, int64_t count, int n_max, const double* btable, double* out,
+                               cudaStream_t stream);
 
 // (P|Q) for all aux shells into M[N][N] (internal order, row-major, ld = ldm).
 cudaError_t launch_metric(const DevShell* aux, const double* exps, const double* coefs,

@@ -39,7 +39,6 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BK = 64;  // one 128-byte swizzle row of BF16
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: far above any legitimate wait here
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -78,19 +77,35 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Bounded wait: gives up after kWaitNs, or as soon as another CTA has recorded
-// an error, and records its own failure; returns whether the phase completed.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+// Bounded wait: gives up after wait_ns, or as soon as another thread has
+// recorded an error, and records its own failure; returns whether the phase
+// completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, uint64_t wait_ns) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t start = global_ns();
     for (uint32_t i = 1;; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((i & 255) == 0) {
             if (*(volatile int*)err != 0) return false;
-            if (global_ns() - start > kWaitNs) {
+            if (global_ns() - start > wait_ns) {
                 atomicExch(err, 1);
                 return false;
             }
+        }
+    }
+}
+
+// Wait for copies already issued to land before the CTA exits: bounded by
+// wait_ns only (an error recorded elsewhere does not cut it short, since the
+// copies still write this CTA's shared memory).
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity, int* err, uint64_t wait_ns) {
+    if (mbar_try_wait(bar, parity)) return;
+    const uint64_t start = global_ns();
+    for (uint32_t i = 1;; ++i) {
+        if (mbar_try_wait(bar, parity)) return;
+        if ((i & 255) == 0 && global_ns() - start > wait_ns) {
+            atomicExch(err, 1);
+            return;
         }
     }
 }
@@ -171,6 +186,8 @@ struct TcParams {
     // of FP64 atomics into kout; summed into kout by k_reduce_partials
     float* kpart;
     int* err;
+    uint64_t wait_ns;  // limit of every mbarrier wait
+    int stall;         // self-test: the MMA thread first waits on a barrier that nothing completes
 };
 
 // Work item -> (m tile, n tile, split). Stage 1: m-major, n inner (neighbouring
@@ -217,7 +234,8 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
     uint64_t* acc_full = empty + P.stages;   // [2]
     uint64_t* acc_empty = acc_full + 2;      // [2]
     uint64_t* mma_done = acc_empty + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+    uint64_t* never = mma_done + 1;          // no thread ever arrives here (the stall self-test)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(never + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -230,6 +248,7 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
             mbar_init(&acc_empty[b], 128);
         }
         mbar_init(mma_done, 1);
+        mbar_init(never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 4 && lane == 0) {
@@ -257,7 +276,7 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
                 for (int kt = kt0; kt < kt1; ++kt, ++it) {
                     const int s = it % P.stages;
                     const uint32_t ph = (it / P.stages) & 1;
-                    if (!mbar_wait(&empty[s], ph ^ 1, P.err)) {
+                    if (!mbar_wait(&empty[s], ph ^ 1, P.err, P.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -274,26 +293,27 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
             // Before the CTA can exit, every copy this thread issued has landed
             // (already true on the normal path, where the MMA thread consumed them).
             for (int j = max(0, issued - P.stages); j < issued; ++j)
-                mbar_wait(&full[j % P.stages], (j / P.stages) & 1, P.err);
+                mbar_drain(&full[j % P.stages], (j / P.stages) & 1, P.err, P.wait_ns);
         }
     } else if (warp == 5) {
         if (lane == 0) {
             const uint32_t idesc = idesc_bf16(P.bn);
             int it = 0, local = 0;
-            bool ok = true;
+            // the stall self-test: a wait that runs out, recorded like any other
+            bool ok = !(P.stall && !mbar_wait(never, 0, P.err, P.wait_ns));
             for (int w = blockIdx.x; ok && w < P.items; w += gridDim.x, ++local) {
                 int mt, nt, split;
                 decode_item(P, w, mt, nt, split);
                 const int kt0 = split * P.k_tiles, kt1 = min(P.k_tiles_total, kt0 + P.k_tiles);
                 const int buf = local & 1;
                 // the epilogue has drained this buffer's previous item
-                if (!mbar_wait(&acc_empty[buf], ((local >> 1) & 1) ^ 1, P.err)) break;
+                if (!mbar_wait(&acc_empty[buf], ((local >> 1) & 1) ^ 1, P.err, P.wait_ns)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const uint32_t acc_tmem = tmem + (uint32_t)(buf * 256);
                 for (int kt = kt0; kt < kt1; ++kt, ++it) {
                     const int s = it % P.stages;
                     const uint32_t ph = (it / P.stages) & 1;
-                    if (!mbar_wait(&full[s], ph, P.err)) {
+                    if (!mbar_wait(&full[s], ph, P.err, P.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -325,7 +345,7 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
             int mt, nt, split;
             decode_item(P, w, mt, nt, split);
             const int buf = local & 1;
-            bool ready = mbar_wait(&acc_full[buf], (local >> 1) & 1, P.err) && *(volatile int*)P.err == 0;
+            bool ready = mbar_wait(&acc_full[buf], (local >> 1) & 1, P.err, P.wait_ns) && *(volatile int*)P.err == 0;
             // tcgen05.ld is warp-collective: the whole warp reads or none of it does
             ready = __all_sync(0xffffffffu, ready);
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -395,7 +415,7 @@ __global__ void __launch_bounds__(192, 1) k_tc_split3(const __grid_constant__ CU
             mbar_arrive(&acc_empty[buf]);
         }
     }
-    if (warp == 5 && lane == 0) mbar_wait(mma_done, 0, P.err);
+    if (warp == 5 && lane == 0) mbar_drain(mma_done, 0, P.err, P.wait_ns);
     __syncthreads();
     if (warp == 5) {
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -598,7 +618,7 @@ cudaError_t tc_split_b(const JkPlan& p, int64_t npad, void* bf16_b, cudaStream_t
 }
 
 cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const double* Ct_fp64, int64_t ct_ld,
-                                double* K, double* Kp, void* work, size_t work_bytes, int* d_err,
+                                double* K, double* Kp, void* work, size_t work_bytes, const TcWait& wait,
                                 cudaStream_t stream, int64_t n, const double* sign) {
     (void)ct_ld;
     const int64_t npad = t.npad;
@@ -654,7 +674,9 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         P.npad = (int)npad;
         P.opad = t.opad;
         P.ocols = t.opad;
-        P.err = d_err;
+        P.err = wait.err;
+        P.wait_ns = wait.wait_ns;
+        P.stall = q0 == 0 ? wait.stall : 0;
         cudaError_t e = launch_tc(mAh, mAl, mCh, mCl, P, stream);
         if (e != cudaSuccess) return e;
         // stage 2: K += X X^T over this chunk, split over k
@@ -679,7 +701,9 @@ cudaError_t exchange_build_bf16(const TcPlan& t, const void* bf16_b, const doubl
         Q.kout = Kp;
         Q.ldk = npad;
         Q.kpart = kpart;
-        Q.err = d_err;
+        Q.err = wait.err;
+        Q.wait_ns = wait.wait_ns;
+        Q.stall = 0;
         e = launch_tc(mXh, mXl, mXh2, mXl2, Q, stream);
         if (e != cudaSuccess) return e;
         k_reduce_partials<<<(unsigned)((npad * npad + 255) / 256), 256, 0, stream>>>(kpart, Q.splits, npad, bn2, Kp);

@@ -69,6 +69,7 @@ typedef struct hf_stats {
     double ms_gradient_metric;  /* last gradient: (dP P|Q) against the metric weights */
     double ms_gradient_three_center; /* last gradient: exchange weights and (dP P|uv), (P|dA uv) */
     double ms_gradient_one_electron; /* last gradient: S, T, V derivatives */
+    int64_t device_allocations; /* cudaMalloc / cudaMallocAsync calls made for this context so far */
 } hf_stats;
 
 /* Context lifetime (no reference counterpart: the reference's kernels are
@@ -78,6 +79,15 @@ int hf_ctx_destroy(hf_ctx* ctx);
 const char* hf_last_error(const hf_ctx* ctx);
 /* Launch on this stream (cudaStream_t) from now on; NULL = the context's own. */
 int hf_set_stream(hf_ctx* ctx, void* stream);
+
+/* Limit of every device-side wait of the split-BF16 exchange's pipeline (its
+ * mbarrier waits), in nanoseconds, 1 us .. 60 s; 2 s by default. A wait that
+ * runs out ends the kernel cleanly (in-flight copies drained, tensor memory
+ * freed) and the build returns HF_ERR_TIMEOUT; the context stays usable. With
+ * stall_next_build set, the next split-BF16 build waits once on a barrier that
+ * nothing completes, so that path can be tested without a fault. No reference
+ * counterpart (the reference has no device code). */
+int hf_set_wait_limit(hf_ctx* ctx, int64_t wait_ns, int stall_next_build);
 
 /* Upload the orbital and auxiliary shells (replaces the _kernels.ShellTable
  * marshalling of native.py:16-24; validation of integrals/mod.rs:111-173).
@@ -102,7 +112,10 @@ int hf_coulomb(hf_ctx* ctx, const double* density, double* coulomb, int on_devic
  * loading this library holds until exit, so n_ao <= 1536 and n_aux <= 8192
  * (HF_ERR_ARG beyond). Calls share that array: calls that overlap on the GPU
  * race. The first call on a device resolves the array's address; make it
- * before any stream capture. */
+ * before any stream capture. That address is kept for the life of the
+ * process, so no call may follow a reset of the device (cudaDeviceReset) in
+ * the same process. The call returns once J is complete: it waits for the
+ * context's stream. */
 int hf_coulomb_static(hf_ctx* ctx, const double* density, double* coulomb);
 
 /* K[u][v] = sum_wx (uw|xv) D[w][x] (coulomb_exchange.py:184-190) for a symmetric
@@ -168,6 +181,15 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
                         const double* positions, int64_t natoms, double* terms, int on_device);
 
 int hf_get_stats(const hf_ctx* ctx, hf_stats* out);
+
+/* F_n(t), n = 0..n_max, for count arguments t (host arrays; out is
+ * [count][n_max + 1]) by the device evaluation the integral kernels use: an
+ * 8-term Taylor expansion on a 0.05 grid below t = 36, then downward
+ * recursion; the large-t form and upward recursion above. Replaces the PyO3
+ * boys_function (crates/hafnium-py/src/lib.rs:39-46, special.rs:34-51) for
+ * testing the device path; n_max <= 9 (the integrals' highest order plus one
+ * for their derivatives); a negative or non-finite t is HF_ERR_ARG. */
+int hf_boys(hf_ctx* ctx, const double* t, int64_t count, int n_max, double* out);
 
 #ifdef __cplusplus
 }

@@ -16,11 +16,20 @@ import pathlib
 import sys
 
 HERE = pathlib.Path(__file__).resolve().parent
-DEFAULT_REFERENCE = pathlib.Path(os.environ.get("HF_REFERENCE_ROOT", "/root/reference"))
 
 
-def install(reference: pathlib.Path = DEFAULT_REFERENCE) -> None:
+def default_reference() -> pathlib.Path | None:
+    """The reference tree named by HF_REFERENCE_ROOT, or None when it is unset."""
+    root = os.environ.get("HF_REFERENCE_ROOT")
+    return pathlib.Path(root) if root else None
+
+
+def install(reference: pathlib.Path | None = None) -> None:
     """Put the shims and the reference tree on ``sys.path`` and register the kernels."""
+    reference = reference or default_reference()
+    if reference is None:
+        raise FileNotFoundError("no reference tree given (pass it, or set HF_REFERENCE_ROOT)")
+    reference = pathlib.Path(reference)
     if not reference.exists():
         raise FileNotFoundError(f"reference tree not found at {reference}")
     shims = str(HERE / "shims")

@@ -3,10 +3,11 @@
 The reference bundles Basis Set Exchange JSON files (BSD-3-Clause, MolSSI/EMSL;
 hafnium/basis/data/README.md) for H-Ar. This script keeps the elements the
 water-cluster workloads and the small test molecules use, verbatim per
-element, and writes one JSON file per basis set beside itself. Run it once
-where the reference tree is mounted:
+element, and writes one JSON file per basis set into hafnium_b200/basis_data/.
+Run it once where the reference tree is mounted (the path as the argument, or
+in HF_REFERENCE_ROOT):
 
-    python hafnium_b200/basis_data/extract_basis.py /path/to/reference
+    python tests/golden/extract_basis.py /path/to/reference
 """
 
 from __future__ import annotations
@@ -20,7 +21,7 @@ ELEMENTS = ("1", "2", "6", "7", "8")
 
 
 def main(reference: str) -> None:
-    here = pathlib.Path(__file__).resolve().parent
+    here = pathlib.Path(__file__).resolve().parent.parent.parent / "hafnium_b200" / "basis_data"
     for name in BASES:
         source = pathlib.Path(reference) / "hafnium" / "basis" / "data" / f"{name}.json"
         data = json.loads(source.read_text(encoding="utf-8"))
@@ -37,4 +38,9 @@ def main(reference: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HF_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("give the reference tree as the argument or in HF_REFERENCE_ROOT")
+    main(root)

@@ -19,6 +19,15 @@ Two kinds of fixture are written:
   checks the oracle's NumPy restatement (oracle/dfrhf.py) against each run.
 * ``reference_gradient_*.npz``: the reference's own DF-RHF nuclear gradient at
   its converged state, with the state itself (see ``reference_gradients``).
+* ``reference_dfrhf_h2o12_s3.npz``, ``reference_dfrhf_h2o16_s0.npz``: the
+  reference's own DF-RHF as above on larger clusters (n = 288, 384), stored as
+  an occupied factor F of the density (D = F F^T) to keep the files small; the
+  oracle's memory-lean restatement (``LeanFittedJK``) is checked against each.
+* ``oracle_dfrhf_h2o32_s0.npz``: (H2O)32 (n = 768), beyond what the reference's
+  full-layout exchange runs in this container's memory in reasonable time, from
+  the lean restatement that the two runs above pin (see ``large_runs``).
+
+The reference tree is given as the first argument or by HF_REFERENCE_ROOT.
 """
 
 from __future__ import annotations
@@ -111,6 +120,91 @@ def reference_runs(reference: pathlib.Path) -> None:
         )
 
 
+LARGE_REFERENCE = [(12, 3), (16, 0)]  # n = 288 (pads to 384, an odd multiple of 128) and 384
+LARGE_ORACLE = [(32, 0)]  # n = 768: the split-precision workload's size
+
+
+def _save_large(path: pathlib.Path, n, seed, mol, energy, density, history, n_iterations, source: str) -> None:
+    from oracle import dfrhf
+
+    factor = dfrhf.psd_factor(density)
+    assert factor.shape[1] == mol.n_alpha, factor.shape
+    assert float(np.max(np.abs(factor @ factor.T - density))) < 1e-13
+    np.savez_compressed(
+        path,
+        n_waters=np.asarray(n),
+        seed=np.asarray(seed),
+        positions_bohr=mol.positions,
+        energy=np.asarray(energy),
+        density_factor=factor,
+        history=np.asarray(history),
+        n_iterations=np.asarray(n_iterations),
+        source=np.asarray(source),
+    )
+
+
+def large_runs(reference: pathlib.Path) -> None:
+    """The reference's own ``hartree_fock`` on (H2O)12 and (H2O)16, and the oracle's
+    lean restatement (in-place fit, exchange through an occupied factor) checked
+    against both to |dE| < 1e-10, max|dD| < 1e-7 and the same iteration count; then
+    the lean restatement alone on (H2O)32."""
+    import time
+
+    from oracle import reference_env
+
+    reference_env.install(reference)
+    from hafnium.basis import BasisLibrary, BasisSet
+    from hafnium.integrals import RustEngine
+    from hafnium.molecule import Molecule as RefMolecule
+    from hafnium.scf import hartree_fock
+
+    from hafnium_b200.basis import ShellTable
+    from oracle import dfrhf
+
+    library = BasisLibrary(offline=True)
+    engine = RustEngine()
+
+    def lean(mol):
+        orb = ShellTable.build("cc-pvdz", mol.symbols, mol.positions)
+        auxt = ShellTable.build("def2-universal-jkfit", mol.symbols, mol.positions)
+        prob = dfrhf.build_problem_lean(orb, auxt, mol.nuclear_charges, mol.positions,
+                                        mol.nuclear_repulsion_energy(), mol.n_alpha)
+        guess = dfrhf.atomic_density_guess(orb, mol.symbols, {"O": 8.0, "H": 1.0})
+        return dfrhf.solve_rhf(prob.s, prob.h, dfrhf.LeanFittedJK(prob.b), prob.e_nuc, prob.n_alpha,
+                               guess=guess), prob.dropped
+
+    for n, seed in LARGE_REFERENCE:
+        mol = molecule_for(n, seed)
+        t0 = time.perf_counter()
+        ref_mol = RefMolecule.from_atoms(list(zip(mol.symbols, map(tuple, mol.positions))), unit="bohr")
+        basis = BasisSet.for_atoms(ref_mol, "cc-pvdz", library=library)
+        aux = BasisSet.for_atoms(ref_mol, "def2-universal-jkfit", library=library)
+        result = hartree_fock(engine, basis, ref_mol, auxiliary=aux)
+        t1 = time.perf_counter()
+        d_ref = np.asarray(result.density.blocks[0])
+        hist = [row.energy for row in result.history]
+        ours, dropped = lean(mol)
+        t2 = time.perf_counter()
+        de = abs(ours.energy - result.energy)
+        dd = float(np.max(np.abs(ours.density - d_ref)))
+        print(f"(H2O){n} seed {seed}: reference E = {result.energy:.12f} in {result.n_iterations} iterations "
+              f"({t1 - t0:.0f} s); lean oracle |dE| = {de:.2e}, max|dD| = {dd:.2e}, iterations "
+              f"{ours.n_iterations} ({t2 - t1:.0f} s); metric eigenvalues dropped: {dropped}", flush=True)
+        assert de < 1e-10 and dd < 1e-7 and ours.n_iterations == result.n_iterations
+        _save_large(HERE / f"reference_dfrhf_h2o{n}_s{seed}.npz", n, seed, mol, result.energy, d_ref, hist,
+                    result.n_iterations, "reference hartree_fock (hafnium/scf/hartree_fock.py:24)")
+    for n, seed in LARGE_ORACLE:
+        mol = molecule_for(n, seed)
+        t0 = time.perf_counter()
+        ours, dropped = lean(mol)
+        print(f"(H2O){n} seed {seed}: lean oracle E = {ours.energy:.12f} in {ours.n_iterations} iterations "
+              f"({time.perf_counter() - t0:.0f} s); metric eigenvalues dropped: {dropped}", flush=True)
+        assert ours.converged
+        _save_large(HERE / f"oracle_dfrhf_h2o{n}_s{seed}.npz", n, seed, mol, ours.energy, ours.density,
+                    [row.energy for row in ours.history], ours.n_iterations,
+                    "oracle restatement (oracle/dfrhf.py LeanFittedJK), pinned by the (H2O)12/16 reference runs")
+
+
 GRADIENT_CASES = [("water_pyscf", "def2-svp"), ("water", "cc-pvdz"), ("h2o2_s0", "cc-pvdz"), ("h2o4_s1", "cc-pvdz")]
 
 
@@ -179,8 +273,21 @@ def reference_gradients(reference: pathlib.Path) -> None:
         )
 
 
+def reference_root() -> pathlib.Path:
+    import os
+
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = args[0] if args else os.environ.get("HF_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("give the reference tree as the first argument or in HF_REFERENCE_ROOT")
+    return pathlib.Path(root)
+
+
 if __name__ == "__main__":
-    ref = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
-    stored_pyscf(ref)
-    reference_runs(ref)
-    reference_gradients(ref)
+    ref = reference_root()
+    if "--large" in sys.argv:
+        large_runs(ref)
+    else:
+        stored_pyscf(ref)
+        reference_runs(ref)
+        reference_gradients(ref)

@@ -1,7 +1,10 @@
 """Whole DF-RHF on the device against the reference's recorded runs (B200).
 
 |dE| <= 1e-8 Eh and max|dD| <= 1e-6 against the reference's own DF-RHF
-(tests/golden/reference_dfrhf_*.npz, made by tests/golden/make_golden.py).
+(tests/golden/reference_dfrhf_*.npz, made by tests/golden/make_golden.py) up to
+(H2O)16 (n = 384; (H2O)12 has n = 288, which the split-BF16 builds pad to an odd
+multiple of 128), and against the oracle's lean restatement at (H2O)32 (n = 768,
+oracle_dfrhf_h2o32_s0.npz), which the reference runs at 12 and 16 waters pin.
 """
 
 from __future__ import annotations
@@ -10,15 +13,14 @@ import numpy as np
 import pytest
 
 from hafnium_b200.scf import DeviceHamiltonian, ScfOptions, solve_rhf
-from tests.conftest import golden
-from tests.helpers import molecule
+from tests.helpers import golden_run, molecule
 
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("tag", ["water", "h2o2_s0", "h2o4_s1", "h2o8_s2"])
+@pytest.mark.parametrize("tag", ["water", "h2o2_s0", "h2o4_s1", "h2o8_s2", "h2o12_s3", "h2o16_s0", "h2o32_s0"])
 def test_device_dfrhf_matches_reference(tag):
-    ref = golden(f"reference_dfrhf_{tag}.npz")
+    ref = golden_run(tag)
     mol = molecule(tag)
     ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
     result = solve_rhf(ham, options=ScfOptions(energy_tolerance=1e-11, gradient_tolerance=1e-8))
@@ -40,12 +42,12 @@ def test_sad_guess_matches_oracle():
     np.testing.assert_allclose(got, expected, atol=1e-8, rtol=0)
 
 
-@pytest.mark.parametrize("tag", ["h2o4_s1", "h2o8_s2"])
+@pytest.mark.parametrize("tag", ["h2o4_s1", "h2o8_s2", "h2o12_s3", "h2o16_s0", "h2o32_s0"])
 def test_sad_started_scf_follows_the_reference_iterations(tag):
     """With the reference's SAD guess the device SCF takes the reference's iterations."""
     from hafnium_b200.scf import atomic_density_guess
 
-    ref = golden(f"reference_dfrhf_{tag}.npz")
+    ref = golden_run(tag)
     mol = molecule(tag)
     ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
     result = solve_rhf(ham, guess=atomic_density_guess(mol, "cc-pvdz"))
@@ -54,13 +56,13 @@ def test_sad_started_scf_follows_the_reference_iterations(tag):
     assert abs(result.energy - float(ref["energy"])) <= 1e-8
 
 
-@pytest.mark.parametrize("tag", ["h2o4_s1", "h2o8_s2"])
+@pytest.mark.parametrize("tag", ["h2o4_s1", "h2o8_s2", "h2o12_s3", "h2o16_s0", "h2o32_s0"])
 def test_mixed_schedule_matches_reference(tag):
     """Split-BF16 builds, an FP64 anchor, incremental builds on the signed difference
     density, then FP64: the reference's converged FP64 energy and density."""
     from hafnium_b200.scf import PrecisionSchedule, atomic_density_guess
 
-    ref = golden(f"reference_dfrhf_{tag}.npz")
+    ref = golden_run(tag)
     mol = molecule(tag)
     ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
     result = solve_rhf(ham, guess=atomic_density_guess(mol, "cc-pvdz"),

@@ -79,3 +79,30 @@ def test_bf16_exchange_is_reproducible(two_body):
     first = ctx.exchange_factored_host(c, None, _lib.PREC_BF16X3)
     second = ctx.exchange_factored_host(c, None, _lib.PREC_BF16X3)
     assert np.array_equal(first, second)
+
+
+def test_a_device_wait_that_runs_out_is_reported_and_the_context_recovers():
+    """The pipeline's bounded waits: the stall self-test makes the MMA thread wait
+    on a barrier that nothing completes; with a 1 ms limit the wait runs out, the
+    kernel ends (copies drained, tensor memory freed) and the build reports
+    HF_ERR_TIMEOUT as BackendError. The next build on the same context, at the
+    default limit, is correct again."""
+    from hafnium_b200.errors import BackendError, InputError
+
+    mol = molecule("h2o4_s1")
+    orb, aux = tables(mol)
+    two_body = B200DensityFittedCoulombExchange.from_tables(orb, aux)
+    ctx = two_body.context
+    rng = np.random.default_rng(5)
+    c = rng.normal(size=(two_body.n_ao, 20)) / np.sqrt(two_body.n_ao)
+    k64 = ctx.exchange_factored_host(c, None, _lib.PREC_FP64)
+    ctx.exchange_factored_host(c, None, _lib.PREC_BF16X3)  # the BF16 copy of B exists before the stall
+    ctx.set_wait_limit(1e-3, stall_next_build=True)
+    with pytest.raises(BackendError, match="wait ran out"):
+        ctx.exchange_factored_host(c, None, _lib.PREC_BF16X3)
+    ctx.set_wait_limit(2.0)
+    for _ in range(2):
+        k16 = ctx.exchange_factored_host(c, None, _lib.PREC_BF16X3)
+        assert np.max(np.abs(k16 - k64)) <= REL_TOL * np.max(np.abs(k64))
+    with pytest.raises(InputError, match="wait limit"):
+        ctx.set_wait_limit(1e-9)

@@ -80,6 +80,31 @@ def test_reference_dfrhf_runs(tag):
     np.testing.assert_allclose([h.energy for h in result.history], ref["history"], atol=1e-9)
 
 
+def test_lean_oracle_reproduces_the_reference_run_at_twelve_waters():
+    """The memory-lean restatement (in-place fit, exchange through an occupied
+    factor), which makes the (H2O)32 fixture, against the reference's own run on
+    (H2O)12 (n = 288): the same energy, density and iteration count."""
+    from tests.helpers import golden_run
+
+    ref = golden_run("h2o12_s3")
+    mol = molecule("h2o12_s3")
+    np.testing.assert_allclose(mol.positions, ref["positions_bohr"], atol=1e-14)
+    orb, aux = tables(mol)
+    prob = dfrhf.build_problem_lean(orb, aux, mol.nuclear_charges, mol.positions, mol.nuclear_repulsion_energy(),
+                                    mol.n_alpha)
+    guess = dfrhf.atomic_density_guess(orb, mol.symbols, {"O": 8.0, "H": 1.0})
+    result = dfrhf.solve_rhf(prob.s, prob.h, dfrhf.LeanFittedJK(prob.b), prob.e_nuc, prob.n_alpha, guess=guess)
+    assert result.energy == pytest.approx(float(ref["energy"]), abs=ENERGY_TOL)
+    assert result.n_iterations == int(ref["n_iterations"])
+    np.testing.assert_allclose(result.density, ref["density"], atol=1e-9)
+
+
+def test_lean_exchange_refuses_an_indefinite_density():
+    b = np.random.default_rng(0).normal(size=(3, 4, 4))
+    with pytest.raises(ValueError, match="positive semidefinite"):
+        dfrhf.LeanFittedJK(b).exchange(np.diag([1.0, -1.0, 0.5, 0.0]))
+
+
 def test_planted_error_is_caught(pyscf_water):
     """A metric with one element perturbed by 1e-10 fails the 1e-12 check."""
     mol = water_sto3g_pyscf_geometry(pyscf_water["df_positions_bohr"])

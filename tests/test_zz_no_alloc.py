@@ -26,16 +26,25 @@ def test_static_coulomb_matches_the_allocating_entry_point_twice():
 
     mol = molecule("h2o4_s1")
     orb, aux = tables(mol)
-    two_body = B200DensityFittedCoulombExchange.from_tables(orb, aux)
-    ctx = two_body.context
     rng = np.random.default_rng(11)
-    c = rng.normal(size=(two_body.n_ao, 20)) / np.sqrt(two_body.n_ao)
+    # a fresh context whose first J build is the static one: that build must not allocate
+    fresh = B200DensityFittedCoulombExchange.from_tables(orb, aux)
+    n = fresh.n_ao
+    c = rng.normal(size=(n, 20)) / np.sqrt(n)
     d = torch.as_tensor(c @ c.T, device="cuda")
+    got = torch.full_like(d, float("nan"))
+    before = fresh.context.stats()["device_allocations"]
+    fresh.context.coulomb_static_device(d, got)
+    assert fresh.context.stats()["device_allocations"] == before
+    first = got.clone()
+    # the allocating entry point on another context gives the expected J
+    two_body = B200DensityFittedCoulombExchange.from_tables(orb, aux)
     expected = torch.empty_like(d)
-    ctx.coulomb_device(d, expected)
+    two_body.context.coulomb_device(d, expected)
+    np.testing.assert_allclose(first.cpu().numpy(), expected.cpu().numpy(), atol=JK_TOL, rtol=0)
     for _ in range(2):  # two calls in a row share (and must re-clear) the static scratch
         got = torch.full_like(d, float("nan"))
-        ctx.check(ctx.lib.hf_coulomb_static(ctx.handle, d.data_ptr(), got.data_ptr()), "hf_coulomb_static")
+        two_body.context.coulomb_static_device(d, got)
         torch.cuda.synchronize()
         np.testing.assert_allclose(got.cpu().numpy(), expected.cpu().numpy(), atol=JK_TOL, rtol=0)
 
@@ -51,4 +60,4 @@ def test_static_coulomb_rejects_systems_beyond_its_limit():
     ctx.upload(orb, aux)  # no fitted tensor needed: the size check comes first
     d = torch.zeros((4, 4), dtype=torch.float64, device="cuda")
     with pytest.raises(InputError, match="n_ao <= 1536"):
-        ctx.check(ctx.lib.hf_coulomb_static(ctx.handle, d.data_ptr(), d.data_ptr()), "hf_coulomb_static")
+        ctx.coulomb_static_device(d, d)
