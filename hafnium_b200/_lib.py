@@ -25,7 +25,7 @@ EXPORTS = (
     "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
     "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_four_center", "hf_get_stats",
     "hf_coulomb_static", "hf_mp2_energy", "hf_nuclear_gradient", "hf_mo_fitted_tensor", "hf_set_wait_limit",
-    "hf_boys",
+    "hf_boys", "hf_release_retained", "hf_density_factor",
 )
 
 BATCH_EXPORTS = (
@@ -125,6 +125,8 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_coulomb_static.argtypes = [v, v, v]
     lib.hf_set_wait_limit.argtypes = [v, i64, i]
     lib.hf_boys.argtypes = [v, v, i64, i, v]
+    lib.hf_release_retained.argtypes = [i]
+    lib.hf_density_factor.argtypes = [v, v, v, i64, p(i64), i]
     lib.hf_mp2_energy.argtypes = [v, v, v, i64, i64, ctypes.POINTER(ctypes.c_double), i]
     lib.hf_nuclear_gradient.argtypes = [v, v, i64, v, v, v, i64, v, i]
     lib.hf_mo_fitted_tensor.argtypes = [v, v, i64, v, i64, v, i]
@@ -172,6 +174,14 @@ def torch_sync(tensor) -> None:
     import torch
 
     torch.cuda.current_stream(tensor.device).synchronize()
+
+
+def release_retained(device: int = 0) -> None:
+    """Free the fitted-tensor blocks the library keeps on ``device`` for the next
+    context of the same size (see hf_release_retained in include/hfjk.h)."""
+    status = load().hf_release_retained(int(device))
+    if status != HF_OK:
+        raise InputError(f"hf_release_retained({device}) failed with status {status}")
 
 
 class Context:
@@ -289,6 +299,29 @@ class Context:
         torch_sync(d)
         torch_sync(out)
         self.check(self.lib.hf_coulomb_static(self.handle, d.data_ptr(), out.data_ptr()), "hf_coulomb_static")
+
+    def overlap_device(self):
+        """The orbital overlap matrix S as a torch CUDA tensor (hf_one_electron)."""
+        import torch
+
+        n, _ = self.dims()
+        s = torch.empty((n, n), dtype=torch.float64, device=torch.device("cuda", self.device))
+        torch_sync(s)
+        self.check(self.lib.hf_one_electron(self.handle, 0, None, None, 0, s.data_ptr(), 1), "hf_one_electron")
+        return s
+
+    def density_factor_device(self, d, max_rank: int):
+        """``F`` ([n_ao, rank], a torch CUDA tensor) with ``F F^T = D`` for a
+        positive semidefinite device density, by the library's pivoted Cholesky."""
+        import torch
+
+        torch_sync(d)
+        n = d.shape[0]
+        rows = torch.empty((max(1, min(int(max_rank), n)), n), dtype=torch.float64, device=d.device)
+        rank = ctypes.c_int64()
+        self.check(self.lib.hf_density_factor(self.handle, d.data_ptr(), rows.data_ptr(), rows.shape[0],
+                                              ctypes.byref(rank), 1), "hf_density_factor")
+        return rows[: rank.value].T.contiguous()
 
     def exchange_device(self, d, out, precision: int = PREC_FP64) -> None:
         torch_sync(d)

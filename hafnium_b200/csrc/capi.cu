@@ -58,7 +58,9 @@ struct hf_ctx {
     size_t kscratch_bytes = 0;
     double* d_stage = nullptr;  // exchange staging: C, w, Ct, sign, D, Lc, K
     size_t stage_bytes = 0;
+    size_t b_alloc_bytes = 0;  // size of the block holding d_B (retained blocks may be larger)
     void* d_bf16_b = nullptr;  // full BF16 hi/lo copies of B (split-BF16 exchange)
+    size_t bf16_alloc_bytes = 0;
     double* d_tcwork = nullptr;  // split-BF16 exchange: factor and X chunk
     size_t tcwork_bytes = 0;
     double* d_ctc = nullptr;  // split-BF16 exchange: the padded FP64 factor
@@ -102,6 +104,92 @@ template <class T>
 void release(T*& p) {
     if (p) cudaFree((void*)p);
     p = nullptr;
+}
+
+// Retained device blocks for the fitted tensor and its BF16 copy (tens of GB at
+// the largest clusters). A context that is destroyed, or that rebuilds for
+// another molecule, hands these blocks to a per-device cache instead of
+// freeing them, and the next context on that device whose tensor fits takes
+// one back: a run over many geometries of one size (a scan, a benchmark)
+// then maps its two large tensors once instead of once per geometry, and a
+// cudaFree of tens of GB, which synchronises the device, is avoided. At most
+// kRetainBlocks blocks are kept per device; a failed allocation empties the
+// cache and retries; hf_release_retained frees it on request.
+constexpr size_t kRetainMinBytes = (size_t)1 << 30;
+constexpr int kRetainBlocks = 2;
+constexpr int kRetainDevices = 64;
+struct Retained {
+    void* p;
+    size_t bytes;
+};
+std::mutex g_retain_mutex;
+std::vector<Retained> g_retained[kRetainDevices];
+
+void free_retained(int device) {
+    std::vector<Retained> blocks;
+    {
+        std::lock_guard<std::mutex> lock(g_retain_mutex);
+        if (device < 0 || device >= kRetainDevices) return;
+        blocks.swap(g_retained[device]);
+    }
+    for (const Retained& r : blocks) cudaFree(r.p);
+}
+
+// A block of at least `bytes` for a fitted tensor: a retained one that wastes
+// at most an eighth of its size, else a new allocation (after emptying the cache
+// if the first attempt fails). *have is the block's size.
+int big_alloc(hf_ctx* ctx, void** p, size_t bytes, size_t* have) {
+    *p = nullptr;
+    *have = 0;
+    if (bytes >= kRetainMinBytes && ctx->device >= 0 && ctx->device < kRetainDevices) {
+        std::lock_guard<std::mutex> lock(g_retain_mutex);
+        auto& pool = g_retained[ctx->device];
+        int best = -1;
+        for (int i = 0; i < (int)pool.size(); ++i)
+            if (pool[i].bytes >= bytes && pool[i].bytes - bytes <= pool[i].bytes / 8 &&
+                (best < 0 || pool[i].bytes < pool[best].bytes))
+                best = i;
+        if (best >= 0) {
+            *p = pool[best].p;
+            *have = pool[best].bytes;
+            pool.erase(pool.begin() + best);
+            return HF_OK;
+        }
+    }
+    if (alloc(ctx, p, bytes) != HF_OK) {
+        free_retained(ctx->device);
+        if (alloc(ctx, p, bytes) != HF_OK) return HF_ERR_OOM;
+    }
+    *have = bytes;
+    return HF_OK;
+}
+
+// Return a fitted-tensor block: large blocks go to the device's cache (the
+// oldest one is freed when it is full), small ones are freed.
+template <class T>
+void big_release(hf_ctx* ctx, T*& p, size_t& have) {
+    if (!p) return;
+    void* q = (void*)p;
+    p = nullptr;
+    const size_t bytes = have;
+    have = 0;
+    if (bytes < kRetainMinBytes || ctx->device < 0 || ctx->device >= kRetainDevices) {
+        cudaFree(q);
+        return;
+    }
+    // the block may still be read by work queued on this context's stream
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    void* evict = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_retain_mutex);
+        auto& pool = g_retained[ctx->device];
+        if ((int)pool.size() >= kRetainBlocks) {
+            evict = pool.front().p;
+            pool.erase(pool.begin());
+        }
+        pool.push_back({q, bytes});
+    }
+    if (evict) cudaFree(evict);
 }
 
 // The build's stream-ordered temporaries (several GB for large molecules) come
@@ -333,12 +421,12 @@ int hf_ctx_destroy(hf_ctx* ctx) {
     free_shells(ctx);
     release(ctx->d_btable);
     release(ctx->d_metric);
-    release(ctx->d_B);
+    big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
     release(ctx->d_work);
     release(ctx->d_io);
     release(ctx->d_kscratch);
     release(ctx->d_stage);
-    release(ctx->d_bf16_b);
+    big_release(ctx, ctx->d_bf16_b, ctx->bf16_alloc_bytes);
     release(ctx->d_tcwork);
     release(ctx->d_ctc);
     release(ctx->d_info);
@@ -358,6 +446,19 @@ int hf_set_stream(hf_ctx* ctx, void* stream) {
     return HF_OK;
 }
 
+int hf_release_retained(int device) {
+    if (device < 0 || device >= kRetainDevices) return HF_ERR_ARG;
+    int previous = 0;
+    cudaGetDevice(&previous);
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return HF_ERR_ARG;
+    }
+    free_retained(device);
+    cudaSetDevice(previous);
+    return HF_OK;
+}
+
 int hf_set_wait_limit(hf_ctx* ctx, int64_t wait_ns, int stall_next_build) {
     if (!ctx) return HF_ERR_ARG;
     if (wait_ns < 1000 || wait_ns > 60000000000ll)
@@ -374,9 +475,9 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
     if ((s = check_table(ctx, orbt, "orbital", kMaxOrbL, false)) != HF_OK) return s;
     if (auxt && (s = check_table(ctx, auxt, "auxiliary", kMaxAuxL, true)) != HF_OK) return s;
     free_shells(ctx);
-    release(ctx->d_B);
+    big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
     release(ctx->d_metric);
-    release(ctx->d_bf16_b);
+    big_release(ctx, ctx->d_bf16_b, ctx->bf16_alloc_bytes);
     ctx->built = false;
     std::vector<double> exps, coefs;
     auto add = [&](const hf_shell_table* t, int64_t sh, int fn) {
@@ -605,9 +706,9 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     trelease(ctx, wk);
 
     // B = L^-1 (P|mu nu), chunked over tile rows.
-    release(ctx->d_B);
+    big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
     const int64_t ldb = ctx->ntiles * 4096;
-    if (alloc(ctx, (void**)&ctx->d_B, sizeof(double) * (size_t)N * ldb)) {
+    if (big_alloc(ctx, (void**)&ctx->d_B, sizeof(double) * (size_t)N * ldb, &ctx->b_alloc_bytes)) {
         trelease(ctx, Linv);
         return HF_ERR_OOM;
     }
@@ -736,13 +837,13 @@ static int exchange_from_ct(hf_ctx* ctx, const double* Ct, int opad, const doubl
 static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, double* dK, const double* sign = nullptr) {
     const JkPlan p = plan_of(ctx);
     if (!ctx->d_bf16_b) {
-        if (alloc(ctx, &ctx->d_bf16_b, tc_b_bytes(ctx->n, ctx->naux)))
+        if (big_alloc(ctx, &ctx->d_bf16_b, tc_b_bytes(ctx->n, ctx->naux), &ctx->bf16_alloc_bytes))
             return fail(ctx, HF_ERR_OOM, "no room for the BF16 copies of the fitted tensor (" +
                                              std::to_string(tc_b_bytes(ctx->n, ctx->naux)) + " bytes)");
         HF_CU(tc_split_b(p, t.npad, ctx->d_bf16_b, ctx->stream));
         int s = check_async(ctx, "BF16 copy of B");
         if (s != HF_OK) {
-            release(ctx->d_bf16_b);
+            big_release(ctx, ctx->d_bf16_b, ctx->bf16_alloc_bytes);
             return s;
         }
     }
@@ -835,6 +936,42 @@ int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const doub
     ctx->stats.exchange_rank = ncols;
     if (s == HF_OK) s = check_async(ctx, "hf_exchange_factored");
     return s;
+}
+
+int hf_density_factor(hf_ctx* ctx, const double* D, double* F, int64_t max_rank, int64_t* rank, int on_device) {
+    if (!ctx || !D || !F || !rank || max_rank < 1) return HF_ERR_ARG;
+    if (!ctx->uploaded) return fail(ctx, HF_ERR_STATE, "upload shells first");
+    cudaSetDevice(ctx->device);
+    const int64_t n = ctx->n;
+    const size_t nn = (size_t)n * n;
+    const int64_t cap = std::min<int64_t>(max_rank, n);
+    Carver cv;
+    const size_t oD = cv.take(nn), oL = cv.take((size_t)cap * n);
+    int st = ensure_scratch(ctx, &ctx->d_stage, &ctx->stage_bytes, sizeof(double) * cv.used);
+    if (st != HF_OK) return st;
+    double* sD = ctx->d_stage + oD;
+    double* Lc = on_device ? F : ctx->d_stage + oL;
+    const double* dD = D;
+    if (!on_device) {
+        HF_CU(cudaMemcpyAsync(sD, D, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
+        dD = sD;
+    }
+    time_begin(ctx);
+    HF_CU(cudaMemsetAsync(ctx->d_info, 0, 2 * sizeof(int), ctx->stream));
+    HF_CU(pivoted_cholesky(dD, 0, (int)n, 1e-14, (int)cap, Lc, 0, ctx->d_info, 1, nullptr, ctx->stream));
+    ++ctx->stats.kernel_launches;
+    int res[2] = {0, 0};
+    HF_CU(cudaMemcpyAsync(res, ctx->d_info, sizeof(res), cudaMemcpyDeviceToHost, ctx->stream));
+    HF_CU(cudaStreamSynchronize(ctx->stream));
+    ctx->stats.ms_factorize_density = time_end(ctx);
+    if (res[1])
+        return fail(ctx, HF_ERR_NUMERIC, "the density is not positive semidefinite");
+    *rank = res[0];
+    if (!on_device) {
+        HF_CU(cudaMemcpyAsync(F, Lc, sizeof(double) * (size_t)res[0] * n, cudaMemcpyDeviceToHost, ctx->stream));
+        return check_async(ctx, "hf_density_factor");
+    }
+    return HF_OK;
 }
 
 int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_device) {
@@ -1159,7 +1296,10 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
         size_t freeb = 0, totalb = 0;
         cudaMemGetInfo(&freeb, &totalb);
         const size_t need = sizeof(double) * (2 * (size_t)oo * N + 5 * NN + 4 * nn) + ((size_t)2 << 30);
-        if (ctx->d_bf16_b && freeb < need) release(ctx->d_bf16_b);
+        if (ctx->d_bf16_b && freeb < need) {
+            big_release(ctx, ctx->d_bf16_b, ctx->bf16_alloc_bytes);
+            free_retained(ctx->device);
+        }
     }
     const int nso = (int)ctx->orb.size(), nsa = (int)ctx->aux.size();
     struct Temps {

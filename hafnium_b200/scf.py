@@ -26,7 +26,7 @@ import numpy as np
 from hafnium_b200 import _lib
 from hafnium_b200.basis import ShellTable
 from hafnium_b200.errors import ConvergenceError, InputError
-from hafnium_b200.jk import B200DensityFittedCoulombExchange
+from hafnium_b200.jk import B200DensityFittedCoulombExchange, difference_factors
 
 NULL_SPACE_TOLERANCE = 1e-14  # diis.py:17
 DEFAULT_OVERLAP_THRESHOLD = 1e-10  # orthogonalization.py:12
@@ -70,19 +70,24 @@ class PrecisionSchedule:
     ``anchor_gradient``. The next build is an FP64 anchor K64(D_a), where the
     DIIS history restarts (it held BF16-accurate matrices). After it every
     build is incremental, K(D_n) = K64(D_a) + K16(D_n - D_a), with the
-    difference density factored exactly into its positive and negative parts,
-    so the BF16 error scales with |D_n - D_a| rather than with |D_n|. Once the
+    difference density factored exactly (``jk.difference_factors``), so the
+    BF16 error scales with |D_n - D_a| rather than with |D_n|. Once the
     gradient of an incremental build is below the convergence tolerance, the
-    builds are FP64 again. The convergence test then needs two FP64 energies,
-    and the finishing build (driver.py:336) serves as the second. If the
-    gradient stops falling (``stall_window`` builds without halving), FP64 takes
-    over at once. DIIS, the eigensolves, J and the energy are FP64 throughout.
+    finishing build (driver.py:336) is made in FP64 at the aufbau density of
+    that Fock matrix; its FP64 orbital gradient decides convergence. A gradient
+    below the tolerance bounds the energy error quadratically (far below the
+    energy tolerance), so this replaces the reference's test on two
+    consecutive FP64 energies, and the reported energy and density are FP64.
+    Otherwise that FP64 build becomes the new anchor and the iterations go on.
+    If the gradient stops falling (``stall_window`` builds without halving),
+    the BF16 phase moves to the anchor and the incremental phase re-anchors.
+    DIIS, the eigensolves, J and the energy are FP64 throughout; a mixed run
+    makes two FP64 exchange builds when nothing stalls.
     """
 
     mode: str = "fp64"
     anchor_gradient: float = 3e-3
     stall_window: int = 4
-    drop_tolerance: float = 1e-13
 
     def __post_init__(self) -> None:
         if self.mode not in ("fp64", "mixed"):
@@ -136,7 +141,11 @@ class DeviceHamiltonian:
         return cache[threshold]
 
     @classmethod
-    def build(cls, molecule, basis: str, auxiliary: str, *, device: int = 0) -> "DeviceHamiltonian":
+    def build(cls, molecule, basis: str, auxiliary: str, *, device: int = 0,
+              exchange_schedule: str = "fp64") -> "DeviceHamiltonian":
+        """One-electron integrals and the fitted two-body term of ``molecule``;
+        ``exchange_schedule`` is the builder's own schedule for ``exchange(D)``
+        (``"mixed"`` for the protocol-driven mixed-precision path)."""
         torch = _torch()
         t0 = time.perf_counter()
         orb = ShellTable.build(basis, molecule.symbols, molecule.positions)
@@ -164,7 +173,7 @@ class DeviceHamiltonian:
         ctx.build()
         torch.cuda.synchronize(dev)
         t2 = time.perf_counter()
-        two_body = B200DensityFittedCoulombExchange(ctx)
+        two_body = B200DensityFittedCoulombExchange(ctx, schedule=exchange_schedule)
         timings = {"one_electron_s": t1 - t0, "fitted_tensor_s": t2 - t1, **ctx.stats()}
         return cls(s, t + v, two_body, molecule.nuclear_repulsion_energy(), molecule.n_alpha, timings)
 
@@ -374,10 +383,12 @@ class _HostTwoBody:
 
 class _Rhf:
     def __init__(self, ham: DeviceHamiltonian, options: ScfOptions, schedule: PrecisionSchedule,
-                 host_io: bool = False, averaged: bool = False) -> None:
+                 host_io: bool = False, averaged: bool = False, protocol: bool = False) -> None:
         torch = _torch()
         self.torch = torch
         self.host_io = host_io
+        self.protocol = protocol
+        self.last_precision = "fp64"
         self.averaged = averaged
         self.h2d_bytes = 0
         self.d2h_bytes = 0
@@ -463,22 +474,15 @@ class _Rhf:
         return out
 
     def difference_factors(self, factor):
-        """(V, s) with D_n - D_a = V diag(s) V^T, s = +-1, from a thin QR of
-        [C_n, C_a]: [C_n, C_a] = Q R, D_n - D_a = Q (R S R^T) Q^T with
-        S = diag(I, -I), and the small middle matrix diagonalised; eigenvalues
-        below ``drop_tolerance`` of the largest are dropped."""
-        torch = self.torch
-        m = torch.cat([factor, self.anchor_factor], dim=1)
-        q, r = torch.linalg.qr(m)
-        k = factor.shape[1]
-        sign = torch.ones(m.shape[1], dtype=m.dtype, device=m.device)
-        sign[k:] = -1.0
-        t = (r * sign[None, :]) @ r.T
-        w, u = torch.linalg.eigh(0.5 * (t + t.T))
-        v = q @ u
-        cut = self.schedule.drop_tolerance * float(w.abs().max())
-        keep = w.abs() > cut
-        return (v[:, keep] * torch.sqrt(w[keep].abs())[None, :]).contiguous(), torch.sign(w[keep]).contiguous()
+        """(V+, V-) with D_n - D_a = V+ V+^T - V- V-^T (``jk.difference_factors``:
+        the anchor's orbitals rotated onto the current ones, then matrix products)."""
+        return difference_factors(factor, self.anchor_factor, self.ham.s)
+
+    def gradient_norm(self, f, d) -> float:
+        """driver.py:248-260: |X^T (F D S - S D F) X| with the factor 2 of the restricted trace."""
+        s = self.ham.s
+        g = self.x.T @ (f @ d @ s - s @ d @ f) @ self.x
+        return math.sqrt(2.0 * float(self.torch.sum(g * g))), g
 
     def exchange(self, d, factor, precision: str, two_body=None):
         """K for this iteration in the arithmetic ``precision`` names: ``fp64``,
@@ -496,18 +500,15 @@ class _Rhf:
             if factor is None:
                 return self._timed("bf16", lambda: two_body.context_exchange_bf16(d))
             return self._timed("bf16", lambda: two_body.exchange_factored(factor, precision=_lib.PREC_BF16X3))
-        v, sign = self.difference_factors(factor)
+        vp, vm = self.difference_factors(factor)
 
         def increment():
-            # the positive and negative parts as two unsigned split-BF16 builds: with
-            # n_occ columns each they keep the X chunks large (a single signed build
-            # over 2 n_occ columns measured 2.6x slower at (H2O)64)
+            # the positive and negative parts as two unsigned split-BF16 builds of
+            # n_occ columns each (a single signed build over 2 n_occ columns measured
+            # 2.6x slower at (H2O)64: its X chunks are four times smaller)
             out = self.anchor_k.clone()
-            pos, neg = sign > 0, sign < 0
-            if bool(pos.any()):
-                out += two_body.exchange_factored(v[:, pos].contiguous(), precision=_lib.PREC_BF16X3)
-            if bool(neg.any()):
-                out -= two_body.exchange_factored(v[:, neg].contiguous(), precision=_lib.PREC_BF16X3)
+            out += two_body.exchange_factored(vp, precision=_lib.PREC_BF16X3)
+            out -= two_body.exchange_factored(vm, precision=_lib.PREC_BF16X3)
             return out
 
         return self._timed("incremental", increment)
@@ -517,7 +518,16 @@ class _Rhf:
         torch = self.torch
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         ev[0].record()
-        if self.host_io:
+        if self.protocol:
+            # the reference's calls only: coulomb(2 D) and exchange(D), the builder
+            # choosing its own arithmetic (coulomb_exchange.py:426, 509)
+            two_body = _HostTwoBody(self.ham.two_body, self) if self.host_io else self.ham.two_body
+            j = two_body.coulomb((2.0 * d).contiguous())
+            ev[1].record()
+            k = two_body.exchange(d.contiguous())
+            log = getattr(getattr(self.ham.two_body, "schedule", None), "log", None)
+            self.last_precision = log[-1]["precision"] if log else "fp64"
+        elif self.host_io:
             # the reference-facing calls: host NumPy arrays in, host NumPy J/K out
             host = _HostTwoBody(self.ham.two_body, self)
             j = host.coulomb((2.0 * d).contiguous())
@@ -549,11 +559,10 @@ class _Rhf:
         else:
             d = torch.as_tensor(guess, dtype=torch.float64, device=self.ham.s.device)
             factor = None
-        s = self.ham.s
         focks, errors, history = [], [], []
-        mixed = self.schedule.mode == "mixed"
+        mixed = self.schedule.mode == "mixed" and not self.protocol
         precision = "bf16" if mixed else "fp64"
-        pending = None  # a Fock build already made for d (the mixed finish fallback)
+        pending = None  # a Fock build already made for d (after an FP64 finish that did not converge)
         f = None
         for index in range(opts.max_iterations):
             if pending is not None:
@@ -561,31 +570,33 @@ class _Rhf:
                 pending = None
             else:
                 f, _, energy = self.fock(d, factor, precision)
-            g = self.x.T @ (f @ d @ s - s @ d @ f) @ self.x
-            gnorm = math.sqrt(2.0 * float(torch.sum(g * g)))
+            gnorm, g = self.gradient_norm(f, d)
             previous = history[-1] if history else None
             change = energy - previous.energy if previous else math.inf
-            built = "fp64" if precision == "anchor" else precision
+            built = self.last_precision if self.protocol else ("fp64" if precision == "anchor" else precision)
             history.append(Iteration(index, energy, change, gnorm, built))
             converged = abs(change) < opts.energy_tolerance and gnorm < opts.gradient_tolerance
-            if built == "fp64" and not mixed:
+            if not mixed:
                 if converged:
                     return self.finish(f, history, True, t_start)
-            elif built == "fp64":
-                # the reference's test on two FP64 energies: the previous one, or
-                # else the finishing build (driver.py:336) made now
-                if converged and previous is not None and previous.precision == "fp64":
+            elif built != "bf16" and gnorm < opts.gradient_tolerance:
+                if built == "fp64" and converged:
                     return self.finish(f, history, True, t_start)
-                if gnorm < opts.gradient_tolerance:
-                    w, c = self.solve(f)
-                    d2, factor2 = self.density(w, c, averaged=False)
-                    f2, terms2, e2 = self.fock(d2, factor2, "fp64")
-                    if abs(e2 - energy) < opts.energy_tolerance:
-                        self.torch.cuda.synchronize()
-                        return ScfResult(e2, d2, f2, w, c, True, history, terms2, time.perf_counter() - t_start,
-                                         dict(self.timings))
-                    d, factor, pending = d2, factor2, (f2, e2)
-                    continue
+                # the finishing build (driver.py:336) in FP64 at the aufbau density
+                # of f; its exact orbital gradient decides convergence
+                w, c = self.solve(f)
+                d2, factor2 = self.density(w, c, averaged=False)
+                f2, terms2, e2 = self.fock(d2, factor2, "anchor")
+                g2, _ = self.gradient_norm(f2, d2)
+                if g2 < opts.gradient_tolerance:
+                    self.torch.cuda.synchronize()
+                    self.timings["final_gradient"] = g2
+                    return ScfResult(e2, d2, f2, w, c, True, history, terms2, time.perf_counter() - t_start,
+                                     dict(self.timings))
+                # not yet: that FP64 build is the new anchor and the iterations go on
+                d, factor, pending = d2, factor2, (f2, e2)
+                precision = "anchor"
+                continue
             if precision == "anchor":
                 precision = "incremental"
                 focks, errors = [], []  # the history held BF16-accurate matrices
@@ -594,11 +605,9 @@ class _Rhf:
             elif precision in ("bf16", "incremental"):
                 window = self.schedule.stall_window
                 recent = [h for h in history[-window - 1:] if h.precision == built]
-                stalled = len(recent) > window and gnorm > 0.5 * recent[0].gradient_norm
-                if precision == "bf16" and stalled:
+                if len(recent) > window and gnorm > 0.5 * recent[0].gradient_norm:
+                    # the gradient stopped halving: BF16 noise (or a far anchor) bounds it
                     precision = "anchor"
-                elif stalled or (precision == "incremental" and gnorm < opts.gradient_tolerance):
-                    precision = "fp64"
             focks = (focks + [f])[-opts.diis_size:]
             errors = (errors + [g])[-opts.diis_size:]
             if len(focks) == 1:
@@ -612,6 +621,7 @@ class _Rhf:
         raise ConvergenceError(f"the SCF did not converge in {opts.max_iterations} iterations", result)
 
     def finish(self, f, history, converged: bool, t_start: float) -> ScfResult:
+        """driver.py:331-366: one more Fock build from the aufbau density of ``f``."""
         w, c = self.solve(f)
         d, factor = self.density(w, c, averaged=False)
         final_f, terms, energy = self.fock(d, factor, "fp64")
@@ -621,13 +631,18 @@ class _Rhf:
 
 
 def solve_rhf(ham: DeviceHamiltonian, *, guess=None, options: ScfOptions | None = None,
-              schedule: PrecisionSchedule | None = None, host_io: bool = False) -> ScfResult:
+              schedule: PrecisionSchedule | None = None, host_io: bool = False, protocol: bool = False) -> ScfResult:
     """Converge the restricted state of ``ham`` on the device (driver.py:154-213).
 
     ``host_io`` routes every J and K through the drop-in's host-array API (NumPy
     density in, NumPy J/K out), as the unchanged reference driver would call it.
+    ``protocol`` makes the driver call nothing but ``coulomb(2 D)`` and
+    ``exchange(D)`` of the two-body builder, with the reference's convergence
+    test: the builder's own schedule (``B200DensityFittedCoulombExchange``
+    with ``schedule="mixed"``) then chooses each build's arithmetic, and
+    ``schedule`` is not used.
     """
-    rhf = _Rhf(ham, options or ScfOptions(), schedule or PrecisionSchedule(), host_io)
+    rhf = _Rhf(ham, options or ScfOptions(), schedule or PrecisionSchedule(), host_io, protocol=protocol)
     result = rhf.run(guess)
     result.timings["h2d_bytes"] = rhf.h2d_bytes
     result.timings["d2h_bytes"] = rhf.d2h_bytes

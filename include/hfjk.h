@@ -80,6 +80,14 @@ const char* hf_last_error(const hf_ctx* ctx);
 /* Launch on this stream (cudaStream_t) from now on; NULL = the context's own. */
 int hf_set_stream(hf_ctx* ctx, void* stream);
 
+/* The device blocks of fitted tensors (and their BF16 copies) of at least
+ * 1 GiB are not freed when a context is destroyed or rebuilt: up to two per
+ * device are kept and handed to the next context whose tensor fits, so a run
+ * over many geometries of one size maps them once. A failed allocation
+ * empties the cache first. This frees the blocks kept for `device` now.
+ * No reference counterpart (the reference holds host arrays only). */
+int hf_release_retained(int device);
+
 /* Limit of every device-side wait of the split-BF16 exchange's pipeline (its
  * mbarrier waits), in nanoseconds, 1 us .. 60 s; 2 s by default. A wait that
  * runs out ends the kernel cleanly (in-flight copies drained, tensor memory
@@ -117,6 +125,15 @@ int hf_coulomb(hf_ctx* ctx, const double* density, double* coulomb, int on_devic
  * the same process. The call returns once J is complete: it waits for the
  * context's stream. */
 int hf_coulomb_static(hf_ctx* ctx, const double* density, double* coulomb);
+
+/* A factor of a symmetric positive semidefinite density, D ~= F^T F: F holds
+ * *rank rows of n_ao (row-major [rank][n_ao], capacity max_rank rows) from a
+ * pivoted Cholesky stopped at 1e-14 of the largest diagonal element. It is the
+ * factorisation hf_exchange makes internally; the drop-in's mixed-precision
+ * exchange keeps it between calls to form difference densities. HF_ERR_NUMERIC
+ * for an indefinite D. No reference counterpart (the reference contracts D). */
+int hf_density_factor(hf_ctx* ctx, const double* density, double* factor, int64_t max_rank, int64_t* rank,
+                      int on_device);
 
 /* K[u][v] = sum_wx (uw|xv) D[w][x] (coulomb_exchange.py:184-190) for a symmetric
  * positive semidefinite D, factorised on the device by a pivoted Cholesky;

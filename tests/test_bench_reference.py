@@ -17,7 +17,7 @@ from tests.conftest import ROOT
 
 def test_reference_arm_prints_one_contract_line():
     out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=str(ROOT))
+                          "--warmup", "0", "--fit-waters", "4"], capture_output=True, text=True, timeout=600, cwd=str(ROOT))
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
@@ -31,3 +31,5 @@ def test_reference_arm_prints_one_contract_line():
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"] == {"value": line["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert [p["waters"] for p in line["measured"]] == [8, 4]
+    assert line["cpu_baseline"]["extrapolated"] is True and "fit" in line

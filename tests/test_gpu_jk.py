@@ -86,3 +86,29 @@ def test_shape_mismatch_raises(system):
     two_body, _ = system
     with pytest.raises(InputError):
         two_body.coulomb(np.zeros((3, 3)))
+
+
+def test_a_rebuilt_context_takes_the_retained_fitted_tensor_block():
+    """The fitted tensor of (H2O)16 (1.2 GB) is kept when its context closes and
+    handed to the next context of that size, so the second build makes one
+    device allocation fewer and gives the same J."""
+    import torch
+
+    from hafnium_b200 import _lib
+
+    _lib.release_retained(0)
+    mol = molecule("h2o16_s0")
+    orb, aux = tables(mol)
+    counts, coulombs = [], []
+    rng = np.random.default_rng(2)
+    for _ in range(2):
+        two_body = B200DensityFittedCoulombExchange.from_tables(orb, aux)
+        if not coulombs:
+            c = rng.normal(size=(two_body.n_ao, 30)) / np.sqrt(two_body.n_ao)
+            d = torch.as_tensor(c @ c.T, device="cuda")
+        counts.append(two_body.stats()["device_allocations"])
+        coulombs.append(two_body.coulomb(d).cpu().numpy())
+        two_body.context.close()
+    assert counts[1] == counts[0] - 1
+    np.testing.assert_array_equal(coulombs[0], coulombs[1])
+    _lib.release_retained(0)

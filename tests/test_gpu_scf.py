@@ -58,18 +58,83 @@ def test_sad_started_scf_follows_the_reference_iterations(tag):
 
 @pytest.mark.parametrize("tag", ["h2o4_s1", "h2o8_s2", "h2o12_s3", "h2o16_s0", "h2o32_s0"])
 def test_mixed_schedule_matches_reference(tag):
-    """Split-BF16 builds, an FP64 anchor, incremental builds on the signed difference
-    density, then FP64: the reference's converged FP64 energy and density."""
+    """Split-BF16 builds, an FP64 anchor, incremental builds on the exactly
+    factored difference density, then the finishing build in FP64, whose orbital
+    gradient decides convergence (the reference's default tolerances): the
+    reference's converged FP64 energy and density, with two FP64 exchange builds."""
     from hafnium_b200.scf import PrecisionSchedule, atomic_density_guess
 
     ref = golden_run(tag)
     mol = molecule(tag)
     ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
+    result = solve_rhf(ham, guess=atomic_density_guess(mol, "cc-pvdz"), schedule=PrecisionSchedule(mode="mixed"))
+    assert result.converged
+    assert {"bf16", "incremental", "fp64"} <= {h.precision for h in result.history}
+    assert result.timings["exchange_builds_fp64"] == 2  # the anchor and the finishing build
+    assert result.timings["final_gradient"] < 1e-6
+    assert abs(result.energy - float(ref["energy"])) <= 1e-8
+    assert np.max(np.abs(result.density.cpu().numpy() - ref["density"])) <= 1e-6
+
+
+def test_mixed_schedule_at_tight_tolerances():
+    """At tolerances far below the defaults the incremental builds still reach the
+    gradient (re-anchoring if the BF16 rounding of a far anchor stalls them) and
+    the FP64 finish confirms it."""
+    from hafnium_b200.scf import PrecisionSchedule, atomic_density_guess
+
+    ref = golden_run("h2o8_s2")
+    mol = molecule("h2o8_s2")
+    ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
     result = solve_rhf(ham, guess=atomic_density_guess(mol, "cc-pvdz"),
                        options=ScfOptions(energy_tolerance=1e-11, gradient_tolerance=1e-8),
                        schedule=PrecisionSchedule(mode="mixed"))
+    assert result.converged and result.timings["final_gradient"] < 1e-8
+    assert result.timings["exchange_builds_fp64"] <= 4
+    assert abs(result.energy - float(ref["energy"])) <= 1e-8
+    assert np.max(np.abs(result.density.cpu().numpy() - ref["density"])) <= 1e-6
+
+
+@pytest.mark.parametrize("tag", ["h2o4_s1", "h2o8_s2", "h2o16_s0"])
+def test_reference_driver_with_the_mixed_builder_matches_reference(tag):
+    """The reference's SCF loop (restated by the oracle: it calls nothing but
+    coulomb(2 D) and exchange(D), with host NumPy arrays, and tests convergence
+    on two consecutive energies) over the drop-in with schedule="mixed": the
+    builder alone chooses split-BF16, anchored incremental and FP64 builds from
+    the densities it is given, and the result is the reference's."""
+    from hafnium_b200.basis import ShellTable
+    from hafnium_b200.jk import B200DensityFittedCoulombExchange
+    from oracle import dfrhf
+
+    ref = golden_run(tag)
+    mol = molecule(tag)
+    orb = ShellTable.build("cc-pvdz", mol.symbols, mol.positions)
+    aux = ShellTable.build("def2-universal-jkfit", mol.symbols, mol.positions)
+    two_body = B200DensityFittedCoulombExchange.from_tables(orb, aux, schedule="mixed")
+    s = dfrhf.overlap(orb)
+    h = dfrhf.core_hamiltonian(orb, mol.nuclear_charges, mol.positions)
+    guess = dfrhf.atomic_density_guess(orb, mol.symbols, {"O": 8.0, "H": 1.0})
+    result = dfrhf.solve_rhf(s, h, two_body, mol.nuclear_repulsion_energy(), mol.n_alpha, guess=guess)
+    kinds = [entry["precision"] for entry in two_body.schedule.log]
+    assert kinds[0] == "bf16" and "incremental" in kinds
+    assert 1 <= kinds.count("anchor") <= 2
+    assert abs(result.energy - float(ref["energy"])) <= 1e-8
+    assert np.max(np.abs(result.density - ref["density"])) <= 1e-6
+
+
+@pytest.mark.parametrize("tag", ["h2o12_s3", "h2o32_s0"])
+def test_protocol_only_device_driver_matches_reference(tag):
+    """The device driver in protocol mode (only coulomb(2 D) / exchange(D) on host
+    NumPy arrays, the reference's convergence test) over the mixed builder."""
+    from hafnium_b200.scf import atomic_density_guess
+
+    ref = golden_run(tag)
+    mol = molecule(tag)
+    ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit", exchange_schedule="mixed")
+    result = solve_rhf(ham, guess=atomic_density_guess(mol, "cc-pvdz"), protocol=True, host_io=True)
     assert result.converged
-    assert {"bf16", "incremental", "fp64"} <= {h.precision for h in result.history}
+    kinds = [h.precision for h in result.history]
+    assert kinds[0] == "bf16" and "incremental" in kinds and "anchor" in kinds
+    assert result.timings["h2d_bytes"] > 0 and result.timings["d2h_bytes"] > 0
     assert abs(result.energy - float(ref["energy"])) <= 1e-8
     assert np.max(np.abs(result.density.cpu().numpy() - ref["density"])) <= 1e-6
 
