@@ -25,7 +25,7 @@ EXPORTS = (
     "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
     "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_four_center", "hf_get_stats",
     "hf_coulomb_static", "hf_mp2_energy", "hf_nuclear_gradient", "hf_mo_fitted_tensor", "hf_set_wait_limit",
-    "hf_boys", "hf_release_retained", "hf_density_factor",
+    "hf_boys", "hf_release_retained", "hf_density_factor", "hf_set_fitted_rows",
 )
 
 BATCH_EXPORTS = (
@@ -127,6 +127,7 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_boys.argtypes = [v, v, i64, i, v]
     lib.hf_release_retained.argtypes = [i]
     lib.hf_density_factor.argtypes = [v, v, v, i64, p(i64), i]
+    lib.hf_set_fitted_rows.argtypes = [v, i64, i64]
     lib.hf_mp2_energy.argtypes = [v, v, v, i64, i64, ctypes.POINTER(ctypes.c_double), i]
     lib.hf_nuclear_gradient.argtypes = [v, v, i64, v, v, v, i64, v, i]
     lib.hf_mo_fitted_tensor.argtypes = [v, v, i64, v, i64, v, i]
@@ -228,8 +229,28 @@ class Context:
         self.check(self.lib.hf_shells_upload(self.handle, ctypes.byref(o), ctypes.byref(a)), "hf_shells_upload")
         del keep_o, keep_a
 
+    def set_fitted_rows(self, row0: int, row1: int) -> None:
+        """Hold only rows [row0, row1) of the fitted tensor (a shard by auxiliary index)."""
+        self.check(self.lib.hf_set_fitted_rows(self.handle, int(row0), int(row1)), "hf_set_fitted_rows")
+
     def build(self) -> None:
-        self.check(self.lib.hf_build_fitted_tensor(self.handle), "hf_build_fitted_tensor")
+        """The fitted tensor on the device. When the device is out of memory, the
+        contexts Python no longer references are collected (their tensors freed)
+        and torch's cached blocks released before one more attempt."""
+        status = self.lib.hf_build_fitted_tensor(self.handle)
+        if status == HF_ERR_OOM:
+            import gc
+
+            gc.collect()
+            try:
+                import torch
+
+                if torch.cuda.is_available():
+                    torch.cuda.empty_cache()
+            except ImportError:  # pragma: no cover - torch is a dependency of the device path
+                pass
+            status = self.lib.hf_build_fitted_tensor(self.handle)
+        self.check(status, "hf_build_fitted_tensor")
 
     def dims(self) -> tuple[int, int]:
         n, naux = ctypes.c_int64(), ctypes.c_int64()

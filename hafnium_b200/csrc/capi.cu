@@ -5,7 +5,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <future>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -68,6 +70,9 @@ struct hf_ctx {
     int* d_info = nullptr;
     double* d_scalar = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // rows [row0, row1) of the fitted tensor held here (internal auxiliary order;
+    // row1 < 0: all of them), for a tensor sharded over devices by auxiliary index
+    int row0 = 0, row1 = -1;
     // bounded device waits of the split-BF16 exchange (hf_set_wait_limit)
     uint64_t wait_ns = 2000000000ull;  // 2 s: far above any legitimate wait there
     int stall_next = 0;                // the next split-BF16 build runs the stall self-test
@@ -79,6 +84,10 @@ int fail(hf_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
 }
+
+// Rows of the fitted tensor this context holds, and whether it holds them all.
+int fitted_rows(const hf_ctx* c) { return (c->row1 < 0 ? c->naux : c->row1) - c->row0; }
+bool holds_all_rows(const hf_ctx* c) { return c->row0 == 0 && fitted_rows(c) == c->naux; }
 
 #define HF_CU(call)                                                                           \
     do {                                                                                      \
@@ -106,17 +115,18 @@ void release(T*& p) {
     p = nullptr;
 }
 
-// Retained device blocks for the fitted tensor and its BF16 copy (tens of GB at
-// the largest clusters). A context that is destroyed, or that rebuilds for
-// another molecule, hands these blocks to a per-device cache instead of
-// freeing them, and the next context on that device whose tensor fits takes
-// one back: a run over many geometries of one size (a scan, a benchmark)
-// then maps its two large tensors once instead of once per geometry, and a
-// cudaFree of tens of GB, which synchronises the device, is avoided. At most
-// kRetainBlocks blocks are kept per device; a failed allocation empties the
-// cache and retries; hf_release_retained frees it on request.
-constexpr size_t kRetainMinBytes = (size_t)1 << 30;
-constexpr int kRetainBlocks = 2;
+// Retained device blocks: the fitted tensor and its BF16 copy (tens of GB at the
+// largest clusters) and the J/K scratch areas. A context that is destroyed, or
+// that rebuilds for another molecule, hands its blocks of at least
+// kRetainMinBytes to a per-device cache instead of freeing them, and the next
+// context on that device whose request fits takes one back: a run over many
+// geometries of one size (a scan, a benchmark) then maps its large buffers
+// once instead of once per geometry, and a cudaFree of tens of GB, which
+// synchronises the device, is avoided. At most kRetainBlocks blocks are kept
+// per device; a failed allocation empties the cache and retries;
+// hf_release_retained frees it on request.
+constexpr size_t kRetainMinBytes = (size_t)256 << 20;
+constexpr int kRetainBlocks = 8;
 constexpr int kRetainDevices = 64;
 struct Retained {
     void* p;
@@ -234,20 +244,14 @@ void trelease(hf_ctx* ctx, T*& p) {
 
 int ensure_work(hf_ctx* ctx, size_t bytes) {
     if (ctx->work_bytes >= bytes) return HF_OK;
-    release(ctx->d_work);
-    ctx->work_bytes = 0;
-    int s = alloc(ctx, (void**)&ctx->d_work, bytes);
-    if (s == HF_OK) ctx->work_bytes = bytes;
-    return s;
+    big_release(ctx, ctx->d_work, ctx->work_bytes);
+    return big_alloc(ctx, (void**)&ctx->d_work, bytes, &ctx->work_bytes);
 }
 
 int ensure_io(hf_ctx* ctx, size_t bytes) {
     if (ctx->io_bytes >= bytes) return HF_OK;
-    release(ctx->d_io);
-    ctx->io_bytes = 0;
-    int s = alloc(ctx, (void**)&ctx->d_io, bytes);
-    if (s == HF_OK) ctx->io_bytes = bytes;
-    return s;
+    big_release(ctx, ctx->d_io, ctx->io_bytes);
+    return big_alloc(ctx, (void**)&ctx->d_io, bytes, &ctx->io_bytes);
 }
 
 // Validation of integrals/mod.rs:111-173 plus the device kernels' limits.
@@ -330,11 +334,8 @@ struct Carver {
 // Grow-only scratch owned by the context: the K build's Kp/X chunks.
 int ensure_scratch(hf_ctx* ctx, double** p, size_t* have, size_t bytes) {
     if (*have >= bytes) return HF_OK;
-    release(*p);
-    *have = 0;
-    int s = alloc(ctx, (void**)p, bytes);
-    if (s == HF_OK) *have = bytes;
-    return s;
+    big_release(ctx, *p, *have);
+    return big_alloc(ctx, (void**)p, bytes, have);
 }
 
 int check_async(hf_ctx* ctx, const char* what) {
@@ -349,6 +350,7 @@ int check_async(hf_ctx* ctx, const char* what) {
 namespace hf {
 int context_view(const hf_ctx* ctx, TensorView* out) {
     if (!ctx || !out) return HF_ERR_ARG;
+    if (!holds_all_rows(ctx)) return HF_ERR_STATE;
     out->device = ctx->device;
     out->B = ctx->d_B;
     out->n = ctx->n;
@@ -422,13 +424,13 @@ int hf_ctx_destroy(hf_ctx* ctx) {
     release(ctx->d_btable);
     release(ctx->d_metric);
     big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
-    release(ctx->d_work);
-    release(ctx->d_io);
-    release(ctx->d_kscratch);
-    release(ctx->d_stage);
+    big_release(ctx, ctx->d_work, ctx->work_bytes);
+    big_release(ctx, ctx->d_io, ctx->io_bytes);
+    big_release(ctx, ctx->d_kscratch, ctx->kscratch_bytes);
+    big_release(ctx, ctx->d_stage, ctx->stage_bytes);
     big_release(ctx, ctx->d_bf16_b, ctx->bf16_alloc_bytes);
-    release(ctx->d_tcwork);
-    release(ctx->d_ctc);
+    big_release(ctx, ctx->d_tcwork, ctx->tcwork_bytes);
+    big_release(ctx, ctx->d_ctc, ctx->ctc_bytes);
     release(ctx->d_info);
     release(ctx->d_scalar);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -443,6 +445,21 @@ const char* hf_last_error(const hf_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 int hf_set_stream(hf_ctx* ctx, void* stream) {
     if (!ctx) return HF_ERR_ARG;
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+    return HF_OK;
+}
+
+int hf_set_fitted_rows(hf_ctx* ctx, int64_t row0, int64_t row1) {
+    if (!ctx) return HF_ERR_ARG;
+    if (!ctx->uploaded) return fail(ctx, HF_ERR_STATE, "upload shells first");
+    if (row0 < 0 || row1 <= row0 || row1 > ctx->naux)
+        return fail(ctx, HF_ERR_ARG, "the rows lie in 0 <= row0 < row1 <= n_aux = " + std::to_string(ctx->naux) +
+                                         " (got " + std::to_string(row0) + ", " + std::to_string(row1) + ")");
+    cudaSetDevice(ctx->device);
+    big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
+    big_release(ctx, ctx->d_bf16_b, ctx->bf16_alloc_bytes);
+    ctx->built = false;
+    ctx->row0 = (int)row0;
+    ctx->row1 = (int)row1;
     return HF_OK;
 }
 
@@ -479,6 +496,8 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
     release(ctx->d_metric);
     big_release(ctx, ctx->d_bf16_b, ctx->bf16_alloc_bytes);
     ctx->built = false;
+    ctx->row0 = 0;
+    ctx->row1 = -1;
     std::vector<double> exps, coefs;
     auto add = [&](const hf_shell_table* t, int64_t sh, int fn) {
         DevShell d{};
@@ -598,10 +617,33 @@ static double pair_bound(const hf_ctx* ctx, const DevShell& A, const DevShell& B
     return best;
 }
 
-// Pair tasks for tile rows [row0, row1): pairs (a <= b) with a touching those rows
-// and at least one primitive pair above the screening bound.
-static void chunk_tasks(const hf_ctx* ctx, int row0, int row1, std::vector<PairTask> (&tasks)[3][3],
-                        int (&max_npp)[3][3]) {
+// Every shell pair (a <= b) with at least one primitive pair above the screening
+// bound, listed by its first shell; the host threads split the first shells.
+static std::vector<std::vector<PairTask>> screen_pairs(const hf_ctx* ctx) {
+    const int ns = (int)ctx->orb.size();
+    std::vector<std::vector<PairTask>> by_a(ns);
+    auto work = [&](int begin, int step) {
+        for (int a = begin; a < ns; a += step) {
+            const DevShell& A = ctx->orb[a];
+            for (int b = a; b < ns; ++b) {
+                const DevShell& B = ctx->orb[b];
+                if (pair_bound(ctx, A, B, ctx->h_exps, ctx->h_coefs) < 1e-22) continue;
+                by_a[a].push_back(PairTask{a, b, A.l > B.l ? 1 : 0, 0});
+            }
+        }
+    };
+    const int nthreads = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) pool.emplace_back(work, t, nthreads);
+    work(0, nthreads);
+    for (auto& t : pool) t.join();
+    return by_a;
+}
+
+// Pair tasks for tile rows [row0, row1): the screened pairs whose first shell
+// touches those rows, bucketed by (la <= lb).
+static void chunk_tasks_from(const hf_ctx* ctx, const std::vector<std::vector<PairTask>>& by_a, int row0, int row1,
+                             std::vector<PairTask> (&tasks)[3][3], int (&max_npp)[3][3]) {
     for (auto& r : tasks)
         for (auto& v : r) v.clear();
     for (auto& r : max_npp)
@@ -611,18 +653,18 @@ static void chunk_tasks(const hf_ctx* ctx, int row0, int row1, std::vector<PairT
         const DevShell& A = ctx->orb[a];
         const int f0 = A.fn, f1 = A.fn + A.ncontr * nsph(A.l) - 1;
         if ((f1 >> 6) < row0 || (f0 >> 6) >= row1) continue;
-        for (int b = a; b < ns; ++b) {
-            const DevShell& B = ctx->orb[b];
-            if (pair_bound(ctx, A, B, ctx->h_exps, ctx->h_coefs) < 1e-22) continue;
-            int la = A.l, lb = B.l, swap = 0;
-            if (la > lb) {
-                std::swap(la, lb);
-                swap = 1;
-            }
-            tasks[la][lb].push_back(PairTask{a, b, swap, 0});
+        for (const PairTask& t : by_a[a]) {
+            const DevShell& B = ctx->orb[t.second];
+            const int la = std::min(A.l, B.l), lb = std::max(A.l, B.l);
+            tasks[la][lb].push_back(t);
             max_npp[la][lb] = std::max(max_npp[la][lb], A.nprim * B.nprim);
         }
     }
+}
+
+static void chunk_tasks(const hf_ctx* ctx, int row0, int row1, std::vector<PairTask> (&tasks)[3][3],
+                        int (&max_npp)[3][3]) {
+    chunk_tasks_from(ctx, screen_pairs(ctx), row0, row1, tasks, max_npp);
 }
 
 // Three-centre integrals of tile rows [row0, row1) into T ([cols][naux]).
@@ -657,6 +699,8 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     cudaSetDevice(ctx->device);
     const int N = ctx->naux;
     int s;
+    // the host screens the shell pairs while the device builds and factors the metric
+    auto screened = std::async(std::launch::async, [ctx]() { return screen_pairs(ctx); });
     time_begin(ctx);
     if ((s = build_metric(ctx)) != HF_OK) return s;
     ctx->stats.ms_metric = time_end(ctx);
@@ -708,60 +752,106 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     // B = L^-1 (P|mu nu), chunked over tile rows.
     big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
     const int64_t ldb = ctx->ntiles * 4096;
-    if (big_alloc(ctx, (void**)&ctx->d_B, sizeof(double) * (size_t)N * ldb, &ctx->b_alloc_bytes)) {
+    const int rows = fitted_rows(ctx), row0 = ctx->row0, row1 = row0 + rows;
+    if (big_alloc(ctx, (void**)&ctx->d_B, sizeof(double) * (size_t)rows * ldb, &ctx->b_alloc_bytes)) {
         trelease(ctx, Linv);
         return HF_ERR_OOM;
     }
-    ctx->stats.b_bytes = (int64_t)sizeof(double) * N * ldb;
+    ctx->stats.b_bytes = (int64_t)sizeof(double) * rows * ldb;
+    // Chunks of tile rows whose three-centre integrals fit one buffer; each chunk's
+    // integrals, then its fit. (Running the integrals of the next chunk beside the
+    // fit of this one, on a second stream, measured no faster at (H2O)64: both
+    // need the FP64 units.)
     const size_t row_bytes = sizeof(double) * 4096 * (size_t)N * ctx->nt;  // the widest row
     size_t budget = std::max<size_t>(row_bytes, (size_t)4 << 30);
     budget = std::min<size_t>(budget, sizeof(double) * 4096 * (size_t)N * ctx->ntiles);
     size_t freeb = 0, totalb = 0;
     cudaMemGetInfo(&freeb, &totalb);
     if (budget > freeb / 2) budget = std::max(row_bytes, freeb / 2);
-    double* T = nullptr;
-    const size_t ns = ctx->orb.size();
-    PairTask* d_tasks = nullptr;
-    const size_t task_cap = ns * (ns + 1) / 2 + 16;
-    if (talloc(ctx, (void**)&T, budget) || talloc(ctx, (void**)&d_tasks, sizeof(PairTask) * task_cap)) {
-        trelease(ctx, T);
-        trelease(ctx, Linv);
-        return HF_ERR_OOM;
-    }
-    double ms3c = 0.0, msfit = 0.0;
+    std::vector<std::pair<int, int>> chunks;
     for (int row0 = 0; row0 < ctx->nt;) {
         int row1 = row0 + 1;
         while (row1 < ctx->nt &&
                sizeof(double) * 4096 * (size_t)N * (tile_index(row1 + 1, row1 + 1, ctx->nt) - tile_index(row0, row0, ctx->nt)) <= budget)
             ++row1;
-        const int64_t t0 = tile_index(row0, row0, ctx->nt), t1 = tile_index(row1, row1, ctx->nt);
-        const int64_t ncols = (t1 - t0) * 4096;
-        time_begin(ctx);
-        HF_CU(cudaMemsetAsync(T, 0, sizeof(double) * (size_t)ncols * N, ctx->stream));
-        if ((s = three_center_chunk(ctx, row0, row1, T, d_tasks, task_cap)) != HF_OK) {
-            trelease(ctx, T);
-            trelease(ctx, d_tasks);
-            trelease(ctx, Linv);
-            return s;
-        }
-        ms3c += time_end(ctx);
-        time_begin(ctx);
-        HF_CU(apply_inverse_factor(Linv, N, N, T, N, ncols, ctx->d_B + t0 * 4096, ldb, ctx->stream));
-        ++ctx->stats.kernel_launches;
-        if ((s = check_async(ctx, "fitted tensor chunk")) != HF_OK) {
-            trelease(ctx, T);
-            trelease(ctx, d_tasks);
-            trelease(ctx, Linv);
-            return s;
-        }
-        msfit += time_end(ctx);
+        chunks.push_back({row0, row1});
         row0 = row1;
     }
+    // every chunk's pair tasks, built on the host first and copied in one go
+    struct Launch {
+        int la, lb, max_npp;
+        size_t off, count;
+    };
+    std::vector<std::vector<Launch>> launches(chunks.size());
+    std::vector<PairTask> all_tasks;
+    const std::vector<std::vector<PairTask>> by_a = screened.get();
+    for (size_t c = 0; c < chunks.size(); ++c) {
+        std::vector<PairTask> tasks[3][3];
+        int max_npp[3][3];
+        chunk_tasks_from(ctx, by_a, chunks[c].first, chunks[c].second, tasks, max_npp);
+        for (int la = 0; la <= 2; ++la)
+            for (int lb = la; lb <= 2; ++lb) {
+                const auto& v = tasks[la][lb];
+                if (v.empty()) continue;
+                launches[c].push_back(Launch{la, lb, max_npp[la][lb], all_tasks.size(), v.size()});
+                all_tasks.insert(all_tasks.end(), v.begin(), v.end());
+            }
+    }
+    double* T = nullptr;
+    PairTask* d_tasks = nullptr;
+    if (talloc(ctx, (void**)&d_tasks, sizeof(PairTask) * std::max<size_t>(1, all_tasks.size())) ||
+        talloc(ctx, (void**)&T, budget)) {
+        trelease(ctx, T);
+        trelease(ctx, d_tasks);
+        trelease(ctx, Linv);
+        return HF_ERR_OOM;
+    }
+    if (!all_tasks.empty())
+        HF_CU(cudaMemcpyAsync(d_tasks, all_tasks.data(), sizeof(PairTask) * all_tasks.size(), cudaMemcpyHostToDevice,
+                              ctx->stream));
+    // per chunk: start, integrals done, fit done (timing only; one stream)
+    const size_t nc = chunks.size();
+    std::vector<cudaEvent_t> ev(3 * nc, nullptr);
+    for (auto& x : ev) cudaEventCreate(&x);
+    cudaError_t e = cudaSuccess;
+    for (size_t c = 0; c < nc && e == cudaSuccess; ++c) {
+        const int row0 = chunks[c].first, row1 = chunks[c].second;
+        const int64_t t0 = tile_index(row0, row0, ctx->nt), t1 = tile_index(row1, row1, ctx->nt);
+        const int64_t ncols = (t1 - t0) * 4096;
+        cudaEventRecord(ev[3 * c], ctx->stream);
+        e = cudaMemsetAsync(T, 0, sizeof(double) * (size_t)ncols * N, ctx->stream);
+        const ChunkDesc cd{row0, row1, ctx->nt, t0, ctx->naux};
+        for (const Launch& l : launches[c]) {
+            if (e != cudaSuccess) break;
+            e = launch_three_center(l.la, l.lb, d_tasks + l.off, (int)l.count, l.max_npp, ctx->d_orb, ctx->d_aux,
+                                    ctx->d_exps, ctx->d_coefs, ctx->d_aux_by_l, ctx->aux_count, ctx->d_btable, cd, T,
+                                    ctx->stream);
+            ctx->stats.kernel_launches += 5;
+        }
+        cudaEventRecord(ev[3 * c + 1], ctx->stream);
+        if (e == cudaSuccess)
+            e = apply_inverse_factor(Linv, N, N, T, N, ncols, ctx->d_B + t0 * 4096, ldb, ctx->stream, row0, row1);
+        ++ctx->stats.kernel_launches;
+        cudaEventRecord(ev[3 * c + 2], ctx->stream);
+    }
+    cudaError_t se = cudaStreamSynchronize(ctx->stream);  // the host task vector outlives its copy
+    if (e == cudaSuccess) e = se;
+    if (e == cudaSuccess) e = cudaGetLastError();
+    double ms3c = 0.0, msfit = 0.0;
+    if (e == cudaSuccess)
+        for (size_t c = 0; c < nc; ++c) {
+            float a = 0.f, b = 0.f;
+            cudaEventElapsedTime(&a, ev[3 * c], ev[3 * c + 1]);
+            cudaEventElapsedTime(&b, ev[3 * c + 1], ev[3 * c + 2]);
+            ms3c += a;
+            msfit += b;
+        }
+    for (auto& x : ev) cudaEventDestroy(x);
     trelease(ctx, T);
     trelease(ctx, d_tasks);
     trelease(ctx, Linv);
+    if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("fitted tensor: ") + cudaGetErrorString(e));
     HF_CU(cudaStreamSynchronize(ctx->stream));
-    HF_CU(cudaGetLastError());
     ctx->stats.ms_three_center = ms3c;
     ctx->stats.ms_fit = msfit;
     ctx->built = true;
@@ -775,7 +865,7 @@ static JkPlan plan_of(const hf_ctx* ctx) {
     p.n = ctx->n;
     p.nt = ctx->nt;
     p.ntiles = ctx->ntiles;
-    p.naux = ctx->naux;
+    p.naux = fitted_rows(ctx);
     return p;
 }
 
@@ -814,7 +904,7 @@ static int exchange_from_ct(hf_ctx* ctx, const double* Ct, int opad, const doubl
     cudaMemGetInfo(&freeb, &totalb);
     const size_t per_q = sizeof(double) * npad * opad * (any_negative ? 2 : 1);
     size_t budget = std::min<size_t>((size_t)4 << 30, freeb / 3);
-    int qchunk = (int)std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)ctx->naux));
+    int qchunk = (int)std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)p.naux));
     qchunk = std::min(qchunk, 65535);
     const size_t kp_doubles = (size_t)round_up(npad * npad, 32);
     const size_t part_doubles = (size_t)round_up(syrk_partial_doubles(npad, 1), 32);
@@ -827,7 +917,7 @@ static int exchange_from_ct(hf_ctx* ctx, const double* Ct, int opad, const doubl
     double* Xs = any_negative ? X + npad * (int64_t)qchunk * opad : nullptr;
     cudaError_t e = exchange_build_fp64(p, Ct, opad, any_negative ? sign : nullptr, dK, Kp, X, Xs, part, qchunk,
                                         ctx->stream);
-    ctx->stats.kernel_launches += 3 * ((ctx->naux + qchunk - 1) / qchunk) + 2;
+    ctx->stats.kernel_launches += 3 * ((p.naux + qchunk - 1) / qchunk) + 2;
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("exchange: ") + cudaGetErrorString(e));
     return check_async(ctx, "exchange");
 }
@@ -837,9 +927,9 @@ static int exchange_from_ct(hf_ctx* ctx, const double* Ct, int opad, const doubl
 static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, double* dK, const double* sign = nullptr) {
     const JkPlan p = plan_of(ctx);
     if (!ctx->d_bf16_b) {
-        if (big_alloc(ctx, &ctx->d_bf16_b, tc_b_bytes(ctx->n, ctx->naux), &ctx->bf16_alloc_bytes))
+        if (big_alloc(ctx, &ctx->d_bf16_b, tc_b_bytes(ctx->n, p.naux), &ctx->bf16_alloc_bytes))
             return fail(ctx, HF_ERR_OOM, "no room for the BF16 copies of the fitted tensor (" +
-                                             std::to_string(tc_b_bytes(ctx->n, ctx->naux)) + " bytes)");
+                                             std::to_string(tc_b_bytes(ctx->n, p.naux)) + " bytes)");
         HF_CU(tc_split_b(p, t.npad, ctx->d_bf16_b, ctx->stream));
         int s = check_async(ctx, "BF16 copy of B");
         if (s != HF_OK) {
@@ -854,7 +944,7 @@ static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, doub
     const size_t kp_doubles = (size_t)round_up(t.npad * t.npad, 32);
     size_t budget = std::min<size_t>((size_t)2 << 30, freeb / 3);
     size_t want = round_up((int64_t)ct_bytes, 256) + tc_partial_bytes(t.npad) +
-                  per_q * std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)ctx->naux));
+                  per_q * std::max<size_t>(1, std::min<size_t>(budget / per_q, (size_t)p.naux));
     want = round_up((int64_t)want, 256) + sizeof(double) * kp_doubles;
     int st = ensure_scratch(ctx, &ctx->d_tcwork, &ctx->tcwork_bytes, want);
     if (st != HF_OK) return st;
@@ -865,7 +955,7 @@ static int exchange_bf16(hf_ctx* ctx, const TcPlan& t, const double* Ct_tc, doub
     ctx->stall_next = 0;
     cudaError_t e = exchange_build_bf16(t, ctx->d_bf16_b, Ct_tc, t.npad, dK, Kp, work, want - sizeof(double) * kp_doubles,
                                         wait, ctx->stream, ctx->n, sign);
-    ctx->stats.kernel_launches += 3 * ((ctx->naux + 1023) / 1024) + 3;
+    ctx->stats.kernel_launches += 3 * ((p.naux + 1023) / 1024) + 3;
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("split-BF16 exchange: ") + cudaGetErrorString(e));
     int s = check_async(ctx, "split-BF16 exchange");
     if (s != HF_OK) return s;
@@ -911,7 +1001,7 @@ int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const doub
         dw = w ? sw : nullptr;
     }
     if (precision == HF_PREC_BF16X3) {
-        const TcPlan t = tc_plan(n, ctx->naux, ncols);
+        const TcPlan t = tc_plan(n, fitted_rows(ctx), ncols);
         int sc = ensure_scratch(ctx, &ctx->d_ctc, &ctx->ctc_bytes, sizeof(double) * ((size_t)t.opad * t.npad + t.opad));
         if (sc != HF_OK) return sc;
         double* Ct_tc = ctx->d_ctc;
@@ -1008,7 +1098,7 @@ int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_d
                                          "hf_exchange_factored");
     const int64_t rank = res[0];
     if (precision == HF_PREC_BF16X3) {
-        const TcPlan t = tc_plan(n, ctx->naux, rank);
+        const TcPlan t = tc_plan(n, fitted_rows(ctx), rank);
         int sc = ensure_scratch(ctx, &ctx->d_ctc, &ctx->ctc_bytes, sizeof(double) * ((size_t)t.opad * t.npad + t.opad));
         if (sc != HF_OK) return sc;
         double* Ct_tc = ctx->d_ctc;
@@ -1092,6 +1182,7 @@ int hf_three_center(hf_ctx* ctx, double* out) {
 int hf_fitted_eri(hf_ctx* ctx, double* out) {
     if (!ctx || !out) return HF_ERR_ARG;
     if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    if (!holds_all_rows(ctx)) return fail(ctx, HF_ERR_STATE, "this needs every row of the fitted tensor; the context holds a shard");
     cudaSetDevice(ctx->device);
     const int N = ctx->naux, n = ctx->n, nt = ctx->nt;
     const int64_t ldb = ctx->ntiles * 4096;
@@ -1192,6 +1283,7 @@ int hf_mp2_energy(hf_ctx* ctx, const double* mo_coefficients, const double* mo_e
     if (!ctx || !mo_coefficients || !mo_energies || !correlation || n_mo < 1 || n_occ < 1 || n_occ > n_mo)
         return HF_ERR_ARG;
     if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    if (!holds_all_rows(ctx)) return fail(ctx, HF_ERR_STATE, "this needs every row of the fitted tensor; the context holds a shard");
     if (n_mo > ctx->n) return fail(ctx, HF_ERR_ARG, "more orbitals than basis functions");
     cudaSetDevice(ctx->device);
     const JkPlan p = plan_of(ctx);
@@ -1219,6 +1311,7 @@ int hf_mo_fitted_tensor(hf_ctx* ctx, const double* c_bra, int64_t n_bra, const d
                         double* out, int on_device) {
     if (!ctx || !c_bra || !c_ket || !out || n_bra < 1 || n_ket < 1) return HF_ERR_ARG;
     if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    if (!holds_all_rows(ctx)) return fail(ctx, HF_ERR_STATE, "this needs every row of the fitted tensor; the context holds a shard");
     cudaSetDevice(ctx->device);
     const JkPlan p = plan_of(ctx);
     const int64_t n = ctx->n, N = ctx->naux;
@@ -1279,6 +1372,7 @@ int hf_nuclear_gradient(hf_ctx* ctx, const double* C, int64_t nocc, const double
                         const double* positions, int64_t natoms, double* terms, int on_device) {
     if (!ctx || !C || !W || !charges || !positions || !terms || nocc < 1 || natoms < 1) return HF_ERR_ARG;
     if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    if (!holds_all_rows(ctx)) return fail(ctx, HF_ERR_STATE, "this needs every row of the fitted tensor; the context holds a shard");
     if (nocc > ctx->n) return fail(ctx, HF_ERR_ARG, "more occupied orbitals than basis functions");
     if ((int64_t)nocc * nocc > INT32_MAX / 2) return fail(ctx, HF_ERR_ARG, "too many occupied orbitals");
     cudaSetDevice(ctx->device);

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN
     double* C = g.C + (int64_t)zz * g.strideC;
     int kb = 0, ke = g.K;
     if (g.kmode == 1) kb = n0;
-    if (g.kmode == 2) ke = min(g.K, m0 + BM);
+    if (g.kmode == 2) ke = min(g.K, g.koff + m0 + BM);
     kb = (kb / BK) * BK;
     if (g.splits > 1) {
         const int span = ((ke - kb + g.splits - 1) / g.splits + BK - 1) / BK * BK;

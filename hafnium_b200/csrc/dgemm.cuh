@@ -8,7 +8,8 @@
 //
 // kmode restricts the k range per output tile (triangular operands):
 //   0: [0, K)   1: [n0, K) (Bop upper: Bop[n][k] = 0 for k < n)
-//   2: [0, min(K, m0 + BM)) (A lower: A[m][k] = 0 for k > m)
+//   2: [0, min(K, koff + m0 + BM)) (A lower: A[m][k] = 0 for k > koff + m, koff the
+//      row of the full triangle that A's first row is)
 // epi selects the store:
 //   0: C[m][n] (row stride ldc)      1: C[n][m] (transposed store)
 //   2: as 0, only tiles touching the lower triangle (n0 <= m0 + BM - 1)
@@ -43,6 +44,7 @@ struct GemmArgs {
     const double* beta_v;
     int tile;    // index into kTileShapes
     int splits;  // > 1: split-K; blockIdx.z = batch * splits + split, C + blockIdx.z * strideC
+    int koff;    // kmode 2: the first row of A within its triangle
 };
 
 // CTA tile shapes (BM x BN); warps = (BM / 32) * (BN / 32).

@@ -218,12 +218,14 @@ cudaError_t triangular_inverse(const double* L, int n, int64_t ld, double* Linv,
 }
 
 cudaError_t apply_inverse_factor(const double* Linv, int n, int64_t ld, const double* T, int64_t ldt, int64_t ncols,
-                                 double* B, int64_t ldb, cudaStream_t stream) {
+                                 double* B, int64_t ldb, cudaStream_t stream, int row0, int row1) {
+    if (row1 < 0) row1 = n;
     GemmArgs g{};
-    g.M = n;
+    g.M = row1 - row0;
     g.N = (int)ncols;
-    g.K = n;
-    g.A = Linv;
+    g.K = row1;  // L^-1 is lower triangular: rows below row1 need columns below row1
+    g.koff = row0;
+    g.A = Linv + (int64_t)row0 * ld;
     g.lda = ld;
     g.B = T;
     g.ldb = ldt;

@@ -107,7 +107,11 @@ class MixedExchangeSchedule:
     """
 
     def __init__(self, two_body, anchor_change: float = 1e-3, final_change: float = 1e-5) -> None:
-        self.two_body = two_body
+        import weakref
+
+        # a weak reference: the builder owns this schedule, and a cycle would keep
+        # the builder's device memory (tens of GB) alive until a garbage collection
+        self.two_body = weakref.proxy(two_body)
         self.anchor_change = anchor_change
         self.final_change = final_change
         self._overlap = None
@@ -172,11 +176,15 @@ class B200DensityFittedCoulombExchange:
 
     @classmethod
     def from_tables(cls, orbital, auxiliary, *, device: int = 0, precision: int = _lib.PREC_FP64,
-                    schedule: str = "fp64"):
+                    schedule: str = "fp64", rows: tuple[int, int] | None = None):
         """Build from structure-of-arrays shell tables (``hafnium_b200.basis.ShellTable``
-        or the reference's own ``hafnium.integrals.ShellTable``)."""
+        or the reference's own ``hafnium.integrals.ShellTable``). ``rows`` keeps
+        only those rows of the fitted tensor (a shard by auxiliary index,
+        ``hafnium_b200.sharded``): J and K are then the sums over those rows."""
         context = _lib.Context(device)
         context.upload(orbital, auxiliary)
+        if rows is not None:
+            context.set_fitted_rows(*rows)
         context.build()
         return cls(context, precision, schedule)
 

@@ -80,12 +80,13 @@ const char* hf_last_error(const hf_ctx* ctx);
 /* Launch on this stream (cudaStream_t) from now on; NULL = the context's own. */
 int hf_set_stream(hf_ctx* ctx, void* stream);
 
-/* The device blocks of fitted tensors (and their BF16 copies) of at least
- * 1 GiB are not freed when a context is destroyed or rebuilt: up to two per
- * device are kept and handed to the next context whose tensor fits, so a run
- * over many geometries of one size maps them once. A failed allocation
- * empties the cache first. This frees the blocks kept for `device` now.
- * No reference counterpart (the reference holds host arrays only). */
+/* The device blocks of fitted tensors, their BF16 copies and the J/K scratch
+ * areas, when at least 256 MiB, are not freed when a context is destroyed or
+ * rebuilt: up to eight per device are kept and handed to the next context
+ * whose request fits, so a run over many geometries of one size maps them
+ * once. A failed allocation empties the cache first. This frees the blocks
+ * kept for `device` now. No reference counterpart (the reference holds host
+ * arrays only). */
 int hf_release_retained(int device);
 
 /* Limit of every device-side wait of the split-BF16 exchange's pipeline (its
@@ -106,6 +107,19 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbital, const hf_shell_
  * device (replaces DensityFitting.build + df_tensor, density_fitting.py:59-107,
  * and the Rust coulomb_two_center / coulomb_three_center, two_electron.rs:74-297). */
 int hf_build_fitted_tensor(hf_ctx* ctx);
+
+/* Hold only rows [row0, row1) of the fitted tensor (auxiliary functions in the
+ * library's internal order: shells sorted by angular momentum), for a tensor
+ * sharded over devices by auxiliary index. Call after hf_shells_upload and
+ * before hf_build_fitted_tensor; the rows of all shards must cover
+ * 0 .. n_aux - 1 once. J and K of such a context are the sums over its rows,
+ * J = sum_{q in rows} (B_q . D) B_q and K = sum_{q in rows} B_q D B_q, which the
+ * caller adds over the shards (an all-reduce of n_ao^2 doubles each); the
+ * metric is factored in full on every shard, and the three-centre integrals of
+ * the rows below row1 are computed. MP2, the orbital-basis tensor, the fitted
+ * ERIs and the gradient need every row (HF_ERR_STATE otherwise). No reference
+ * counterpart (the reference is not distributed). */
+int hf_set_fitted_rows(hf_ctx* ctx, int64_t row0, int64_t row1);
 
 int hf_dims(const hf_ctx* ctx, int64_t* n_ao, int64_t* n_aux);
 

@@ -36,7 +36,9 @@ def install(reference: pathlib.Path | None = None) -> None:
     if shims not in sys.path:
         sys.path.insert(0, shims)
     if str(reference) not in sys.path:
-        sys.path.insert(1, str(reference))
+        # last: the reference tree has its own ``tests`` package, which must not
+        # shadow this repository's
+        sys.path.append(str(reference))
     if str(HERE.parent) not in sys.path:
         sys.path.insert(0, str(HERE.parent))
     from oracle import kernels

@@ -110,5 +110,37 @@ def test_a_rebuilt_context_takes_the_retained_fitted_tensor_block():
         coulombs.append(two_body.coulomb(d).cpu().numpy())
         two_body.context.close()
     assert counts[1] == counts[0] - 1
-    np.testing.assert_array_equal(coulombs[0], coulombs[1])
+    np.testing.assert_allclose(coulombs[0], coulombs[1], atol=1e-13, rtol=0)
     _lib.release_retained(0)
+
+
+@pytest.mark.parametrize("tag", ["h2o4_s1", "h2o12_s3"])
+def test_row_shards_of_the_fitted_tensor_sum_to_the_whole(tag):
+    """Three contexts holding rows [0, q1), [q1, q2), [q2, N) of B (the split a
+    process group over three GPUs would make, here on one GPU): their J and K
+    add up to the whole tensor's, in FP64 to 1e-10 and split-BF16 to the split's
+    own error; a shard refuses what needs every row."""
+    import torch
+
+    from hafnium_b200 import _lib
+    from hafnium_b200.errors import InputError
+    from hafnium_b200.sharded import shard_rows
+
+    mol = molecule(tag)
+    orb, aux = tables(mol)
+    whole = B200DensityFittedCoulombExchange.from_tables(orb, aux)
+    shards = [B200DensityFittedCoulombExchange.from_tables(orb, aux, rows=shard_rows(whole.n_aux, 3, r))
+              for r in range(3)]
+    d, c = psd_density(whole.n_ao, 25, 4)
+    dt = torch.as_tensor(d, device="cuda")
+    ct = torch.as_tensor(c, device="cuda")
+    j = sum(s.coulomb(dt) for s in shards)
+    k = sum(s.exchange(dt) for s in shards)
+    np.testing.assert_allclose(j.cpu().numpy(), whole.coulomb(d), atol=JK_TOL, rtol=0)
+    np.testing.assert_allclose(k.cpu().numpy(), whole.exchange(d), atol=JK_TOL, rtol=0)
+    k16 = sum(s.exchange_factored(ct, precision=_lib.PREC_BF16X3) for s in shards).cpu().numpy()
+    k64 = whole.exchange_factored(c)
+    assert np.max(np.abs(k16 - k64)) <= 1e-4 * np.max(np.abs(k64))
+    assert sum(s.stats()["b_bytes"] for s in shards) == whole.stats()["b_bytes"]
+    with pytest.raises(InputError, match="every row"):
+        shards[1].orbital_tensor(c[:, :3], c[:, :3])
