@@ -752,7 +752,8 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
     // B = L^-1 (P|mu nu), chunked over tile rows.
     big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
     const int64_t ldb = ctx->ntiles * 4096;
-    const int rows = fitted_rows(ctx), row0 = ctx->row0, row1 = row0 + rows;
+    // the auxiliary rows [q_begin, q_end) this context holds
+    const int rows = fitted_rows(ctx), q_begin = ctx->row0, q_end = q_begin + rows;
     if (big_alloc(ctx, (void**)&ctx->d_B, sizeof(double) * (size_t)rows * ldb, &ctx->b_alloc_bytes)) {
         trelease(ctx, Linv);
         return HF_ERR_OOM;
@@ -830,7 +831,7 @@ int hf_build_fitted_tensor(hf_ctx* ctx) {
         }
         cudaEventRecord(ev[3 * c + 1], ctx->stream);
         if (e == cudaSuccess)
-            e = apply_inverse_factor(Linv, N, N, T, N, ncols, ctx->d_B + t0 * 4096, ldb, ctx->stream, row0, row1);
+            e = apply_inverse_factor(Linv, N, N, T, N, ncols, ctx->d_B + t0 * 4096, ldb, ctx->stream, q_begin, q_end);
         ++ctx->stats.kernel_launches;
         cudaEventRecord(ev[3 * c + 2], ctx->stream);
     }
