@@ -23,7 +23,7 @@ LIBRARY = OUT_DIR / "libhfjk.so"
 INCLUDE = HERE.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", f"-I{INCLUDE}"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-Xcompiler", "-Wshadow=local", f"-I{INCLUDE}"]
 
 
 def nvcc() -> str:

@@ -47,7 +47,7 @@ struct hf_ctx {
     double* d_exps = nullptr;
     double* d_coefs = nullptr;
     int* d_aux_by_l[kMaxAuxL + 1] = {};
-    double* d_btable = nullptr;
+    const double* d_btable = nullptr;  // shared by the device's contexts (shared_boys_table)
     // tensors
     double* d_metric = nullptr;  // N x N internal order
     double* d_B = nullptr;       // N x ntiles*4096
@@ -97,9 +97,30 @@ bool holds_all_rows(const hf_ctx* c) { return c->row0 == 0 && fitted_rows(c) == 
                         std::string(#call) + ": " + cudaGetErrorString(_e));                  \
     } while (0)
 
+// Device memory that a context keeps. Blocks below kRetainMinBytes (shell
+// tables, the metric, small scratch) come from the device's stream-ordered
+// pool (cudaMallocAsync on the context's stream, then that stream is waited
+// for, so the block can be used anywhere at once): unlike cudaMalloc and
+// cudaFree, which may synchronise the whole device, the pool serves them
+// without a device-wide synchronisation, which matters when many contexts are
+// built at once (the batched SCF's clusters). Larger blocks are cudaMalloc'd
+// (and retained, below). cudaFree releases both kinds; every caller frees a
+// block only after the work that used it has completed.
+constexpr size_t kPoolMaxBytes = (size_t)256 << 20;
 int alloc(hf_ctx* ctx, void** p, size_t bytes) {
     ctx->stats.device_allocations++;
-    cudaError_t e = cudaMalloc(p, bytes ? bytes : 8);
+    const size_t size = bytes ? bytes : 8;
+    cudaError_t e = cudaErrorMemoryAllocation;
+    if (size < kPoolMaxBytes && ctx->stream) {
+        e = cudaMallocAsync(p, size, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+            cudaGetLastError();
+        }
+    }
+    if (e != cudaSuccess) e = cudaMalloc(p, size);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
@@ -113,6 +134,35 @@ template <class T>
 void release(T*& p) {
     if (p) cudaFree((void*)p);
     p = nullptr;
+}
+
+// The Boys-function Taylor grid (boys_grid_host) on each device, uploaded once
+// and shared by every context there: a constant of the library, like the c2s
+// tables, so a context's creation needs no copy and no synchronisation for it.
+// Resolved with that device current; kept until the process exits.
+const double* shared_boys_table(int device) {
+    static std::mutex mutex;
+    static double* tables[64] = {};
+    if (device < 0 || device >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mutex);
+    if (!tables[device]) {
+        const auto grid = boys_grid_host();
+        double* p = nullptr;
+        if (cudaMalloc((void**)&p, sizeof(double) * grid.size()) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        // a copy from pageable memory may return before its DMA lands: wait for the
+        // device, so kernels on any stream see the table
+        if (cudaMemcpy(p, grid.data(), sizeof(double) * grid.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaDeviceSynchronize() != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(p);
+            return nullptr;
+        }
+        tables[device] = p;
+    }
+    return tables[device];
 }
 
 // Retained device blocks: the fitted tensor and its BF16 copy (tens of GB at the
@@ -390,17 +440,13 @@ int hf_ctx_create(int device, hf_ctx** out) {
     cudaEventCreate(&ctx->ev1);
     upload_c2s(ctx->stream);
     keep_pool_memory(device);
-    auto grid = boys_grid_host();
-    if (alloc(ctx, (void**)&ctx->d_btable, sizeof(double) * grid.size()) != HF_OK ||
-        alloc(ctx, (void**)&ctx->d_info, 4 * sizeof(int)) != HF_OK ||
+    ctx->d_btable = shared_boys_table(device);
+    if (!ctx->d_btable || alloc(ctx, (void**)&ctx->d_info, 4 * sizeof(int)) != HF_OK ||
         alloc(ctx, (void**)&ctx->d_scalar, 4 * sizeof(double)) != HF_OK) {
         hf_ctx_destroy(ctx);
         return HF_ERR_OOM;
     }
-    // stream-ordered copies: a synchronous cudaMemcpy from pageable memory may
-    // return before its DMA lands, unordered with kernels on this non-blocking stream
-    cudaMemcpyAsync(ctx->d_btable, grid.data(), sizeof(double) * grid.size(), cudaMemcpyHostToDevice, ctx->stream);
-    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    if (cudaGetLastError() != cudaSuccess) {
         hf_ctx_destroy(ctx);
         return HF_ERR_CUDA;
     }
@@ -421,7 +467,6 @@ int hf_ctx_destroy(hf_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_shells(ctx);
-    release(ctx->d_btable);
     release(ctx->d_metric);
     big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
     big_release(ctx, ctx->d_work, ctx->work_bytes);
