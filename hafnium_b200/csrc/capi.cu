@@ -677,7 +677,9 @@ static std::vector<std::vector<PairTask>> screen_pairs(const hf_ctx* ctx) {
             }
         }
     };
-    const int nthreads = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    // a thread per 64 first shells, at most 16: small molecules are screened on the
+    // calling thread (many of them are built at once by the batched SCF's threads)
+    const int nthreads = std::max(1, std::min({16, (int)std::thread::hardware_concurrency(), ns / 64}));
     std::vector<std::thread> pool;
     for (int t = 1; t < nthreads; ++t) pool.emplace_back(work, t, nthreads);
     work(0, nthreads);

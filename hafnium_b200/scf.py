@@ -88,6 +88,7 @@ class PrecisionSchedule:
     mode: str = "fp64"
     anchor_gradient: float = 3e-3
     stall_window: int = 4
+    restart_diis_at_anchor: bool = True
 
     def __post_init__(self) -> None:
         if self.mode not in ("fp64", "mixed"):
@@ -599,7 +600,8 @@ class _Rhf:
                 continue
             if precision == "anchor":
                 precision = "incremental"
-                focks, errors = [], []  # the history held BF16-accurate matrices
+                if self.schedule.restart_diis_at_anchor:
+                    focks, errors = [], []  # the history held BF16-accurate matrices
             elif precision == "bf16" and gnorm < self.schedule.anchor_gradient:
                 precision = "anchor"
             elif precision in ("bf16", "incremental"):
