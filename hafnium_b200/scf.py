@@ -86,7 +86,7 @@ class PrecisionSchedule:
     """
 
     mode: str = "fp64"
-    anchor_gradient: float = 3e-3
+    anchor_gradient: float = 1e-3
     stall_window: int = 4
     restart_diis_at_anchor: bool = True
 
