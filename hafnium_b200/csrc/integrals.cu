@@ -276,11 +276,14 @@ struct PairLayout {
     static constexpr int NSA = nsph(LA), NSB = nsph(LB), NSAB = NSA * NSB;
     static constexpr int KA = kMaxOrbContr[LA], KB = kMaxOrbContr[LB], KK = KA * KB;
     static constexpr int NH = ntet(LA + LB);
-    // per primitive pair: p, Px, Py, Pz, cc[KK], Etil[NSAB][NH]
-    static constexpr int STRIDE = 4 + KK + NSAB * NH;
+    // per primitive pair: p, Px, Py, Pz, 1/p, cc[KK], Etil[NSAB][NH]
+    static constexpr int CC = 5, ET = CC + KK;
+    static constexpr int STRIDE = ET + NSAB * NH;
 };
 
 
+// s_pos holds 2 kMaxPrimPairs + 1 ints: [pp0] -> compacted index or -1, the count
+// at [kMaxPrimPairs], and compacted index -> pp0 from [kMaxPrimPairs + 1].
 template <int LA, int LB>
 __device__ int pair_prologue(const DevShell& A, const DevShell& B, const double* __restrict__ exps,
                              const double* __restrict__ coefs, double* smem, int* s_pos) {
@@ -289,6 +292,7 @@ __device__ int pair_prologue(const DevShell& A, const DevShell& B, const double*
     const int npp = A.nprim * B.nprim;
     const double abx = A.x - B.x, aby = A.y - B.y, abz = A.z - B.z;
     const double rab2 = abx * abx + aby * aby + abz * abz;
+    int* s_src = s_pos + kMaxPrimPairs + 1;
     // significance flags, then a serial prefix (npp <= 256) for a deterministic order
     for (int pp0 = threadIdx.x; pp0 < npp; pp0 += blockDim.x) {
         const int i = pp0 / B.nprim, j = pp0 % B.nprim;
@@ -305,42 +309,57 @@ __device__ int pair_prologue(const DevShell& A, const DevShell& B, const double*
         for (int pp0 = 0; pp0 < npp; ++pp0) {
             const int keep = s_pos[pp0];
             s_pos[pp0] = keep ? k : -1;
+            if (keep) s_src[k] = pp0;
             k += keep;
         }
         s_pos[kMaxPrimPairs] = k;
     }
     __syncthreads();
-    for (int pp0 = threadIdx.x; pp0 < npp; pp0 += blockDim.x) {
-        const int pp = s_pos[pp0];
-        if (pp < 0) continue;
+    // One task per (surviving primitive pair, spherical component pair m): the
+    // pair's row Etil[m][*] (each task builds that pair's Cartesian Hermite
+    // tables itself), and for m = 0 the pair's scalars. Spreading the rows over
+    // the threads matters for the high angular momenta, whose shells have one or
+    // few primitives.
+    const int nk = s_pos[kMaxPrimPairs];
+    for (int w = threadIdx.x; w < nk * PL::NSAB; w += blockDim.x) {
+        const int pp = w / PL::NSAB, m = w - pp * PL::NSAB;
+        const int ma = m / PL::NSB, mb = m - ma * PL::NSB;
+        const int pp0 = s_src[pp];
         const int i = pp0 / B.nprim, j = pp0 % B.nprim;
         const double a = exps[A.prim + i], b = exps[B.prim + j];
         const double p = a + b;
         const double mu = a * b / p;
         const double px = (a * A.x + b * B.x) / p, py = (a * A.y + b * B.y) / p, pz = (a * A.z + b * B.z) / p;
         double* s = smem + pp * PL::STRIDE;
-        s[0] = p;
-        s[1] = px;
-        s[2] = py;
-        s[3] = pz;
+        if (m == 0) {
+            s[0] = p;
+            s[1] = px;
+            s[2] = py;
+            s[3] = pz;
+            s[4] = 1.0 / p;
 #pragma unroll
-        for (int ka = 0; ka < PL::KA; ++ka)
+            for (int ka = 0; ka < PL::KA; ++ka)
 #pragma unroll
-            for (int kb = 0; kb < PL::KB; ++kb)
-                s[4 + ka * PL::KB + kb] = (ka < A.ncontr && kb < B.ncontr)
-                                              ? coefs[A.coef + ka * A.nprim + i] * coefs[B.coef + kb * B.nprim + j]
-                                              : 0.0;
+                for (int kb = 0; kb < PL::KB; ++kb)
+                    s[PL::CC + ka * PL::KB + kb] = (ka < A.ncontr && kb < B.ncontr)
+                                                  ? coefs[A.coef + ka * A.nprim + i] * coefs[B.coef + kb * B.nprim + j]
+                                                  : 0.0;
+        }
         Hermite1D<LA, LB> ex, ey, ez;
         const double e00 = exp(-mu * rab2);
         ex.build(p, e00, px - A.x, px - B.x);
         ey.build(p, 1.0, py - A.y, py - B.y);
         ez.build(p, 1.0, pz - A.z, pz - B.z);
-        double* et = s + 4 + PL::KK;
-        for (int k = 0; k < PL::NSAB * PL::NH; ++k) et[k] = 0.0;
+        double* et = s + PL::ET + m * PL::NH;
+        for (int h = 0; h < PL::NH; ++h) et[h] = 0.0;
 #pragma unroll 1
-        for (int ca = 0; ca < NCA; ++ca)
+        for (int ca = 0; ca < NCA; ++ca) {
+            const double ra = c_c2s[c2s_offset(LA) + ma * NCA + ca];
+            if (ra == 0.0) continue;
 #pragma unroll 1
             for (int cb = 0; cb < NCB; ++cb) {
+                const double w2 = ra * c_c2s[c2s_offset(LB) + mb * NCB + cb];
+                if (w2 == 0.0) continue;
                 const int ix = c_cart[LA][ca][0], iy = c_cart[LA][ca][1], iz = c_cart[LA][ca][2];
                 const int jx = c_cart[LB][cb][0], jy = c_cart[LB][cb][1], jz = c_cart[LB][cb][2];
 #pragma unroll 1
@@ -348,22 +367,13 @@ __device__ int pair_prologue(const DevShell& A, const DevShell& B, const double*
 #pragma unroll 1
                     for (int u = 0; u <= iy + jy; ++u)
 #pragma unroll 1
-                        for (int v = 0; v <= iz + jz; ++v) {
-                            const double w = ex.e[ix][jx][t] * ey.e[iy][jy][u] * ez.e[iz][jz][v];
-#pragma unroll 1
-                            for (int ma = 0; ma < PL::NSA; ++ma) {
-                                const double wa = c_c2s[c2s_offset(LA) + ma * NCA + ca] * w;
-                                if (wa == 0.0) continue;
-#pragma unroll 1
-                                for (int mb = 0; mb < PL::NSB; ++mb)
-                                    et[(ma * PL::NSB + mb) * PL::NH + tet(t, u, v)] +=
-                                        c_c2s[c2s_offset(LB) + mb * NCB + cb] * wa;
-                            }
-                        }
+                        for (int v = 0; v <= iz + jz; ++v)
+                            et[tet(t, u, v)] += w2 * ex.e[ix][jx][t] * ey.e[iy][jy][u] * ez.e[iz][jz][v];
             }
+        }
     }
     __syncthreads();
-    return s_pos[kMaxPrimPairs];
+    return nk;
 }
 
 template <int LA, int LB, int LP>
@@ -381,7 +391,7 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
     constexpr int NCP = ncart(LP), NSP = nsph(LP);
     constexpr int SPB = 128 / NSP;  // aux shells per CTA
     extern __shared__ double smem[];
-    __shared__ int s_pos[kMaxPrimPairs + 1];
+    __shared__ int s_pos[2 * kMaxPrimPairs + 1];
     const PairTask task = tasks[blockIdx.x];
     const DevShell A = orb[task.swap ? task.second : task.first];
     const DevShell B = orb[task.swap ? task.first : task.second];
@@ -404,12 +414,17 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
 
     for (int i = 0; i < P.nprim; ++i) {
         const double q = exps[P.prim + i];
+        const double inv_q = 1.0 / q;
         double cq = coefs[P.coef + i] * pow(2.0 * q, -(double)LP);
         if (LP & 1) cq = -cq;
+        cq *= kTwoPi52 * inv_q;
         for (int pp = 0; pp < npp; ++pp) {
             const double* s = smem + pp * PL::STRIDE;
             const double p = s[0];
-            const double alpha = p * q / (p + q);
+            // one division per primitive triple: 1/(p+q) gives both the reduced
+            // exponent and the prefactor 2 pi^(5/2) / (p q sqrt(p+q))
+            const double inv_pq = 1.0 / (p + q);
+            const double alpha = p * q * inv_pq;
             double R[ntet(L)];
             hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, R);
             double G[ntet(LAB)];
@@ -422,8 +437,8 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
                     g += crow[c] * R[tet(tu + c_cart[LP][c][0], uu + c_cart[LP][c][1], vu + c_cart[LP][c][2])];
                 G[h] = g;
             }
-            const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * cq;
-            const double* et = s + 4 + PL::KK;
+            const double pref = s[4] * sqrt(inv_pq) * cq;
+            const double* et = s + PL::ET;
 #pragma unroll
             for (int m = 0; m < PL::NSAB; ++m) {
                 double val = 0.0;
@@ -431,7 +446,7 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
                 for (int h = 0; h < PL::NH; ++h) val += et[m * PL::NH + h] * G[h];
                 val *= pref;
 #pragma unroll
-                for (int k = 0; k < PL::KK; ++k) acc[k][m] += s[4 + k] * val;
+                for (int k = 0; k < PL::KK; ++k) acc[k][m] += s[PL::CC + k] * val;
             }
         }
     }
