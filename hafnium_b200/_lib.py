@@ -25,7 +25,8 @@ EXPORTS = (
     "hf_build_fitted_tensor", "hf_dims", "hf_coulomb", "hf_exchange", "hf_exchange_factored",
     "hf_metric", "hf_three_center", "hf_fitted_eri", "hf_one_electron", "hf_four_center", "hf_get_stats",
     "hf_coulomb_static", "hf_mp2_energy", "hf_nuclear_gradient", "hf_mo_fitted_tensor", "hf_set_wait_limit",
-    "hf_boys", "hf_release_retained", "hf_density_factor", "hf_set_fitted_rows",
+    "hf_boys", "hf_release_retained", "hf_density_factor", "hf_set_fitted_rows", "hf_exchange_scheduled",
+    "hf_schedule_reset",
 )
 
 BATCH_EXPORTS = (
@@ -58,6 +59,14 @@ class ShellTableC(ctypes.Structure):
         ("coefficients", ctypes.c_void_p),
         ("n_contractions", ctypes.c_void_p),
     ]
+
+
+class ScheduleC(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("anchor_change", ctypes.c_double), ("final_change", ctypes.c_double)]
+
+
+SCHEDULE_FP64, SCHEDULE_MIXED = 0, 1
+BUILD_KINDS = {0: "fp64", 1: "bf16", 2: "anchor", 3: "incremental"}
 
 
 class StatsC(ctypes.Structure):
@@ -128,6 +137,8 @@ def load(path: pathlib.Path | str | None = None) -> ctypes.CDLL:
     lib.hf_release_retained.argtypes = [i]
     lib.hf_density_factor.argtypes = [v, v, v, i64, p(i64), i]
     lib.hf_set_fitted_rows.argtypes = [v, i64, i64]
+    lib.hf_exchange_scheduled.argtypes = [v, v, v, i, p(ScheduleC), p(i)]
+    lib.hf_schedule_reset.argtypes = [v]
     lib.hf_mp2_energy.argtypes = [v, v, v, i64, i64, ctypes.POINTER(ctypes.c_double), i]
     lib.hf_nuclear_gradient.argtypes = [v, v, i64, v, v, v, i64, v, i]
     lib.hf_mo_fitted_tensor.argtypes = [v, v, i64, v, i64, v, i]
@@ -330,6 +341,23 @@ class Context:
         torch_sync(s)
         self.check(self.lib.hf_one_electron(self.handle, 0, None, None, 0, s.data_ptr(), 1), "hf_one_electron")
         return s
+
+    def exchange_scheduled(self, d, out, schedule: "ScheduleC") -> str:
+        """K of ``d`` into ``out`` through hf_exchange_scheduled (torch CUDA tensors,
+        or host NumPy arrays); returns the arithmetic the schedule chose."""
+        kind = ctypes.c_int(-1)
+        if hasattr(d, "data_ptr"):
+            torch_sync(d)
+            status = self.lib.hf_exchange_scheduled(self.handle, d.data_ptr(), out.data_ptr(), 1,
+                                                    ctypes.byref(schedule), ctypes.byref(kind))
+        else:
+            status = self.lib.hf_exchange_scheduled(self.handle, d.ctypes.data, out.ctypes.data, 0,
+                                                    ctypes.byref(schedule), ctypes.byref(kind))
+        self.check(status, "hf_exchange_scheduled")
+        return BUILD_KINDS.get(kind.value, str(kind.value))
+
+    def schedule_reset(self) -> None:
+        self.check(self.lib.hf_schedule_reset(self.handle), "hf_schedule_reset")
 
     def density_factor_device(self, d, max_rank: int):
         """``F`` ([n_ao, rank], a torch CUDA tensor) with ``F F^T = D`` for a

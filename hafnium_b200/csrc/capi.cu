@@ -28,6 +28,24 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// State of hf_exchange_scheduled between calls (device buffers of n x n
+// doubles each, allocated on first use).
+struct ScheduleState {
+    int phase = 0;           // 0: split-BF16 builds, 1: anchored increments
+    bool has_prev = false;   // a previous density is held
+    int64_t anchor_rank = 0;
+    double* prev = nullptr;      // the previous call's density
+    double* anchor_d = nullptr;  // D_a
+    double* anchor_k = nullptr;  // K64(D_a)
+    double* anchor_ft = nullptr; // F_a^T, [anchor_rank][n]
+    double* dens = nullptr;      // this call's density (host input staged here)
+    double* ft = nullptr;        // this call's factor, F^T [rank][n]
+    double* overlap = nullptr;   // S
+    double* work[10] = {};       // products and factors of the difference
+    double* scalar = nullptr;    // device reduction results
+    bool overlap_ready = false;
+};
+
 struct hf_ctx {
     int device = 0;
     cudaStream_t own = nullptr;
@@ -73,6 +91,7 @@ struct hf_ctx {
     // rows [row0, row1) of the fitted tensor held here (internal auxiliary order;
     // row1 < 0: all of them), for a tensor sharded over devices by auxiliary index
     int row0 = 0, row1 = -1;
+    ScheduleState sched;
     // bounded device waits of the split-BF16 exchange (hf_set_wait_limit)
     uint64_t wait_ns = 2000000000ull;  // 2 s: far above any legitimate wait there
     int stall_next = 0;                // the next split-BF16 build runs the stall self-test
@@ -134,6 +153,15 @@ template <class T>
 void release(T*& p) {
     if (p) cudaFree((void*)p);
     p = nullptr;
+}
+
+// Free hf_exchange_scheduled's buffers and forget its state.
+void schedule_release(hf_ctx* ctx) {
+    ScheduleState& st = ctx->sched;
+    for (double** q : {&st.prev, &st.anchor_d, &st.anchor_k, &st.anchor_ft, &st.dens, &st.ft, &st.overlap, &st.scalar})
+        release(*q);
+    for (auto& q : st.work) release(q);
+    st = ScheduleState{};
 }
 
 // The Boys-function Taylor grid (boys_grid_host) on each device, uploaded once
@@ -395,6 +423,148 @@ int check_async(hf_ctx* ctx, const char* what) {
     return HF_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Kernels of hf_exchange_scheduled (small, memory-bound helpers).
+
+// max |a - b| (b may be null: max |a|) into *out, which starts at 0: the bits of
+// non-negative doubles order as unsigned integers, so atomicMax on them is a max.
+__global__ void k_maxabs_diff(const double* __restrict__ a, const double* __restrict__ b, int64_t count,
+                              unsigned long long* out) {
+    double m = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(a[i] - (b ? b[i] : 0.0)));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double wm[32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x + 31) / 32 ? wm[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// max |Y - I| of an r x r matrix into *out (starting at 0).
+__global__ void k_maxabs_minus_eye(const double* __restrict__ y, int64_t r, unsigned long long* out) {
+    double m = 0.0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < r * r; e += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(y[e] - ((e / r == e % r) ? 1.0 : 0.0)));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double wm[32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x + 31) / 32 ? wm[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// dst[c][r] = src[r][c] for a rows x cols row-major src.
+__global__ void k_transpose_plain(const double* __restrict__ src, int64_t rows, int64_t cols, double* __restrict__ dst) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= rows * cols) return;
+    const int64_t c = e / rows, r = e % rows;  // dst element (c, r), written in order
+    dst[e] = src[r * cols + c];
+}
+
+// Z = 3 I - Y (r x r).
+__global__ void k_three_minus(const double* __restrict__ y, int64_t r, double* __restrict__ z) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= r * r) return;
+    z[e] = ((e / r == e % r) ? 3.0 : 0.0) - y[e];
+}
+
+// Rows k of A = F + G and B = F - G ([r][n] each) and their norms (one CTA per row).
+__global__ void k_sum_diff_norms(const double* __restrict__ f, const double* __restrict__ g, int64_t n,
+                                 double* __restrict__ a, double* __restrict__ b, double* __restrict__ na,
+                                 double* __restrict__ nb) {
+    const int64_t row = blockIdx.x;
+    double sa = 0.0, sb = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = f[row * n + i], y = g[row * n + i];
+        const double s = x + y, d = x - y;
+        a[row * n + i] = s;
+        b[row * n + i] = d;
+        sa += s * s;
+        sb += d * d;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sa += __shfl_xor_sync(0xffffffffu, sa, o);
+        sb += __shfl_xor_sync(0xffffffffu, sb, o);
+    }
+    __shared__ double wa[32], wb[32];
+    if ((threadIdx.x & 31) == 0) {
+        wa[threadIdx.x >> 5] = sa;
+        wb[threadIdx.x >> 5] = sb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ta = 0.0, tb = 0.0;
+        for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) {
+            ta += wa[w];
+            tb += wb[w];
+        }
+        na[row] = sqrt(ta);
+        nb[row] = sqrt(tb);
+    }
+}
+
+// V+-[i][k] = (alpha_k A[k][i] +- B[k][i] / alpha_k) / 2, alpha_k = sqrt(|b_k| / |a_k|):
+// the factors of (A^T B + B^T A) / 2 = V+ V+^T - V- V-^T, written [n][r].
+__global__ void k_difference_factors(const double* __restrict__ a, const double* __restrict__ b,
+                                     const double* __restrict__ na, const double* __restrict__ nb, int64_t r,
+                                     int64_t n, double* __restrict__ vp, double* __restrict__ vm) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * r) return;
+    const int64_t i = e / r, k = e % r;
+    const double alpha = sqrt(fmax(nb[k], 1e-300) / fmax(na[k], 1e-300));
+    const double x = alpha * a[k * n + i], y = b[k * n + i] / alpha;
+    vp[e] = 0.5 * (x + y);
+    vm[e] = 0.5 * (x - y);
+}
+
+// K = Ka + Kp - Km.
+__global__ void k_combine(const double* __restrict__ ka, const double* __restrict__ kp, const double* __restrict__ km,
+                          int64_t count, double* __restrict__ k) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e < count) k[e] = ka[e] + kp[e] - km[e];
+}
+
+unsigned blocks_for(int64_t count, int threads = 256) { return (unsigned)((count + threads - 1) / threads); }
+
+// max |a - b| (or max |Y - I| when eye) on the context's stream, read back.
+int device_maxabs(hf_ctx* ctx, const double* a, const double* b, int64_t count, bool eye, int64_t r, double* out) {
+    unsigned long long* slot = reinterpret_cast<unsigned long long*>(ctx->sched.scalar);
+    HF_CU(cudaMemsetAsync(slot, 0, sizeof(unsigned long long), ctx->stream));
+    if (eye) k_maxabs_minus_eye<<<std::min<unsigned>(1024, blocks_for(r * r)), 256, 0, ctx->stream>>>(a, r, slot);
+    else k_maxabs_diff<<<std::min<unsigned>(4 * 148, blocks_for(count)), 256, 0, ctx->stream>>>(a, b, count, slot);
+    unsigned long long bits = 0;
+    HF_CU(cudaMemcpyAsync(&bits, slot, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
+    HF_CU(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(out, &bits, sizeof(double));
+    return HF_OK;
+}
+
+// C (M x N, row-major, ldc) = alpha A B^T with A M x K (lda) and B N x K (ldb), on the DMMA kernel.
+cudaError_t gemm_nt(hf_ctx* ctx, int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const double* B,
+                    int64_t ldb, double* C, int64_t ldc, double alpha) {
+    GemmArgs g{};
+    g.M = (int)M;
+    g.N = (int)N;
+    g.K = (int)K;
+    g.A = A;
+    g.lda = lda;
+    g.B = B;
+    g.ldb = ldb;
+    g.C = C;
+    g.ldc = ldc;
+    g.alpha = alpha;
+    g.beta = 0.0;
+    g.tile = 1;  // 64 x 64: these products are at most n x r x n
+    return dgemm_nt(g, 1, ctx->stream);
+}
 }  // namespace
 
 namespace hf {
@@ -476,6 +646,7 @@ int hf_ctx_destroy(hf_ctx* ctx) {
     big_release(ctx, ctx->d_bf16_b, ctx->bf16_alloc_bytes);
     big_release(ctx, ctx->d_tcwork, ctx->tcwork_bytes);
     big_release(ctx, ctx->d_ctc, ctx->ctc_bytes);
+    schedule_release(ctx);
     release(ctx->d_info);
     release(ctx->d_scalar);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -543,6 +714,7 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
     ctx->built = false;
     ctx->row0 = 0;
     ctx->row1 = -1;
+    schedule_release(ctx);
     std::vector<double> exps, coefs;
     auto add = [&](const hf_shell_table* t, int64_t sh, int fn) {
         DevShell d{};
@@ -1074,6 +1246,140 @@ int hf_exchange_factored(hf_ctx* ctx, const double* C, int64_t ncols, const doub
     ctx->stats.exchange_rank = ncols;
     if (s == HF_OK) s = check_async(ctx, "hf_exchange_factored");
     return s;
+}
+
+int hf_schedule_reset(hf_ctx* ctx) {
+    if (!ctx) return HF_ERR_ARG;
+    ScheduleState& st = ctx->sched;
+    st.phase = 0;
+    st.has_prev = false;
+    st.anchor_rank = 0;
+    return HF_OK;
+}
+
+int hf_exchange_scheduled(hf_ctx* ctx, const double* D, double* K, int on_device, const hf_schedule* sc, int* kind) {
+    if (!ctx || !D || !K || !sc) return HF_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HF_ERR_STATE, "build the fitted tensor first");
+    if (sc->mode == HF_SCHEDULE_FP64) {
+        if (kind) *kind = HF_BUILD_FP64;
+        return hf_exchange(ctx, D, K, HF_PREC_FP64, on_device);
+    }
+    if (sc->mode != HF_SCHEDULE_MIXED) return fail(ctx, HF_ERR_ARG, "unknown schedule mode");
+    if (!(sc->anchor_change > 0.0) || !(sc->final_change > 0.0) || sc->final_change > sc->anchor_change)
+        return fail(ctx, HF_ERR_ARG, "the schedule needs 0 < final_change <= anchor_change");
+    cudaSetDevice(ctx->device);
+    const int64_t n = ctx->n;
+    const size_t nn = (size_t)n * n, bytes = sizeof(double) * nn;
+    ScheduleState& st = ctx->sched;
+    for (double** q : {&st.prev, &st.anchor_d, &st.anchor_k, &st.anchor_ft, &st.dens, &st.ft, &st.overlap})
+        if (!*q && alloc(ctx, (void**)q, bytes)) return HF_ERR_OOM;
+    for (auto& q : st.work)
+        if (!q && alloc(ctx, (void**)&q, bytes)) return HF_ERR_OOM;
+    if (!st.scalar && alloc(ctx, (void**)&st.scalar, sizeof(double) * (2 * (size_t)n + 8))) return HF_ERR_OOM;
+    int s;
+    if (!st.overlap_ready) {
+        if ((s = hf_one_electron(ctx, 0, nullptr, nullptr, 0, st.overlap, 1)) != HF_OK) return s;
+        st.overlap_ready = true;
+    }
+    const double* dD = D;
+    if (!on_device) {
+        HF_CU(cudaMemcpyAsync(st.dens, D, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        dD = st.dens;
+    }
+    // the largest element change from the previous call's density
+    double delta = INFINITY;
+    if (st.has_prev && (s = device_maxabs(ctx, dD, st.prev, (int64_t)nn, false, 0, &delta)) != HF_OK) return s;
+    HF_CU(cudaMemcpyAsync(st.prev, dD, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    st.has_prev = true;
+    if (delta >= sc->anchor_change) st.phase = 0;
+    // D ~= F F^T, F^T in st.ft ([rank][n])
+    int64_t rank = 0;
+    if ((s = hf_density_factor(ctx, dD, st.ft, n, &rank, 1)) != HF_OK) return s;
+    double* const* w = st.work;
+    double* kout = on_device ? K : w[9];
+    if (rank == 0) {  // D = 0: K = 0 exactly
+        HF_CU(cudaMemsetAsync(kout, 0, bytes, ctx->stream));
+        if (kind) *kind = HF_BUILD_FP64;
+        if (!on_device) HF_CU(cudaMemcpyAsync(K, kout, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        return check_async(ctx, "hf_exchange_scheduled");
+    }
+    const unsigned tb = blocks_for(rank * n);
+    auto build_from_factor = [&](int precision) -> int {
+        k_transpose_plain<<<tb, 256, 0, ctx->stream>>>(st.ft, rank, n, w[0]);  // F, [n][rank]
+        return hf_exchange_factored(ctx, w[0], rank, nullptr, kout, precision, 1);
+    };
+    auto anchor = [&]() -> int {
+        int r2 = build_from_factor(HF_PREC_FP64);
+        if (r2 != HF_OK) return r2;
+        HF_CU(cudaMemcpyAsync(st.anchor_d, dD, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        HF_CU(cudaMemcpyAsync(st.anchor_ft, st.ft, sizeof(double) * rank * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        HF_CU(cudaMemcpyAsync(st.anchor_k, kout, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        st.anchor_rank = rank;
+        st.phase = 1;
+        if (kind) *kind = HF_BUILD_ANCHOR;
+        return HF_OK;
+    };
+    // K64(D_a) + K16(V+) - K16(V-) for D - D_a = V+ V+^T - V- V-^T; an anchor when the
+    // rotation of the anchor's factor onto this one does not converge
+    auto increment = [&]() -> int {
+        const int64_t r = std::max(rank, st.anchor_rank);
+        double *fnt = w[1], *fat = w[2], *t1t = w[3], *x = w[4], *xt = w[5], *y = w[6], *z = w[7], *xn = w[8];
+        // the two factors' transposes, zero padded to r rows
+        HF_CU(cudaMemsetAsync(fnt, 0, sizeof(double) * r * n, ctx->stream));
+        HF_CU(cudaMemsetAsync(fat, 0, sizeof(double) * r * n, ctx->stream));
+        HF_CU(cudaMemcpyAsync(fnt, st.ft, sizeof(double) * rank * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        HF_CU(cudaMemcpyAsync(fat, st.anchor_ft, sizeof(double) * st.anchor_rank * n, cudaMemcpyDeviceToDevice,
+                              ctx->stream));
+        // M = F_a^T S F: T1^T = F^T S (S symmetric), then M = F_a^T (T1^T)^T
+        HF_CU(gemm_nt(ctx, r, n, n, fnt, n, st.overlap, n, t1t, n, 1.0));
+        HF_CU(gemm_nt(ctx, r, r, n, fat, n, t1t, n, x, r, 1.0));
+        // its orthogonal polar factor: X <- X (3 I - X^T X) / 2
+        const unsigned rb = blocks_for(r * r);
+        for (int it = 0; it < 8; ++it) {
+            k_transpose_plain<<<rb, 256, 0, ctx->stream>>>(x, r, r, xt);
+            HF_CU(gemm_nt(ctx, r, r, r, xt, r, xt, r, y, r, 1.0));  // X^T X
+            k_three_minus<<<rb, 256, 0, ctx->stream>>>(y, r, z);
+            HF_CU(gemm_nt(ctx, r, r, r, x, r, z, r, xn, r, 0.5));   // X Z / 2 (Z symmetric)
+            std::swap(x, xn);
+        }
+        k_transpose_plain<<<rb, 256, 0, ctx->stream>>>(x, r, r, xt);
+        HF_CU(gemm_nt(ctx, r, r, r, xt, r, xt, r, y, r, 1.0));
+        double orth = INFINITY;
+        int r2 = device_maxabs(ctx, y, nullptr, 0, true, r, &orth);
+        if (r2 != HF_OK) return r2;
+        if (!(orth < 1e-13)) return anchor();
+        // F_a X: with F_a = (F_a^T)^T in t1t ([n][r]), (F_a X)^T = X^T F_a^T -> [r][n]
+        k_transpose_plain<<<blocks_for(r * n), 256, 0, ctx->stream>>>(fat, r, n, t1t);
+        double* frt = y;  // [r][n]
+        HF_CU(gemm_nt(ctx, r, n, r, xt, r, t1t, r, frt, n, 1.0));
+        double* at = z;   // A^T = F^T + (F_a X)^T
+        double* bt = xt;  // B^T = F^T - (F_a X)^T
+        double* norms = st.scalar + 8;
+        k_sum_diff_norms<<<(unsigned)r, 256, 0, ctx->stream>>>(fnt, frt, n, at, bt, norms, norms + r);
+        double *vp = w[0], *vm = w[1];
+        k_difference_factors<<<blocks_for(n * r), 256, 0, ctx->stream>>>(at, bt, norms, norms + r, r, n, vp, vm);
+        double *kp = w[2], *km = w[3];
+        if ((r2 = hf_exchange_factored(ctx, vp, r, nullptr, kp, HF_PREC_BF16X3, 1)) != HF_OK) return r2;
+        if ((r2 = hf_exchange_factored(ctx, vm, r, nullptr, km, HF_PREC_BF16X3, 1)) != HF_OK) return r2;
+        k_combine<<<blocks_for((int64_t)nn), 256, 0, ctx->stream>>>(st.anchor_k, kp, km, (int64_t)nn, kout);
+        if (kind) *kind = HF_BUILD_INCREMENTAL;
+        return HF_OK;
+    };
+    if (st.phase == 0) {
+        if (delta < sc->anchor_change) {
+            s = anchor();
+        } else {
+            s = build_from_factor(HF_PREC_BF16X3);
+            if (s == HF_OK && kind) *kind = HF_BUILD_BF16;
+        }
+    } else {
+        double distance = 0.0;
+        if ((s = device_maxabs(ctx, dD, st.anchor_d, (int64_t)nn, false, 0, &distance)) != HF_OK) return s;
+        s = (delta < sc->final_change && distance > sc->final_change) ? anchor() : increment();
+    }
+    if (s != HF_OK) return s;
+    if (!on_device) HF_CU(cudaMemcpyAsync(K, kout, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_async(ctx, "hf_exchange_scheduled");
 }
 
 int hf_density_factor(hf_ctx* ctx, const double* D, double* F, int64_t max_rank, int64_t* rank, int on_device) {

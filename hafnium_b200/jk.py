@@ -163,6 +163,35 @@ class MixedExchangeSchedule:
         return k
 
 
+class LibraryExchangeSchedule:
+    """``MixedExchangeSchedule``'s decisions made inside the library
+    (``hf_exchange_scheduled``, include/hfjk.h): the same thresholds, the same
+    pivoted-Cholesky factors and polar rotation, computed by the library's own
+    kernels and DMMA products, so that a C host gets the schedule through the C
+    ABI. The drop-in's ``schedule="mixed"`` uses it; ``log`` records each build's
+    arithmetic."""
+
+    def __init__(self, context: _lib.Context, anchor_change: float = 1e-3, final_change: float = 1e-5) -> None:
+        self.context = context
+        self.anchor_change = anchor_change
+        self.final_change = final_change
+        self.log = []
+
+    def reset(self) -> None:
+        self.context.schedule_reset()
+        self.log = []
+
+    def exchange(self, d):
+        """K for the device density ``d`` (a torch CUDA tensor)."""
+        import torch
+
+        out = torch.empty_like(d)
+        kind = self.context.exchange_scheduled(
+            d, out, _lib.ScheduleC(_lib.SCHEDULE_MIXED, self.anchor_change, self.final_change))
+        self.log.append({"precision": kind})
+        return out
+
+
 class B200DensityFittedCoulombExchange:
     """J and K from the packed fitted tensor on one B200."""
 
@@ -170,9 +199,12 @@ class B200DensityFittedCoulombExchange:
         self.context = context
         self._n_ao, self._n_aux = context.dims()
         self.precision = precision
-        if schedule not in ("fp64", "mixed"):
-            raise InputError("the exchange schedule is 'fp64' or 'mixed'")
-        self.schedule = MixedExchangeSchedule(self) if schedule == "mixed" else None
+        if schedule not in ("fp64", "mixed", "mixed-host"):
+            raise InputError("the exchange schedule is 'fp64', 'mixed' or 'mixed-host'")
+        # "mixed": the schedule inside the library; "mixed-host": its host-side
+        # restatement (MixedExchangeSchedule), which the sharded builder also uses
+        self.schedule = (LibraryExchangeSchedule(context) if schedule == "mixed" else
+                         MixedExchangeSchedule(self) if schedule == "mixed-host" else None)
 
     @classmethod
     def from_tables(cls, orbital, auxiliary, *, device: int = 0, precision: int = _lib.PREC_FP64,

@@ -52,6 +52,27 @@ typedef enum hf_precision {
     HF_PREC_BF16X3 = 1     /* 3 split-BF16 products, FP32 accumulation (tcgen05) */
 } hf_precision;
 
+/* The mixed-precision exchange schedule behind hf_exchange_scheduled. */
+typedef enum hf_schedule_mode {
+    HF_SCHEDULE_FP64 = 0,  /* every build FP64 */
+    HF_SCHEDULE_MIXED = 1  /* split-BF16, FP64 anchor, anchored increments, late re-anchor */
+} hf_schedule_mode;
+
+typedef struct hf_schedule {
+    int mode;               /* hf_schedule_mode */
+    double anchor_change;   /* split-BF16 while max|D_n - D_(n-1)| >= this (1e-3) */
+    double final_change;    /* one more FP64 anchor once the change is below this while
+                               the anchor lies farther than it (1e-5) */
+} hf_schedule;
+
+/* What a scheduled build computed. */
+typedef enum hf_build_kind {
+    HF_BUILD_FP64 = 0,        /* FP64 (HF_SCHEDULE_FP64) */
+    HF_BUILD_BF16 = 1,        /* split-BF16 from the density's factor */
+    HF_BUILD_ANCHOR = 2,      /* FP64, kept as the anchor */
+    HF_BUILD_INCREMENTAL = 3  /* anchor + split-BF16 of the exactly factored difference */
+} hf_build_kind;
+
 typedef struct hf_stats {
     double ms_metric;       /* (P|Q) */
     double ms_factor;       /* Cholesky + inverse of the factor */
@@ -139,6 +160,26 @@ int hf_coulomb(hf_ctx* ctx, const double* density, double* coulomb, int on_devic
  * the same process. The call returns once J is complete: it waits for the
  * context's stream. */
 int hf_coulomb_static(hf_ctx* ctx, const double* density, double* coulomb);
+
+/* K for the density of one SCF iteration with the arithmetic chosen by the
+ * schedule from the sequence of densities the context has been given
+ * (hafnium/scf/coulomb_exchange.py:184-190 behind the reference driver's
+ * per-iteration and finishing calls, hafnium/scf/driver.py:198-205, 336):
+ * split-BF16 from the density's pivoted-Cholesky factor while the largest
+ * element change from the previous call is at least anchor_change; then an
+ * FP64 build kept as the anchor; then K64(D_a) + K16(V+) - K16(V-) with
+ * D - D_a = V+ V+^T - V- V-^T from the factors (the anchor's rotated onto the
+ * current one by the polar factor of F_a^T S F, a Newton-Schulz iteration of
+ * matrix products; when it does not converge the build re-anchors in FP64);
+ * once the change is below final_change while the anchor lies farther, one
+ * more FP64 anchor. A jump of the change back above anchor_change restarts the
+ * split-BF16 phase. *kind (may be NULL) receives hf_build_kind. The state is
+ * the context's: one SCF at a time per context; hf_schedule_reset clears it.
+ * HF_ERR_NUMERIC for an indefinite D. No reference counterpart (the reference
+ * computes every K in FP64). */
+int hf_exchange_scheduled(hf_ctx* ctx, const double* density, double* exchange, int on_device,
+                          const hf_schedule* schedule, int* kind);
+int hf_schedule_reset(hf_ctx* ctx);
 
 /* A factor of a symmetric positive semidefinite density, D ~= F^T F: F holds
  * *rank rows of n_ao (row-major [rank][n_ao], capacity max_rank rows) from a

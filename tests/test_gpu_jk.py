@@ -144,3 +144,41 @@ def test_row_shards_of_the_fitted_tensor_sum_to_the_whole(tag):
     assert sum(s.stats()["b_bytes"] for s in shards) == whole.stats()["b_bytes"]
     with pytest.raises(InputError, match="every row"):
         shards[1].orbital_tensor(c[:, :3], c[:, :3])
+
+
+def test_sharded_builder_over_a_one_rank_nccl_group():
+    """The sharded builder's collectives on device tensors through NCCL (a group of
+    one rank on this GPU): J and K of the whole tensor, FP64 and the mixed
+    schedule's first (split-BF16) build."""
+    import os
+
+    import torch
+    import torch.distributed as dist
+
+    from hafnium_b200.sharded import ShardedCoulombExchange, shard_rows
+
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", str(29650 + os.getpid() % 300))
+    created = not dist.is_initialized()
+    if created:
+        dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        mol = molecule("h2o4_s1")
+        orb, aux = tables(mol)
+        whole = B200DensityFittedCoulombExchange.from_tables(orb, aux)
+        local = B200DensityFittedCoulombExchange.from_tables(orb, aux, rows=shard_rows(whole.n_aux, 1, 0))
+        sharded = ShardedCoulombExchange(local)
+        mixed = ShardedCoulombExchange(
+            B200DensityFittedCoulombExchange.from_tables(orb, aux, rows=shard_rows(whole.n_aux, 1, 0)),
+            schedule="mixed")
+        d, c = psd_density(whole.n_ao, 20, 6)
+        dt = torch.as_tensor(d, device="cuda")
+        np.testing.assert_allclose(sharded.coulomb(dt).cpu().numpy(), whole.coulomb(d), atol=JK_TOL, rtol=0)
+        np.testing.assert_allclose(sharded.exchange(dt).cpu().numpy(), whole.exchange(d), atol=JK_TOL, rtol=0)
+        k16 = mixed.exchange(d)  # host arrays in and out, the first build is split-BF16
+        k64 = whole.exchange(d)
+        assert mixed.schedule.log[-1]["precision"] == "bf16"
+        assert np.max(np.abs(k16 - k64)) <= 1e-4 * np.max(np.abs(k64))
+    finally:
+        if created:
+            dist.destroy_process_group()

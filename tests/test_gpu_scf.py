@@ -94,8 +94,9 @@ def test_mixed_schedule_at_tight_tolerances():
     assert np.max(np.abs(result.density.cpu().numpy() - ref["density"])) <= 1e-6
 
 
-@pytest.mark.parametrize("tag", ["h2o4_s1", "h2o8_s2", "h2o16_s0"])
-def test_reference_driver_with_the_mixed_builder_matches_reference(tag):
+@pytest.mark.parametrize("tag,schedule", [("h2o4_s1", "mixed"), ("h2o8_s2", "mixed"), ("h2o16_s0", "mixed"),
+                                          ("h2o8_s2", "mixed-host")])
+def test_reference_driver_with_the_mixed_builder_matches_reference(tag, schedule):
     """The reference's SCF loop (restated by the oracle: it calls nothing but
     coulomb(2 D) and exchange(D), with host NumPy arrays, and tests convergence
     on two consecutive energies) over the drop-in with schedule="mixed": the
@@ -109,7 +110,7 @@ def test_reference_driver_with_the_mixed_builder_matches_reference(tag):
     mol = molecule(tag)
     orb = ShellTable.build("cc-pvdz", mol.symbols, mol.positions)
     aux = ShellTable.build("def2-universal-jkfit", mol.symbols, mol.positions)
-    two_body = B200DensityFittedCoulombExchange.from_tables(orb, aux, schedule="mixed")
+    two_body = B200DensityFittedCoulombExchange.from_tables(orb, aux, schedule=schedule)
     s = dfrhf.overlap(orb)
     h = dfrhf.core_hamiltonian(orb, mol.nuclear_charges, mol.positions)
     guess = dfrhf.atomic_density_guess(orb, mol.symbols, {"O": 8.0, "H": 1.0})
@@ -169,3 +170,48 @@ def test_mixed_schedule_matches_plain_fp64_at_an_odd_padding():
     assert {"bf16", "incremental", "fp64"} <= {h.precision for h in mixed.history}
     assert abs(mixed.energy - plain.energy) <= 1e-8
     assert float((mixed.density - plain.density).abs().max()) <= 1e-6
+
+
+def test_library_and_host_schedules_agree():
+    """hf_exchange_scheduled (the schedule inside the library, for C hosts) and its
+    host-side restatement take the same decisions on the densities of an SCF and
+    give the same K to far below the split-BF16 error."""
+    import torch
+
+    from hafnium_b200 import _lib
+    from hafnium_b200.basis import ShellTable
+    from hafnium_b200.errors import InputError
+    from hafnium_b200.jk import B200DensityFittedCoulombExchange
+    from hafnium_b200.scf import atomic_density_guess
+
+    mol = molecule("h2o8_s2")
+    ham = DeviceHamiltonian.build(mol, "cc-pvdz", "def2-universal-jkfit")
+    seen = []
+
+    class Recorder:
+        """The drop-in's protocol, recording every density it is given."""
+
+        def __init__(self, inner):
+            self.inner, self.n_ao = inner, inner.n_ao
+
+        def coulomb(self, d):
+            return self.inner.coulomb(d)
+
+        def exchange(self, d):
+            seen.append(d.clone())
+            return self.inner.exchange(d)
+
+    ham.two_body = Recorder(ham.two_body)
+    solve_rhf(ham, guess=atomic_density_guess(mol, "cc-pvdz"), protocol=True)
+    orb = ShellTable.build("cc-pvdz", mol.symbols, mol.positions)
+    aux = ShellTable.build("def2-universal-jkfit", mol.symbols, mol.positions)
+    library = B200DensityFittedCoulombExchange.from_tables(orb, aux, schedule="mixed")
+    host = B200DensityFittedCoulombExchange.from_tables(orb, aux, schedule="mixed-host")
+    for d in seen:
+        k_lib, k_host = library.exchange(d), host.exchange(d)
+        assert float((k_lib - k_host).abs().max()) <= 1e-9 * float(k_host.abs().max())
+    kinds = [e["precision"] for e in library.schedule.log]
+    assert kinds == [e["precision"] for e in host.schedule.log]
+    assert kinds[0] == "bf16" and "anchor" in kinds and "incremental" in kinds
+    with pytest.raises(InputError, match="final_change"):
+        library.context.exchange_scheduled(seen[0], torch.empty_like(seen[0]), _lib.ScheduleC(_lib.SCHEDULE_MIXED, 1e-5, 1e-3))
