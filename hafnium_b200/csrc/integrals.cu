@@ -543,8 +543,12 @@ __global__ void __launch_bounds__(128) k_one_electron(const int2* __restrict__ t
     constexpr int KA = kMaxOrbContr[LA], KB = kMaxOrbContr[LB];
     constexpr int XB = (KIND == 1) ? 2 : 0;
     constexpr int LAB = LA + LB;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntasks) return;
+    // the attraction spreads its sum over the nuclei across the 32 lanes of a warp
+    // (one warp per shell pair; small molecules otherwise leave most SMs idle)
+    constexpr int LANES = (KIND == 2) ? 32 : 1;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = gt / LANES, lane = gt % LANES;
+    if (t >= ntasks) return;  // a whole warp at a time when LANES = 32
     const int2 task = tasks[t];
     const DevShell A = orb[task.x];
     const DevShell B = orb[task.y];
@@ -569,13 +573,19 @@ __global__ void __launch_bounds__(128) k_one_electron(const int2* __restrict__ t
                 double Rs[ntet(LAB)];
 #pragma unroll
                 for (int h = 0; h < ntet(LAB); ++h) Rs[h] = 0.0;
-                for (int c = 0; c < natoms; ++c) {
+                for (int c = lane; c < natoms; c += LANES) {
                     double R[ntet(LAB)];
                     hermite_r<LAB>(p, px - positions[3 * c], py - positions[3 * c + 1], pz - positions[3 * c + 2],
                                    btable, R);
                     const double z = charges[c];
 #pragma unroll
                     for (int h = 0; h < ntet(LAB); ++h) Rs[h] -= z * R[h];
+                }
+                if constexpr (LANES > 1) {
+#pragma unroll
+                    for (int h = 0; h < ntet(LAB); ++h)
+#pragma unroll
+                        for (int o = LANES / 2; o > 0; o >>= 1) Rs[h] += __shfl_xor_sync(0xffffffffu, Rs[h], o);
                 }
                 const double pref = 2.0 * kPi / p;
 #pragma unroll
@@ -640,6 +650,7 @@ __global__ void __launch_bounds__(128) k_one_electron(const int2* __restrict__ t
                         }
                 }
         }
+    if (lane != 0) return;
 #pragma unroll
     for (int ka = 0; ka < KA; ++ka)
 #pragma unroll
@@ -658,8 +669,9 @@ static cudaError_t one_electron_one(const int2* tasks, int ntasks, const DevShel
                                     const double* coefs, const double* charges, const double* positions, int natoms,
                                     const double* btable, double* out, int64_t n, cudaStream_t stream) {
     if (ntasks == 0) return cudaSuccess;
-    k_one_electron<LA, LB, KIND><<<(ntasks + 127) / 128, 128, 0, stream>>>(tasks, ntasks, orb, exps, coefs, charges,
-                                                                          positions, natoms, btable, out, n);
+    const int64_t threads = (int64_t)ntasks * (KIND == 2 ? 32 : 1);
+    k_one_electron<LA, LB, KIND><<<(unsigned)((threads + 127) / 128), 128, 0, stream>>>(
+        tasks, ntasks, orb, exps, coefs, charges, positions, natoms, btable, out, n);
     return cudaGetLastError();
 }
 
