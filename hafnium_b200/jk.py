@@ -302,7 +302,14 @@ class B200DensityFittedCoulombExchange:
         dev = torch.device("cuda", self.context.device)
         d = density if on_device else torch.as_tensor(np.asarray(density, dtype=np.float64))
         d = d.to(dev, torch.float64).contiguous()
-        k = self.schedule.exchange(d)
+        try:
+            k = self.schedule.exchange(d)
+        except InputError as error:
+            # an indefinite density (never one of the SCF's) has no factor: FP64 through
+            # a signed factor, as the unscheduled exchange does
+            if "semidefinite" not in str(error):
+                raise
+            return self._exchange_signed(density, on_device)
         return k if on_device else k.cpu().numpy()
 
     def _exchange_signed(self, density, on_device: bool):

@@ -215,3 +215,22 @@ def test_library_and_host_schedules_agree():
     assert kinds[0] == "bf16" and "anchor" in kinds and "incremental" in kinds
     with pytest.raises(InputError, match="final_change"):
         library.context.exchange_scheduled(seen[0], torch.empty_like(seen[0]), _lib.ScheduleC(_lib.SCHEDULE_MIXED, 1e-5, 1e-3))
+
+
+def test_scheduled_exchange_of_an_indefinite_density_is_fp64():
+    """The protocol allows any symmetric density; one without a factor (never an
+    SCF's) goes through the signed FP64 path, with every schedule."""
+    from oracle import dfrhf
+    from tests.helpers import tables
+
+    mol = molecule("h2o2_s0")
+    orb, aux = tables(mol)
+    b = dfrhf.df_tensor(dfrhf.metric(aux), dfrhf.three_center(aux, orb))
+    rng = np.random.default_rng(9)
+    c = rng.normal(size=(orb.n_functions, 6))
+    d = c[:, :3] @ c[:, :3].T - c[:, 3:] @ c[:, 3:].T
+    from hafnium_b200.jk import B200DensityFittedCoulombExchange
+
+    for schedule in ("fp64", "mixed", "mixed-host"):
+        two_body = B200DensityFittedCoulombExchange.from_tables(orb, aux, schedule=schedule)
+        np.testing.assert_allclose(two_body.exchange(d), dfrhf.exchange(b, d), atol=1e-10, rtol=0)
