@@ -376,6 +376,32 @@ __device__ int pair_prologue(const DevShell& A, const DevShell& B, const double*
     return nk;
 }
 
+// Shapes of one (P|mu nu) class. The threads of an auxiliary shell (one per
+// m_P) share each primitive triple's R table: per round, TPR of them each
+// evaluate the Boys function and R table of one triple into shared memory, and
+// after a barrier every thread contracts all TPR tables with its own m_P row of
+// the Cartesian-to-spherical matrix. TPR is NSP unless the tables would pass
+// kRTableBytes (the high classes, whose tables hold up to 165 entries).
+constexpr int kRTableBytes = 48 * 1024;
+template <int LA, int LB, int LP>
+struct ThreeCenterShape {
+    static constexpr int L = LA + LB + LP;
+    static constexpr int NCP = ncart(LP), NSP = nsph(LP), SPB = 128 / NSP;
+    static constexpr int NH = ntet(LA + LB);
+    static constexpr int NR = ntet(L);
+    // the table and its prefactor, padded to an odd count of doubles so that
+    // rows of consecutive threads fall in different banks
+    static constexpr int RS = (NR + 1) | 1;
+    static constexpr int FIT = kRTableBytes / (SPB * RS * 8);
+    static constexpr int TPR = FIT < 1 ? 1 : (FIT > NSP ? NSP : FIT);
+    static constexpr int R_DOUBLES = SPB * TPR * RS;
+};
+
+// One CTA per orbital shell pair of class (LA <= LB) and a slab of SPB auxiliary
+// shells of class LP; thread (slot, m_P) accumulates the pair's NSAB x KK block
+// of (P m_P | mu nu) for the slot's shell. The pair's primitive data and
+// spherical Hermite coefficients sit in shared memory (broadcast reads), so do
+// the round's R tables (rows of RS doubles, read by the slot's threads).
 template <int LA, int LB, int LP>
 __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict__ tasks,
                                                       const DevShell* __restrict__ orb,
@@ -384,27 +410,58 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
                                                       const double* __restrict__ coefs,
                                                       const int* __restrict__ alist, int nalist,
                                                       const double* __restrict__ btable, ChunkDesc chunk,
-                                                      double* __restrict__ T) {
+                                                      int r_offset, double* __restrict__ T) {
     using PL = PairLayout<LA, LB>;
-    constexpr int L = LA + LB + LP;
-    constexpr int LAB = LA + LB;
-    constexpr int NCP = ncart(LP), NSP = nsph(LP);
-    constexpr int SPB = 128 / NSP;  // aux shells per CTA
+    using SH = ThreeCenterShape<LA, LB, LP>;
+    constexpr int L = SH::L, NCP = SH::NCP, NSP = SH::NSP, SPB = SH::SPB, NH = SH::NH, TPR = SH::TPR;
+    constexpr int RS = SH::RS, NR = SH::NR;
     extern __shared__ double smem[];
     __shared__ int s_pos[2 * kMaxPrimPairs + 1];
+    __shared__ int s_idx[NCP * NH];      // tet(h + c) for Cartesian c of l_P, Hermite h of the pair
+    __shared__ int s_nzc[NSP * NCP];     // per m_P: the Cartesian components with a nonzero weight
+    __shared__ double s_nzw[NSP * NCP];  // ... and the weights
+    __shared__ int s_nnz[NSP];
+    __shared__ int s_tp[SPB * TPR];      // primitive pair of each table of the round, -1 past the end
+    __shared__ int s_rounds;
+    double* sR = smem + r_offset;
+
+    for (int e = threadIdx.x; e < NCP * NH; e += blockDim.x) {
+        const int c = e / NH, h = e - c * NH;
+        s_idx[e] = tet(c_tet_t[h] + c_cart[LP][c][0], c_tet_u[h] + c_cart[LP][c][1], c_tet_v[h] + c_cart[LP][c][2]);
+    }
+    if (threadIdx.x < NSP) {
+        int k = 0;
+        for (int c = 0; c < NCP; ++c) {
+            const double w = c_c2s[c2s_offset(LP) + threadIdx.x * NCP + c];
+            if (w != 0.0) {
+                s_nzc[threadIdx.x * NCP + k] = c;
+                s_nzw[threadIdx.x * NCP + k] = w;
+                ++k;
+            }
+        }
+        s_nnz[threadIdx.x] = k;
+    }
+    if (threadIdx.x == 0) s_rounds = 0;
+
     const PairTask task = tasks[blockIdx.x];
     const DevShell A = orb[task.swap ? task.second : task.first];
     const DevShell B = orb[task.swap ? task.first : task.second];
-    const int npp = pair_prologue<LA, LB>(A, B, exps, coefs, smem, s_pos);
-    if (npp == 0) return;  // the chunk was zeroed; nothing survives screening
+    const int npp = pair_prologue<LA, LB>(A, B, exps, coefs, smem, s_pos);  // ends with a barrier
+    if (npp == 0) return;  // the same for the whole CTA; the chunk was zeroed
 
-    const int slot = threadIdx.x / NSP, mp = threadIdx.x % NSP;
+    const int slot = threadIdx.x / NSP, mp = threadIdx.x - slot * NSP;
     const int ia = blockIdx.y * SPB + slot;
-    if (slot >= SPB || ia >= nalist) return;
-    const DevShell P = aux[alist[ia]];
-    double crow[NCP];
-#pragma unroll
-    for (int c = 0; c < NCP; ++c) crow[c] = c_c2s[c2s_offset(LP) + mp * NCP + c];
+    const bool active = slot < SPB && ia < nalist;
+    DevShell P{};
+    int ntrip = 0;
+    if (active) {
+        P = aux[alist[ia]];
+        ntrip = P.nprim * npp;
+        if (mp == 0) atomicMax(&s_rounds, (ntrip + TPR - 1) / TPR);
+    }
+    __syncthreads();
+    const int rounds = s_rounds;
+    const int nnz = s_nnz[mp < NSP ? mp : 0];
 
     double acc[PL::KK][PL::NSAB];
 #pragma unroll
@@ -412,44 +469,74 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
 #pragma unroll
         for (int m = 0; m < PL::NSAB; ++m) acc[k][m] = 0.0;
 
-    for (int i = 0; i < P.nprim; ++i) {
-        const double q = exps[P.prim + i];
-        const double inv_q = 1.0 / q;
-        double cq = coefs[P.coef + i] * pow(2.0 * q, -(double)LP);
-        if (LP & 1) cq = -cq;
-        cq *= kTwoPi52 * inv_q;
-        for (int pp = 0; pp < npp; ++pp) {
-            const double* s = smem + pp * PL::STRIDE;
-            const double p = s[0];
-            // one division per primitive triple: 1/(p+q) gives both the reduced
-            // exponent and the prefactor 2 pi^(5/2) / (p q sqrt(p+q))
-            const double inv_pq = 1.0 / (p + q);
-            const double alpha = p * q * inv_pq;
-            double R[ntet(L)];
-            hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, R);
-            double G[ntet(LAB)];
-#pragma unroll 1
-            for (int h = 0; h < ntet(LAB); ++h) {
-                const int tu = c_tet_t[h], uu = c_tet_u[h], vu = c_tet_v[h];
-                double g = 0.0;
-#pragma unroll 1
-                for (int c = 0; c < NCP; ++c)
-                    g += crow[c] * R[tet(tu + c_cart[LP][c][0], uu + c_cart[LP][c][1], vu + c_cart[LP][c][2])];
-                G[h] = g;
+    for (int r = 0; r < rounds; ++r) {
+        if (active && mp < TPR) {
+            const int t = r * TPR + mp;
+            int pp = -1;
+            if (t < ntrip) {
+                const int i = t / npp;
+                pp = t - i * npp;
+                const double q = exps[P.prim + i];
+                const double inv_q = 1.0 / q;
+                // c_P (2q)^-l_P (-1)^l_P 2 pi^(5/2) / q
+                double cq = coefs[P.coef + i] * kTwoPi52 * inv_q;
+                const double h2q = 0.5 * inv_q;
+#pragma unroll
+                for (int k = 0; k < LP; ++k) cq *= h2q;
+                if (LP & 1) cq = -cq;
+                const double* s = smem + pp * PL::STRIDE;
+                const double p = s[0];
+                // one division per primitive triple: 1/(p+q) gives both the reduced
+                // exponent and the prefactor 2 pi^(5/2) / (p q sqrt(p+q))
+                const double inv_pq = 1.0 / (p + q);
+                const double alpha = p * q * inv_pq;
+                double* row = sR + (slot * TPR + mp) * RS;
+                if constexpr (L <= 4) {
+                    double R[NR];
+                    hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, R);
+#pragma unroll
+                    for (int e = 0; e < NR; ++e) row[e] = R[e];
+                } else {
+                    hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, row);
+                }
+                row[NR] = s[4] * sqrt(inv_pq) * cq;
             }
-            const double pref = s[4] * sqrt(inv_pq) * cq;
-            const double* et = s + PL::ET;
-#pragma unroll
-            for (int m = 0; m < PL::NSAB; ++m) {
-                double val = 0.0;
+            s_tp[slot * TPR + mp] = pp;
+        }
+        if constexpr (NSP > 1) __syncthreads();
+        if (active) {
 #pragma unroll 1
-                for (int h = 0; h < PL::NH; ++h) val += et[m * PL::NH + h] * G[h];
-                val *= pref;
+            for (int j = 0; j < TPR; ++j) {
+                const int pp = s_tp[slot * TPR + j];
+                if (pp < 0) break;
+                const double* row = sR + (slot * TPR + j) * RS;
+                double G[NH];
 #pragma unroll
-                for (int k = 0; k < PL::KK; ++k) acc[k][m] += s[PL::CC + k] * val;
+                for (int h = 0; h < NH; ++h) G[h] = 0.0;
+#pragma unroll 1
+                for (int k = 0; k < nnz; ++k) {
+                    const int* ix = s_idx + s_nzc[mp * NCP + k] * NH;
+                    const double w = s_nzw[mp * NCP + k];
+#pragma unroll
+                    for (int h = 0; h < NH; ++h) G[h] += w * row[ix[h]];
+                }
+                const double pref = row[NR];
+                const double* s = smem + pp * PL::STRIDE;
+                const double* et = s + PL::ET;
+#pragma unroll
+                for (int m = 0; m < PL::NSAB; ++m) {
+                    double val = 0.0;
+#pragma unroll
+                    for (int h = 0; h < NH; ++h) val += et[m * NH + h] * G[h];
+                    val *= pref;
+#pragma unroll
+                    for (int k = 0; k < PL::KK; ++k) acc[k][m] += s[PL::CC + k] * val;
+                }
             }
         }
+        if constexpr (NSP > 1) __syncthreads();
     }
+    if (!active) return;
 
     // Scatter into the chunk: element (mu, nu) in AO order, both orders where the
     // tile is on or above the diagonal and its row belongs to this chunk.
@@ -493,18 +580,19 @@ static cudaError_t three_center_one(const PairTask* tasks, int ntasks, int max_n
                                     const int* alist, int nalist, const double* btable, ChunkDesc chunk,
                                     double* T, cudaStream_t stream) {
     if (ntasks == 0 || nalist == 0) return cudaSuccess;
-    constexpr int SPB = 128 / nsph(LP);
-    const size_t smem = sizeof(double) * (size_t)max_npp * PairLayout<LA, LB>::STRIDE;
-    // the attribute covers the dynamic part; the static pair list counts against
+    using SH = ThreeCenterShape<LA, LB, LP>;
+    const int r_offset = max_npp * PairLayout<LA, LB>::STRIDE;
+    const size_t smem = sizeof(double) * ((size_t)r_offset + SH::R_DOUBLES);
+    // the attribute covers the dynamic part; the static tables count against
     // the 48 KB default too
     if (smem > 40 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_three_center<LA, LB, LP>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    dim3 grid(ntasks, (nalist + SPB - 1) / SPB);
+    dim3 grid(ntasks, (nalist + SH::SPB - 1) / SH::SPB);
     k_three_center<LA, LB, LP><<<grid, 128, smem, stream>>>(tasks, orb, aux, exps, coefs, alist, nalist, btable,
-                                                            chunk, T);
+                                                            chunk, r_offset, T);
     return cudaGetLastError();
 }
 
