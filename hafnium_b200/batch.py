@@ -30,7 +30,8 @@ from hafnium_b200 import _lib
 from hafnium_b200.basis import ShellTable
 from hafnium_b200.errors import BackendError, ConvergenceError, InputError
 
-TILE_SHAPES = ((128, 64), (64, 64), (64, 32), (32, 32), (128, 128))
+# CTA tiles of hf_dgemm_nt: 0-4 with 3 stages of 16-wide k slices, 5 with 2 stages of 32
+TILE_SHAPES = ((128, 64), (64, 64), (64, 32), (32, 32), (128, 128), (64, 64))
 STATE_NAMES = {0: "iterating", 1: "finishing", 2: "converged", 3: "not_converged", 4: "purification_failed"}
 
 
@@ -296,7 +297,7 @@ BATCH_FIXED_BYTES = 2 << 30  # the K chunk buffer of one batch
 def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-universal-jkfit", *, device: int = 0,
                 options: BatchOptions | None = None, tuner: TileTuner | None = None,
                 memory_fraction: float = 0.6, max_batch: int = 256, keep_densities: bool = False,
-                setup_threads: int = 16, retry_failed: bool = True) -> BatchResult:
+                setup_threads: int = 32, retry_failed: bool = True) -> BatchResult:
     """Converge every molecule's restricted DF-RHF; energies (and, with
     ``keep_densities``, the converged per-spin densities) in input order."""
     torch = _torch()

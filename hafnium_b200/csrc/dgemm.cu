@@ -1,8 +1,10 @@
 // FP64 DMMA GEMM (see dgemm.cuh for the contract).
 //
-// Warps of 32 x 32 output (2 x 4 mma.sync.m16n8k8 FP64 tiles), a 3-stage
-// cp.async pipeline from global memory into shared tiles stored row-major with
-// a 20-double row pitch (conflict-free fragment loads), BK = 16. Operands are
+// Warps of 32 x 32 output (2 x 4 mma.sync.m16n8k8 FP64 tiles), a cp.async
+// pipeline from global memory into shared tiles stored row-major with a row
+// pitch of BK + 4 doubles (conflict-free fragment loads): 3 stages of BK = 16,
+// or for the 64 x 64 tile of the large products 2 stages of BK = 32 (half the
+// barriers per k; 34.0 against 33.5 TF/s on a 7232 x 16384 x 7232 product). Operands are
 // K-contiguous rows (A[m][k], B[n][k]); copies are 8 bytes so any row stride and
 // offset is legal, and out-of-range elements are zero-filled.
 #include <mutex>
@@ -12,7 +14,6 @@
 namespace hf {
 
 namespace {
-constexpr int BK = 16, LD = BK + 4, STAGES = 3;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -45,16 +46,17 @@ __host__ __device__ constexpr int threads_of() {
     return (BM / 32) * (BN / 32) * 32;
 }
 
-template <int BM, int BN>
+template <int BM, int BN, int BK, int STAGES>
 __host__ __device__ constexpr int smem_of() {
-    return STAGES * (BM + BN) * LD * (int)sizeof(double);
+    return STAGES * (BM + BN) * (BK + 4) * (int)sizeof(double);
 }
 
 // VEC: operands 16-byte aligned with even row strides, copied two doubles at a time.
-template <int BM, int BN, bool VEC>
+template <int BM, int BN, int BK, int STAGES, bool VEC>
 __global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN>()) < 1 ? 1 : 512 / threads_of<BM, BN>())
     k_dgemm_nt(GemmArgs g) {
     constexpr int THREADS = threads_of<BM, BN>();
+    constexpr int LD = BK + 4;
     constexpr int WARPS_N = BN / 32;
     const int zz = blockIdx.z;
     int z = zz, sp = 0;
@@ -187,13 +189,13 @@ __global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN
             }
 }
 
-template <int BM, int BN>
+template <int BM, int BN, int BK = 16, int STAGES = 3>
 cudaError_t configure_one() {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_dgemm_nt<BM, BN, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_of<BM, BN>());
+    cudaError_t e = cudaFuncSetAttribute(k_dgemm_nt<BM, BN, BK, STAGES, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_of<BM, BN, BK, STAGES>());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_dgemm_nt<BM, BN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                smem_of<BM, BN>());
+    return cudaFuncSetAttribute(k_dgemm_nt<BM, BN, BK, STAGES, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem_of<BM, BN, BK, STAGES>());
 }
 
 bool aligned16(const GemmArgs& g) {
@@ -203,13 +205,14 @@ bool aligned16(const GemmArgs& g) {
     return ok(g.A, g.lda, g.strideA) && ok(g.B, g.ldb, g.strideB);
 }
 
-template <int BM, int BN>
+template <int BM, int BN, int BK = 16, int STAGES = 3>
 cudaError_t launch(const GemmArgs& g, int batch, cudaStream_t stream) {
     dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, batch * (g.splits > 1 ? g.splits : 1));
+    constexpr int smem = smem_of<BM, BN, BK, STAGES>();
     if (aligned16(g))
-        k_dgemm_nt<BM, BN, true><<<grid, threads_of<BM, BN>(), smem_of<BM, BN>(), stream>>>(g);
+        k_dgemm_nt<BM, BN, BK, STAGES, true><<<grid, threads_of<BM, BN>(), smem, stream>>>(g);
     else
-        k_dgemm_nt<BM, BN, false><<<grid, threads_of<BM, BN>(), smem_of<BM, BN>(), stream>>>(g);
+        k_dgemm_nt<BM, BN, BK, STAGES, false><<<grid, threads_of<BM, BN>(), smem, stream>>>(g);
     return cudaGetLastError();
 }
 
@@ -230,6 +233,7 @@ cudaError_t dgemm_configure() {
     if ((e = configure_one<64, 32>()) != cudaSuccess) return e;
     if ((e = configure_one<32, 32>()) != cudaSuccess) return e;
     if ((e = configure_one<128, 128>()) != cudaSuccess) return e;
+    if ((e = configure_one<64, 64, 32, 2>()) != cudaSuccess) return e;
     g_configured[dev] = true;
     return cudaSuccess;
 }
@@ -245,6 +249,7 @@ cudaError_t dgemm_nt(const GemmArgs& g, int batch, cudaStream_t stream) {
         case 2: return launch<64, 32>(g, batch, stream);
         case 3: return launch<32, 32>(g, batch, stream);
         case 4: return launch<128, 128>(g, batch, stream);
+        case 5: return launch<64, 64, 32, 2>(g, batch, stream);
         default: return cudaErrorInvalidValue;
     }
 }

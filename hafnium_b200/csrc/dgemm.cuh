@@ -2,9 +2,11 @@
 //
 // Both operands are K-contiguous ("NT"): A[m][k] with row stride lda, Bop[n][k]
 // with row stride ldb. DMMA mma.sync.m16n8k8.f64 (the FP64 tensor path;
-// tcgen05 has no FP64 kind), warps of 32x32 output, a 3-stage cp.async pipeline
-// of BK = 16 slices. The CTA tile is one of kTileShapes (selected by `tile`):
-// an autotuner picks the shape per problem size.
+// tcgen05 has no FP64 kind), warps of 32x32 output, a cp.async pipeline of
+// 3 stages of BK = 16 slices (tile 5: 2 stages of BK = 32). The CTA tile is one
+// of kTileShapes (selected by `tile`): an autotuner picks the shape per problem
+// size for the batched products; the fit of B and the FP64 exchange's SYRK use
+// tile 5.
 //
 // kmode restricts the k range per output tile (triangular operands):
 //   0: [0, K)   1: [n0, K) (Bop upper: Bop[n][k] = 0 for k < n)
@@ -48,8 +50,8 @@ struct GemmArgs {
 };
 
 // CTA tile shapes (BM x BN); warps = (BM / 32) * (BN / 32).
-constexpr int kTileCount = 5;
-constexpr int kTileShapes[kTileCount][2] = {{128, 64}, {64, 64}, {64, 32}, {32, 32}, {128, 128}};
+constexpr int kTileCount = 6;
+constexpr int kTileShapes[kTileCount][2] = {{128, 64}, {64, 64}, {64, 32}, {32, 32}, {128, 128}, {64, 64}};
 
 cudaError_t dgemm_nt(const GemmArgs& g, int batch, cudaStream_t stream);  // batch: matrices (not counting splits)
 

@@ -529,15 +529,19 @@ cudaError_t fitted_charges(const JkPlan& p, const double* D, double* d, double* 
     return cudaGetLastError();
 }
 
+// The SYRK's CTA tile: 64 x 64 with 2 stages of 32-wide k slices (tile 5).
+constexpr int kSyrkTile = 5;
+
 int syrk_splits(int64_t npad, int count) {
-    const int64_t mt = (npad + 127) / 128, nt = (npad + 63) / 64;
+    const int bm = kTileShapes[kSyrkTile][0], bn = kTileShapes[kSyrkTile][1];
+    const int64_t mt = (npad + bm - 1) / bm, nt = (npad + bn - 1) / bn;
     int64_t upper = 0;
     for (int64_t i = 0; i < mt; ++i)
         for (int64_t j = 0; j < nt; ++j)
-            if (i * 128 <= j * 64 + 63) ++upper;
+            if (i * bm <= j * bn + bn - 1) ++upper;
     const int64_t ctas = upper * std::max(1, count);
-    // enough CTAs for many waves: with two per SM the tail of a last partial wave
-    // cost up to 13 % of an FP64 K build at (H2O)64 (156 tiles x 2 splits = 312 CTAs)
+    // enough CTAs for many waves: the tail of a last partial wave cost up to 13 %
+    // of an FP64 K build at (H2O)64 with two splits
     const int64_t want = 12 * 148;
     int s = (int)std::min<int64_t>(32, (want + ctas - 1) / ctas);
     while (s > 1 && (int64_t)s * std::max(1, count) > 65535) --s;
@@ -585,6 +589,7 @@ cudaError_t exchange_build_fp64(const JkPlan& p, const double* Ct, int64_t strid
         g.beta = 1.0;
         g.kmode = 0;
         g.epi = 3;
+        g.tile = kSyrkTile;
         g.strideA = g.strideB = strideX;
         g.strideC = npad * npad;
         g.active = p.active;

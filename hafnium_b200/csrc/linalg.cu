@@ -235,6 +235,7 @@ cudaError_t apply_inverse_factor(const double* Linv, int n, int64_t ld, const do
     g.beta = 0.0;
     g.kmode = 2;
     g.epi = 0;
+    g.tile = 5;  // 64 x 64 with 2 stages of 32-wide k slices: the fastest tile for this product
     return dgemm_nt(g, 1, stream);
 }
 

@@ -57,7 +57,7 @@ typedef struct hf_batch_options {
     double gradient_tolerance; /* reference default 1e-6 */
     int purify_steps;          /* purification steps captured per iteration (1..128) */
     double purify_tolerance;   /* tr(P - P^2) below which one more step ends purification */
-    int gemm_tile;             /* DMMA tile shape for the n x n products (0..4, see hf_dgemm_nt) */
+    int gemm_tile;             /* DMMA tile shape for the n x n products (0..5, see hf_dgemm_nt) */
     int use_graph;             /* 1: one CUDA graph with a device-side loop; 0: host loop */
 } hf_batch_options;
 
@@ -98,8 +98,9 @@ int hf_batch_exchange(hf_batch* batch, const double* density, int64_t max_rank, 
 
 /* Strided-batched FP64 tensor-core GEMM, C = alpha A B^T + beta C, for the
  * tile autotuner: A [m][k] (lda), B [n][k] (ldb), C [m][n] (ldc), device
- * pointers advanced by the strides per batch; tile 0..4 selects the CTA tile
- * 128x64, 64x64, 64x32, 32x32, 128x128. */
+ * pointers advanced by the strides per batch; tile 0..5 selects the CTA tile
+ * 128x64, 64x64, 64x32, 32x32, 128x128 (3 stages of 16-wide k slices) or
+ * 64x64 with 2 stages of 32-wide k slices. */
 int hf_dgemm_nt(int64_t m, int64_t n, int64_t k, const double* a, int64_t lda, int64_t stride_a, const double* b,
                 int64_t ldb, int64_t stride_b, double* c, int64_t ldc, int64_t stride_c, double alpha, double beta,
                 int batch, int tile, void* stream);

@@ -34,7 +34,7 @@ def small_clusters():
     return mols, [_oracle(m) for m in mols]
 
 
-@pytest.mark.parametrize("tile", range(5))
+@pytest.mark.parametrize("tile", range(6))
 def test_dgemm_tiles_match_torch(tile):
     import torch
 
