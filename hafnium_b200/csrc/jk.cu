@@ -165,13 +165,16 @@ __global__ void k_symmetrize_upper(const double* __restrict__ Kp, int64_t ldk, i
     K[e] = mu <= nu ? Kp[mu * ldk + nu] : Kp[nu * ldk + mu];
 }
 
-// X[p][ql][i] = sum_r B_q[p][r] Ct[i][r] for q = q0 + ql: 128 x 64 tiles, 8 warps,
-// mma.sync.m16n8k8 (FP64), a 3-stage pipeline of 16-byte cp.async copies. The A
-// operand comes from the packed tiles: tile (Ip, J) when Ip <= J, else tile
-// (J, Ip) read in its own orientation and transposed by the fragment loads.
-constexpr int XBM = 128, XBN = 64, XBK = 16, XLD = XBK + 4, XST = 3, XTHREADS = 256;
+// X[p][ql][i] = sum_r B_q[p][r] Ct[i][r] for q = q0 + ql: 64 x 64 tiles, 4 warps,
+// mma.sync.m16n8k8 (FP64), a 2-stage pipeline of 32-wide k slices moved by
+// 16-byte cp.async copies (three CTAs per SM; 128 x 64 tiles with 3 stages of 16
+// were 4 % slower). The A operand comes from the packed tiles: tile (Ip, J) when
+// Ip <= J, else tile (J, Ip) read in its own orientation and transposed by the
+// fragment loads.
+constexpr int XBM = 64, XBN = 64, XBK = 32, XLD = XBK + 4, XST = 2, XTHREADS = 128;
 constexpr int XLDT = 64 + 4;  // pitch of a k-major half: conflict-free fragment loads
 static_assert(XBK * XLDT <= 64 * XLD, "a k-major half fits in the p-major half's space");
+static_assert(XBM % 64 == 0 && 64 % XBK == 0, "a k slice stays inside one packed tile");
 
 __device__ __forceinline__ uint32_t xsmem(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
@@ -194,7 +197,7 @@ __device__ __forceinline__ void xmma(double (&c)[4], const double (&a)[4], const
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-__global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* const* __restrict__ Btab,
+__global__ void __launch_bounds__(XTHREADS, 3) k_exchange_half(const double* const* __restrict__ Btab,
                                                              const double* __restrict__ B, int64_t ldb, int q0, int nt,
                                                              const double* __restrict__ Ct, int64_t ldc_t,
                                                              int64_t strideCt, int npad, double* __restrict__ X,
@@ -229,8 +232,9 @@ __global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* con
         double* as = As + stage * XBM * XLD;
         double* bs = Bs + stage * XBN * XLD;
         const int J = k0 >> 6, kin = k0 & 63;
+        constexpr int PIECES = 64 * XBK / 2;  // 16-byte pieces of a 64 x XBK half
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < XBM / 64; ++h) {
             const int p0 = m0 + 64 * h;
             const int Ip = p0 >> 6;
             double* ah = as + h * 64 * XLD;
@@ -238,10 +242,10 @@ __global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* con
             const bool below = Ip > J;
             const double* tile = valid ? (below ? tile_at(J, Ip) : tile_at(Ip, J)) : Bq;
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const int e = tid + c * XTHREADS;  // 512 16-byte pieces of a 64 x 16 half
+            for (int c = 0; c < PIECES / XTHREADS; ++c) {
+                const int e = tid + c * XTHREADS;
                 if (!below) {
-                    const int r = e >> 3, kp = (e & 7) * 2;
+                    const int r = e / (XBK / 2), kp = (e % (XBK / 2)) * 2;
                     xcp16(ah + r * XLD + kp, tile + r * 64 + kin + kp, Bq, valid);
                 } else {
                     const int k = e >> 5, pp = (e & 31) * 2;
@@ -250,9 +254,9 @@ __global__ void __launch_bounds__(XTHREADS, 2) k_exchange_half(const double* con
             }
         }
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int e = tid + c * XTHREADS;  // 512 16-byte pieces of the 64 x 16 B tile
-            const int r = e >> 3, kp = (e & 7) * 2;
+        for (int c = 0; c < XBN * XBK / 2 / XTHREADS; ++c) {
+            const int e = tid + c * XTHREADS;  // the 16-byte pieces of the XBN x XBK tile of Ct
+            const int r = e / (XBK / 2), kp = (e % (XBK / 2)) * 2;
             xcp16(bs + r * XLD + kp, Ct + (int64_t)(n0 + r) * ldc_t + k0 + kp, Ct, true);
         }
     };
