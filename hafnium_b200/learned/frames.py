@@ -1,13 +1,15 @@
-"""Water frames and the rotation of AO blocks between global and local frames.
+"""Atom frames and the rotation of AO blocks between global and local frames.
 
-Each rigid water (atoms O, H, H) defines a right-handed frame: x along the HOH
-bisector, z along the plane normal (H1 - O) x (H2 - O), y = z x x. A density
-block expressed in the frames of its two waters, D~_ij = U_i^T D_ij U_j, does not
-change when the whole cluster is rotated or translated, which is what the
-network predicts. U_i rotates the cc-pVDZ functions of water i: 1 for s shells,
-the frame matrix for p shells (functions ordered x, y, z) and the induced 5x5
-rotation of the sphere-normalised real solid harmonics for d shells
-(hafnium/basis conventions, cartesian.rs:93-110).
+Every atom gets a right-handed frame from its neighbours: x towards the nearest
+atom, y towards the next atom that is not in line with the first (its part
+orthogonal to x), z = x cross y. Neighbours at equal distance (to 1e-6 bohr) are
+taken in atom order, so the frames depend only on the geometry's internal
+coordinates and the atom order. A density block expressed in the frames of its
+two atoms, D~_ij = U_i^T D_ij U_j, does not change when the whole molecule is
+rotated or translated, which is what the network predicts. U_i rotates the
+functions of atom i: 1 for s shells, the frame matrix for p shells (functions
+ordered x, y, z) and the induced rotation of the sphere-normalised real solid
+harmonics for d shells (hafnium/basis conventions, cartesian.rs:93-110).
 """
 
 from __future__ import annotations
@@ -74,14 +76,32 @@ def harmonic_rotation(r: np.ndarray, l: int) -> np.ndarray:
     return u
 
 
-def water_frame(o: np.ndarray, h1: np.ndarray, h2: np.ndarray) -> np.ndarray:
-    """Columns: the local x, y, z axes in global coordinates."""
-    x = (h1 - o) + (h2 - o)
-    x /= np.linalg.norm(x)
-    z = np.cross(h1 - o, h2 - o)
-    z /= np.linalg.norm(z)
-    y = np.cross(z, x)
-    return np.stack([x, y, z], axis=1)
+def atom_frames(positions: np.ndarray):
+    """Frame matrices (columns: the local x, y, z axes in global coordinates) of
+    every atom, or None when an atom has no two neighbours off one line (fewer
+    than three atoms, or a linear molecule)."""
+    pos = np.asarray(positions, dtype=np.float64)
+    n = len(pos)
+    if n < 3:
+        return None
+    frames = []
+    for i in range(n):
+        d = np.linalg.norm(pos - pos[i], axis=1)
+        order = sorted((j for j in range(n) if j != i), key=lambda j: (round(float(d[j]), 6), j))
+        x = (pos[order[0]] - pos[i]) / d[order[0]]
+        frame = None
+        for j in order[1:]:
+            v = pos[j] - pos[i]
+            v = v - (v @ x) * x
+            norm = np.linalg.norm(v)
+            if norm > 0.1 * d[j]:  # more than about 6 degrees off the x axis
+                y = v / norm
+                frame = np.stack([x, y, np.cross(x, y)], axis=1)
+                break
+        if frame is None:
+            return None
+        frames.append(frame)
+    return frames
 
 
 def shell_layout(table, atom_index: int):
@@ -104,14 +124,3 @@ def ao_rotation(r: np.ndarray, layout) -> np.ndarray:
         out[at:at + m, at:at + m] = b
         at += m
     return out
-
-
-def cluster_frames(molecule):
-    """Per water: origin (O position) and frame matrix; atoms ordered O, H, H."""
-    pos = np.asarray(molecule.positions)
-    nw = len(molecule.symbols) // 3
-    frames = []
-    for w in range(nw):
-        o, h1, h2 = pos[3 * w], pos[3 * w + 1], pos[3 * w + 2]
-        frames.append((o, water_frame(o, h1, h2)))
-    return frames

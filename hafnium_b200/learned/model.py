@@ -1,21 +1,27 @@
-"""The learned initial density: a message-passing network over waters.
+"""The learned initial density: a message-passing network over atoms and the
+AO shell-pair blocks between them.
 
-Nodes are the waters of a cluster, edges the ordered pairs whose oxygens are
-closer than ``R_CUT``. Every edge carries the geometry of water j seen from the
-frame of water i (oxygen and hydrogen positions, the relative rotation, a radial
-basis of the O-O distance), so everything the network sees and predicts is
-independent of how the cluster sits in space. Four residual message-passing
-layers of width 128 feed two heads: the 24 x 24 diagonal block of each water's
-density in its own frame (300 upper entries, on top of the training set's mean
-block) and the 24 x 24 block between the two waters of each edge. Blocks between
-waters further apart than ``R_CUT`` are zero.
+Nodes are the atoms of a molecule, edges the ordered atom pairs closer than
+``R_CUT``. A node starts from a learned embedding of its element; every edge
+carries the geometry of atom j seen from the frame of atom i (j's position, the
+relative rotation of the two frames, a radial basis of the distance), so
+everything the network sees and predicts is independent of how the molecule
+sits in space. Four residual message-passing layers of width 128 feed two
+heads: the diagonal block of each atom's density in its own frame (the upper
+triangle of the atom's shell-pair blocks, on top of the training set's mean
+block for its element) and the block between the two atoms of each edge (all
+their shell pairs), both laid out on NA_AO functions per atom (cc-pVDZ: 14 for
+B-Ne, 5 for H and He; the unused rows and columns are trained towards zero).
+Blocks between atoms further apart than ``R_CUT`` are zero.
 
 Forward, backward and Adam run on the device through the kernels of
-include/hfnn.h (FP32). ``predict`` turns the blocks into a global density and
-projects it onto the occupied space (the n_occ leading natural orbitals in the
-overlap metric), so the SCF starts from an idempotent density with the right
-electron count. Without trained weights or for anything but water clusters the
-caller falls back to the superposition of atomic densities.
+include/hfnn.h (FP32). ``predict_density`` turns the blocks into a global
+density, which the SCF projects onto the occupied space (the n_occ leading
+natural orbitals in the overlap metric) so that it starts from an idempotent
+density with the right electron count. For a molecule with an element the
+network was not trained on, an atom without a frame (a linear molecule), a basis
+other than cc-pVDZ or without trained weights the caller falls back to the
+superposition of atomic densities.
 """
 
 from __future__ import annotations
@@ -28,85 +34,117 @@ import pathlib
 
 import numpy as np
 
-from hafnium_b200.learned.frames import ao_rotation, cluster_frames
+from hafnium_b200.learned.frames import ao_rotation, atom_frames, shell_layout
 
-R_CUT = 9.0  # bohr, O-O
+R_CUT = 10.0  # bohr, atom-atom
 N_RBF = 16
-EDGE_FEATURES = 3 * 3 + 9 + N_RBF  # positions of j's atoms in i's frame, R_i^T R_j, RBF
+EDGE_FEATURES = 3 + 9 + N_RBF  # position of j in i's frame, R_i^T R_j, RBF of the distance
 WIDTH = 128
 LAYERS = 4
-NW_AO = 24  # cc-pVDZ functions per water
-DIAG = NW_AO * (NW_AO + 1) // 2
-OFF = NW_AO * NW_AO
-WEIGHTS = pathlib.Path(__file__).resolve().parent / "weights_ccpvdz_water.npz"
-_IU = np.triu_indices(NW_AO)
-
-WATER_LAYOUT = None  # (l, n_contractions) per shell of one water in cc-pVDZ
-
-
-def water_layout():
-    global WATER_LAYOUT
-    if WATER_LAYOUT is None:
-        from hafnium_b200.basis import ShellTable
-        from hafnium_b200.molecule import water
-
-        mol = water()
-        t = ShellTable.build("cc-pvdz", mol.symbols, mol.positions)
-        WATER_LAYOUT = [(int(l), int(k)) for l, k in zip(t.angular_momenta, t.n_contractions)]
-    return WATER_LAYOUT
+ELEMENTS = ("H", "He", "Li", "Be", "B", "C", "N", "O", "F", "Ne")  # embedding rows, Z = 1..10
+NA_AO = 14  # functions of one atom, padded (cc-pVDZ: 14 for B-Ne, 5 for H and He)
+DIAG = NA_AO * (NA_AO + 1) // 2
+OFF = NA_AO * NA_AO
+BASIS = "cc-pvdz"
+WEIGHTS = pathlib.Path(__file__).resolve().parent / "weights_ccpvdz_atoms.npz"
+_IU = np.triu_indices(NA_AO)
 
 
-def is_water_cluster(molecule) -> bool:
-    s = molecule.symbols
-    return len(s) % 3 == 0 and all(s[3 * w: 3 * w + 3] == ("O", "H", "H") for w in range(len(s) // 3))
+def element_index(symbol: str) -> int:
+    """Row of the element's embedding (Z - 1), -1 outside H-Ne."""
+    name = symbol.capitalize()
+    return ELEMENTS.index(name) if name in ELEMENTS else -1
 
 
-def build_graph(molecule) -> dict:
-    """Nodes, edges, edge features and the per-water AO rotations (host arrays)."""
-    frames = cluster_frames(molecule)
-    pos = np.asarray(molecule.positions)
-    nw = len(frames)
-    layout = water_layout()
-    rot = np.stack([ao_rotation(r, layout) for _, r in frames])  # [nw, 24, 24]
-    src, dst, feats, fcut = [], [], [], []
-    centers = np.linspace(1.5, R_CUT, N_RBF)
+def build_graph(molecule, table=None) -> dict | None:
+    """Nodes, edges, edge features, the per-atom AO rotations and function
+    ranges (host arrays); None when an atom has no frame or lies outside H-Ne."""
+    from hafnium_b200.basis import ShellTable
+
+    elem = np.array([element_index(s) for s in molecule.symbols], dtype=np.int32)
+    if len(elem) == 0 or np.any(elem < 0):
+        return None
+    pos = np.asarray(molecule.positions, dtype=np.float64)
+    frames = atom_frames(pos)
+    if frames is None:
+        return None
+    if table is None:
+        table = ShellTable.build(BASIS, molecule.symbols, pos)
+    n = len(pos)
+    rot = np.zeros((n, NA_AO, NA_AO))
+    nfun = np.zeros(n, dtype=np.int64)
+    for a in range(n):
+        u = ao_rotation(frames[a], shell_layout(table, a))
+        if u.shape[0] > NA_AO:
+            return None
+        nfun[a] = u.shape[0]
+        rot[a, : u.shape[0], : u.shape[0]] = u
+    offsets = np.concatenate([[0], np.cumsum(nfun)[:-1]])
+    fr = np.stack(frames)  # [atom, 3, 3], columns the local axes
+    diff = pos[None, :, :] - pos[:, None, :]  # [i, j] = r_j - r_i
+    dist = np.linalg.norm(diff, axis=2)
+    src, dst = np.nonzero((dist < R_CUT) & ~np.eye(n, dtype=bool))
+    d = dist[src, dst]
+    rel = np.einsum("eab,ea->eb", fr[src], diff[src, dst]) / R_CUT
+    rr = np.einsum("eab,eac->ebc", fr[src], fr[dst]).reshape(-1, 9)
+    centers = np.linspace(1.0, R_CUT, N_RBF)
     width = centers[1] - centers[0]
-    for i in range(nw):
-        oi, ri = frames[i]
-        for j in range(nw):
-            if i == j:
-                continue
-            oj, rj = frames[j]
-            d = np.linalg.norm(oj - oi)
-            if d >= R_CUT:
-                continue
-            rel = np.concatenate([ri.T @ (pos[3 * j + a] - oi) for a in range(3)]) / R_CUT
-            rbf = np.exp(-((d - centers) / width) ** 2)
-            feats.append(np.concatenate([rel, (ri.T @ rj).reshape(-1), rbf]))
-            src.append(i)
-            dst.append(j)
-            fcut.append(0.5 * (math.cos(math.pi * d / R_CUT) + 1.0))
+    rbf = np.exp(-(((d[:, None] - centers[None, :]) / width) ** 2))
     return {
-        "n_nodes": nw,
-        "src": np.asarray(src, dtype=np.int32),
-        "dst": np.asarray(dst, dtype=np.int32),
-        "edge": np.asarray(feats, dtype=np.float64).reshape(-1, EDGE_FEATURES),
-        "fcut": np.asarray(fcut, dtype=np.float64),
+        "n_nodes": n,
+        "elem": elem,
+        "src": src.astype(np.int32),
+        "dst": dst.astype(np.int32),
+        "edge": np.concatenate([rel, rr, rbf], axis=1).reshape(-1, EDGE_FEATURES),
+        "fcut": 0.5 * (np.cos(np.pi * d / R_CUT) + 1.0),
         "rot": rot,
+        "nfun": nfun,
+        "offsets": offsets,
+        "n_ao": int(nfun.sum()),
     }
 
 
+def _padded_index(graph: dict):
+    """(atom, local function) of every global function, in global order."""
+    nf = graph["nfun"]
+    atom, local = np.nonzero(np.arange(NA_AO)[None, :] < nf[:, None])
+    return atom, local
+
+
 def local_targets(graph: dict, density: np.ndarray, mean_diag: np.ndarray | None = None) -> dict:
-    """Blocks of a converged (per-spin) density in the frames of their waters."""
+    """Blocks of a converged (per-spin) density in the frames of their atoms,
+    laid out on NA_AO functions per atom."""
+    n = graph["n_nodes"]
+    atom, local = _padded_index(graph)
+    dp = np.zeros((n, NA_AO, n, NA_AO))
+    dp[atom[:, None], local[:, None], atom[None, :], local[None, :]] = density
     rot = graph["rot"]
-    nw = graph["n_nodes"]
-    blk = lambda i, j: density[NW_AO * i: NW_AO * (i + 1), NW_AO * j: NW_AO * (j + 1)]  # noqa: E731
-    d = np.stack([(rot[i].T @ blk(i, i) @ rot[i])[_IU] for i in range(nw)])
+    dl = np.einsum("iab,iajc,jcd->ibjd", rot, dp, rot, optimize=True)
+    idx = np.arange(n)
+    d = dl[idx, :, idx, :][:, _IU[0], _IU[1]]
     if mean_diag is not None:
-        d = d - mean_diag
-    o = np.stack([(rot[i].T @ blk(i, j) @ rot[j]).reshape(-1) for i, j in zip(graph["src"], graph["dst"])]) \
-        if len(graph["src"]) else np.zeros((0, OFF))
+        d = d - mean_diag[graph["elem"]]
+    o = dl[graph["src"], :, graph["dst"], :].reshape(-1, OFF)
     return {"d": d, "o": o}
+
+
+def blocks_to_density(graph: dict, d_blocks: np.ndarray, o_blocks: np.ndarray, mean_diag: np.ndarray) -> np.ndarray:
+    """Global per-spin density from local-frame blocks (symmetrised over the two
+    edges of an atom pair)."""
+    n = graph["n_nodes"]
+    dl = np.zeros((n, NA_AO, n, NA_AO))
+    diag = np.zeros((n, NA_AO, NA_AO))
+    diag[:, _IU[0], _IU[1]] = d_blocks + mean_diag[graph["elem"]]
+    diag = diag + np.transpose(np.triu(diag, 1), (0, 2, 1))
+    idx = np.arange(n)
+    dl[idx, :, idx, :] = diag
+    o = o_blocks.reshape(-1, NA_AO, NA_AO)
+    np.add.at(dl, (graph["src"], slice(None), graph["dst"], slice(None)), 0.5 * o)
+    np.add.at(dl, (graph["dst"], slice(None), graph["src"], slice(None)), 0.5 * np.transpose(o, (0, 2, 1)))
+    rot = graph["rot"]
+    dp = np.einsum("iab,ibjc,jdc->iajd", rot, dl, rot, optimize=True)
+    atom, local = _padded_index(graph)
+    return dp[atom[:, None], local[:, None], atom[None, :], local[None, :]]
 
 
 def init_params(seed: int = 0) -> dict:
@@ -115,7 +153,7 @@ def init_params(seed: int = 0) -> dict:
     def dense(i, o, scale=1.0):
         return (rng.normal(size=(i, o)) * scale / math.sqrt(i)).astype(np.float32), np.zeros(o, np.float32)
 
-    p = {"h0": (rng.normal(size=WIDTH) * 0.5).astype(np.float32)}
+    p = {"h0": (rng.normal(size=(len(ELEMENTS), WIDTH)) * 0.5).astype(np.float32)}  # one row per element
     for l in range(LAYERS):
         p[f"Wm{l}"], p[f"bm{l}"] = dense(2 * WIDTH + EDGE_FEATURES, WIDTH)
         p[f"Wu{l}"], p[f"bu{l}"] = dense(2 * WIDTH, WIDTH, 0.5)
@@ -147,7 +185,7 @@ class DeviceNet:
         self._bind()
         self.p = {k: torch.as_tensor(np.asarray(v, dtype=np.float32), device=self.dev).contiguous()
                   for k, v in params.items()}
-        self.width = int(self.p["h0"].shape[0])
+        self.width = int(self.p["h0"].shape[1])
 
     def _bind(self) -> None:
         L, v, f, i, i64 = self.lib, ctypes.c_void_p, ctypes.c_float, ctypes.c_int, ctypes.c_int64
@@ -188,6 +226,7 @@ class DeviceNet:
         t = self.torch
         return {
             "n": graph["n_nodes"],
+            "elem": t.as_tensor(graph["elem"], dtype=t.int32, device=self.dev),
             "src": t.as_tensor(graph["src"], dtype=t.int32, device=self.dev),
             "dst": t.as_tensor(graph["dst"], dtype=t.int32, device=self.dev),
             "edge": t.as_tensor(graph["edge"], dtype=t.float32, device=self.dev).contiguous(),
@@ -210,7 +249,9 @@ class DeviceNet:
     def forward(self, g):
         t, W, s = self.torch, self.width, self._stream()
         n, ne = g["n"], g["ne"]
-        h = self.p["h0"].unsqueeze(0).repeat(n, 1).contiguous()
+        h = t.empty((n, W), dtype=t.float32, device=self.dev)  # each atom's element embedding
+        self._ok(self.lib.hfnn_gather(n, W, self._ptr(self.p["h0"]), self._ptr(g["elem"]), self._ptr(h), W, 0, s),
+                 "gather")
         cache = []
         for l in range(self.layers):
             xm = self._edge_input(h, g)
@@ -284,8 +325,9 @@ class DeviceNet:
             self._ok(self.lib.hfnn_scatter_add(ne, W, self._ptr(dxm), ld, W, self._ptr(g["dst"]), None,
                                                self._ptr(dh_in), s), "scatter")
             dh = dh_in
-        gh0 = t.empty(W, dtype=t.float32, device=self.dev)
-        self._ok(self.lib.hfnn_colsum(n, W, self._ptr(dh.contiguous()), self._ptr(gh0), s), "colsum")
+        gh0 = t.zeros_like(self.p["h0"])  # per element: the sum over its atoms
+        self._ok(self.lib.hfnn_scatter_add(n, W, self._ptr(dh.contiguous()), W, 0, self._ptr(g["elem"]), None,
+                                           self._ptr(gh0), s), "scatter")
         grads["h0"] = gh0
         return loss, grads
 
@@ -314,7 +356,7 @@ def save_weights(path: pathlib.Path, params: dict, mean_diag: np.ndarray, meta: 
     for k in sorted(arrays):
         digest.update(k.encode())
         digest.update(np.ascontiguousarray(arrays[k]).tobytes())
-    meta = dict(meta, sha256=digest.hexdigest(), version=1, layers=LAYERS, width=WIDTH, r_cut=R_CUT)
+    meta = dict(meta, sha256=digest.hexdigest(), version=2, layers=LAYERS, width=WIDTH, r_cut=R_CUT, na_ao=NA_AO)
     np.savez_compressed(path, meta=json.dumps(meta), **arrays)
     return meta["sha256"]
 
@@ -336,33 +378,20 @@ def load_weights(path: pathlib.Path = WEIGHTS):
     return arrays, mean_diag, meta
 
 
-def blocks_to_density(graph: dict, d_blocks: np.ndarray, o_blocks: np.ndarray, mean_diag: np.ndarray) -> np.ndarray:
-    """Global per-spin density from local-frame blocks (symmetrised over edge pairs)."""
-    nw = graph["n_nodes"]
-    rot = graph["rot"]
-    n = NW_AO * nw
-    dens = np.zeros((n, n))
-    for i in range(nw):
-        b = np.zeros((NW_AO, NW_AO))
-        b[_IU] = d_blocks[i] + mean_diag
-        b = b + np.triu(b, 1).T
-        dens[NW_AO * i: NW_AO * (i + 1), NW_AO * i: NW_AO * (i + 1)] = rot[i] @ b @ rot[i].T
-    for e, (i, j) in enumerate(zip(graph["src"], graph["dst"])):
-        b = rot[i] @ o_blocks[e].reshape(NW_AO, NW_AO) @ rot[j].T
-        dens[NW_AO * i: NW_AO * (i + 1), NW_AO * j: NW_AO * (j + 1)] += 0.5 * b
-        dens[NW_AO * j: NW_AO * (j + 1), NW_AO * i: NW_AO * (i + 1)] += 0.5 * b.T
-    return dens
-
-
 def predict_density(molecule, weights=None, device: int = 0):
-    """The network's per-spin density of a water cluster, or None (fall back to SAD)."""
-    if not is_water_cluster(molecule):
-        return None
+    """The network's per-spin density of a molecule in cc-pVDZ, or None (fall
+    back to SAD): no weights, an element the network was not trained on, or an
+    atom without a frame."""
     loaded = load_weights() if weights is None else weights
     if loaded is None:
         return None
-    params, mean_diag, _ = loaded
+    params, mean_diag, meta = loaded
+    trained = set(meta.get("elements", ()))
+    if any(s.capitalize() not in trained for s in molecule.symbols):
+        return None
     graph = build_graph(molecule)
+    if graph is None:
+        return None
     net = DeviceNet(params, device=device)
     out, _ = net.forward(net.upload_graph(graph))
     d = out["d"].double().cpu().numpy()

@@ -4,8 +4,10 @@
 
 1. Seeded water clusters (H2O)n, n uniform in [2, 12], are converged together
    by the batched device DF-RHF (SAD guess, FP64, the reference's default
-   tolerances); their per-spin densities, expressed in the frames of their
-   waters, are the targets.
+   tolerances).
+   Their per-spin densities, expressed in the frames of their atoms (the
+   shell-pair blocks of every atom and every atom pair within the cutoff), are
+   the targets.
 2. The network (hafnium_b200.learned.model) is trained with Adam on the device,
    forward and backward running on the hfnn kernels, several clusters per step.
 3. Held-out (H2O)16-24 clusters are converged from the SAD guess and from the
@@ -55,15 +57,21 @@ def make_dataset(count: int, seed0: int, n_range=(2, 12), device: int = 0, batch
     data = []
     for mol, d in zip(mols, dens):
         graph = M.build_graph(mol)
-        data.append((graph, M.local_targets(graph, d)))
+        if graph is None:
+            continue
+        tgt = M.local_targets(graph, d)
+        # the training steps need neither the rotations nor FP64 targets
+        graph = {k: v for k, v in graph.items() if k != "rot"}
+        data.append((graph, {"d": tgt["d"], "o": tgt["o"].astype(np.float32)}))
     return data
 
 
 def union(batch):
     """Disjoint union of several graphs and their targets (one training step)."""
     offset = 0
-    src, dst, edge, fcut, d, o = [], [], [], [], [], []
+    elem, src, dst, edge, fcut, d, o = [], [], [], [], [], [], []
     for graph, tgt in batch:
+        elem.append(graph["elem"])
         src.append(graph["src"] + offset)
         dst.append(graph["dst"] + offset)
         edge.append(graph["edge"])
@@ -71,15 +79,27 @@ def union(batch):
         d.append(tgt["d"])
         o.append(tgt["o"])
         offset += graph["n_nodes"]
-    g = {"n_nodes": offset, "src": np.concatenate(src).astype(np.int32), "dst": np.concatenate(dst).astype(np.int32),
+    g = {"n_nodes": offset, "elem": np.concatenate(elem).astype(np.int32),
+         "src": np.concatenate(src).astype(np.int32), "dst": np.concatenate(dst).astype(np.int32),
          "edge": np.concatenate(edge), "fcut": np.concatenate(fcut)}
     return g, {"d": np.concatenate(d), "o": np.concatenate(o)}
+
+
+def element_means(data) -> np.ndarray:
+    """The mean diagonal block of each element over the training atoms (zero for
+    elements that do not occur)."""
+    total = np.zeros((len(M.ELEMENTS), M.DIAG))
+    count = np.zeros(len(M.ELEMENTS))
+    for graph, tgt in data:
+        np.add.at(total, graph["elem"], tgt["d"])
+        np.add.at(count, graph["elem"], 1.0)
+    return total / np.maximum(count, 1.0)[:, None]
 
 
 def train(data, epochs: int, batch: int = 8, lr: float = 1e-3, seed: int = 0, device: int = 0, log=print):
     import torch
 
-    mean_diag = np.mean(np.concatenate([t["d"] for _, t in data]), axis=0)
+    mean_diag = element_means(data)
     net = M.DeviceNet(M.init_params(seed), device=device)
     opt = M.Adam(net, lr)
     rng = np.random.default_rng(seed)
@@ -88,7 +108,7 @@ def train(data, epochs: int, batch: int = 8, lr: float = 1e-3, seed: int = 0, de
     for i in range(0, len(data), batch):
         g, t = union(data[i:i + batch])
         gd = net.upload_graph(g)
-        td = {"d": torch.as_tensor(t["d"] - mean_diag, dtype=torch.float32, device=dev).contiguous(),
+        td = {"d": torch.as_tensor(t["d"] - mean_diag[g["elem"]], dtype=torch.float32, device=dev).contiguous(),
               "o": torch.as_tensor(t["o"], dtype=torch.float32, device=dev).contiguous()}
         prepared.append((gd, td, float(len(t["d"]))))
     history = []
@@ -103,7 +123,7 @@ def train(data, epochs: int, batch: int = 8, lr: float = 1e-3, seed: int = 0, de
         if epoch >= epochs // 2:
             opt.lr = lr * 0.5 * (1 + np.cos(np.pi * (epoch - epochs // 2) / max(1, epochs - epochs // 2)))
         history.append(total / nodes)
-        log(f"epoch {epoch:3d}  loss per water {total / nodes:.4e}")
+        log(f"epoch {epoch:3d}  loss per atom {total / nodes:.4e}")
     params = {k: v.cpu().numpy() for k, v in net.p.items()}
     return params, mean_diag, history
 
@@ -159,7 +179,9 @@ def main() -> None:
     print(f"dataset: {len(data)} clusters in {t1 - t0:.1f} s", flush=True)
     params, mean_diag, history = train(data, args.epochs, args.batch, args.lr, args.seed)
     t2 = time.perf_counter()
-    meta = {"clusters": args.clusters, "n_range": [2, 12], "epochs": args.epochs, "batch": args.batch, "lr": args.lr,
+    trained = sorted({M.ELEMENTS[e] for graph, _ in data for e in graph["elem"]})
+    meta = {"clusters": args.clusters, "n_range": [2, 12], "elements": trained, "epochs": args.epochs,
+            "batch": args.batch, "lr": args.lr,
             "seed": args.seed, "basis": BASIS, "auxiliary": AUX, "loss_history": history,
             "dataset_s": t1 - t0, "train_s": t2 - t1}
     out = pathlib.Path(args.out)

@@ -340,8 +340,8 @@ def project_occupied(ham: DeviceHamiltonian, density, threshold: float = DEFAULT
 def learned_density_guess(molecule, ham: DeviceHamiltonian, *, weights=None, basis: str = "cc-pvdz",
                           device: int = 0):
     """The learned network's density projected onto the occupied space; the SAD
-    guess (atoms.py:76-120) when the network does not apply (no weights, not a
-    water cluster in cc-pVDZ)."""
+    guess (atoms.py:76-120) when the network does not apply (no weights, another
+    basis than cc-pVDZ, an element it was not trained on, a linear molecule)."""
     from hafnium_b200.learned.model import predict_density
 
     predicted = predict_density(molecule, weights, device=device) if basis == "cc-pvdz" else None

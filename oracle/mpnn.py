@@ -5,14 +5,14 @@ kernels (hafnium_b200/csrc/mpnn.cu). The network has no counterpart in the
 reference (it is the north star's new learned initial guess); this file states
 its mathematics independently of the CUDA code:
 
-    h_i^0 = h0                                   (learned embedding, all waters alike)
+    h_i^0 = h0[elem_i]                           (learned embedding of atom i's element)
     for each layer l:
         m_ij = silu(W_m^l [h_i ; h_j ; e_ij] + b_m^l) * fcut_ij
         a_i  = sum_j m_ij
         h_i  <- h_i + silu(W_u^l [h_i ; a_i] + b_u^l)
-    d_i  = W_d h_i + b_d                          (diagonal block, 300 upper entries)
+    d_i  = W_d h_i + b_d                          (diagonal block of atom i, upper entries)
     g_ij = silu(W_e [h_i ; h_j ; e_ij] + b_e)
-    o_ij = W_o g_ij + b_o                         (576 entries of the 24 x 24 block)
+    o_ij = W_o g_ij + b_o                         (the block between atoms i and j)
     loss = sum_i |d_i - t_i|^2 + w_edge sum_ij |o_ij - t_ij|^2
 
 Weights are stored as [in, out]; activations as rows.
@@ -36,8 +36,7 @@ def forward(params: dict, graph: dict, layers: int):
     """Returns the outputs and the cache the backward pass needs."""
     src, dst = graph["src"], graph["dst"]  # edge (i -> j): i = src (receiver), j = dst
     e, fc = graph["edge"], graph["fcut"]
-    n = graph["n_nodes"]
-    h = np.tile(params["h0"], (n, 1))
+    h = params["h0"][graph["elem"]]
     cache = []
     for l in range(layers):
         xm = np.concatenate([h[src], h[dst], e], axis=1)
@@ -98,5 +97,6 @@ def loss_and_grad(params: dict, graph: dict, targets: dict, layers: int, w_edge:
         np.add.at(dh_in, src, dxm[:, :width])
         np.add.at(dh_in, dst, dxm[:, width:2 * width])
         dh = dh_in
-    grads["h0"] = dh.sum(0)
+    grads["h0"] = np.zeros_like(params["h0"])
+    np.add.at(grads["h0"], graph["elem"], dh)
     return loss, grads
