@@ -188,6 +188,30 @@ def torch_sync(tensor) -> None:
     torch.cuda.current_stream(tensor.device).synchronize()
 
 
+def host_empty(shape) -> np.ndarray:
+    """An uninitialised FP64 host array in page-locked memory (torch's caching
+    pinned-memory allocator, so repeated calls reuse blocks), into which the
+    device-to-host copy of a result runs at full bus speed instead of through
+    the driver's staging of pageable memory; plain NumPy memory without a GPU."""
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            return torch.empty(tuple(shape), dtype=torch.float64, pin_memory=True).numpy()
+    except (ImportError, RuntimeError):  # pragma: no cover - a GPU process has torch and CUDA
+        pass
+    return np.empty(tuple(shape))
+
+
+def to_host(tensor) -> np.ndarray:
+    """A device tensor's values as a NumPy array in page-locked memory."""
+    out = host_empty(tensor.shape)
+    import torch
+
+    torch.from_numpy(out).copy_(tensor)
+    return out
+
+
 def release_retained(device: int = 0) -> None:
     """Free the fitted-tensor blocks the library keeps on ``device`` for the next
     context of the same size (see hf_release_retained in include/hfjk.h)."""
@@ -276,13 +300,13 @@ class Context:
     # -- host-array entry points (numpy in, numpy out) ---------------------
     def coulomb_host(self, d: np.ndarray) -> np.ndarray:
         d = np.ascontiguousarray(d, dtype=np.float64)
-        out = np.empty_like(d)
+        out = host_empty(d.shape)
         self.check(self.lib.hf_coulomb(self.handle, d.ctypes.data, out.ctypes.data, 0), "hf_coulomb")
         return out
 
     def exchange_host(self, d: np.ndarray, precision: int = PREC_FP64) -> np.ndarray:
         d = np.ascontiguousarray(d, dtype=np.float64)
-        out = np.empty_like(d)
+        out = host_empty(d.shape)
         self.check(self.lib.hf_exchange(self.handle, d.ctypes.data, out.ctypes.data, precision, 0), "hf_exchange")
         return out
 
@@ -290,7 +314,7 @@ class Context:
         c = np.ascontiguousarray(c, dtype=np.float64)
         n = c.shape[0]
         w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
-        out = np.empty((n, n))
+        out = host_empty((n, n))
         self.check(
             self.lib.hf_exchange_factored(
                 self.handle, c.ctypes.data, c.shape[1], None if w is None else w.ctypes.data, out.ctypes.data,

@@ -310,7 +310,7 @@ class B200DensityFittedCoulombExchange:
             if "semidefinite" not in str(error):
                 raise
             return self._exchange_signed(density, on_device)
-        return k if on_device else k.cpu().numpy()
+        return k if on_device else _lib.to_host(k)
 
     def _exchange_signed(self, density, on_device: bool):
         import torch
@@ -324,7 +324,7 @@ class B200DensityFittedCoulombExchange:
         sign = torch.sign(w[keep]).contiguous()
         out = torch.empty_like(d)
         self.context.exchange_factored_device(c, out, sign, self.precision)
-        return out if on_device else out.cpu().numpy()
+        return out if on_device else _lib.to_host(out)
 
     def orbital_tensor(self, c_bra, c_ket):
         """``B[P, p, q]`` in an orbital basis (hafnium/orbitals/integrals.py:73-157,

@@ -2,6 +2,7 @@
 
     python -m hafnium_b200.profile_case [--waters 16] [--repeats 1] [--batched 0] [--gradient]
                                         [--columns 0]
+    python -m hafnium_b200.profile_case --gemm M,N,K [--repeats 3]
 
 Builds one seeded (H2O)n (one-electron integrals, metric, factor, three-centre
 integrals, fitted tensor), then runs ``repeats`` of each build on the
@@ -11,7 +12,9 @@ With ``--batched C`` it also converges C seeded (H2O)2 clusters through the
 batched graph-resident SCF; with ``--gradient`` it times the DF-RHF nuclear
 gradient of the same orbitals (the kernels do not depend on the values). With
 ``--columns W`` the K builds use a random factor of W columns instead of the
-occupied orbitals. Prints one JSON line with the device time of each step (CUDA
+occupied orbitals. ``--gemm M,N,K`` times only the FP64 DMMA GEMM C = A B^T on
+random operands, every CTA tile of ``hf_dgemm_nt`` in turn and then cuBLAS
+(``torch.matmul``) on the same product, checking each against it. Prints one JSON line with the device time of each step (CUDA
 events), so the same command gives both the timing and, under ``ncu``, the
 launch list of a bounded number of kernels.
 """
@@ -20,6 +23,39 @@ from __future__ import annotations
 
 import argparse
 import json
+
+
+def gemm_case(torch, shape, repeats: int) -> None:
+    """TF/s of every hf_dgemm_nt tile and of cuBLAS on C[M][N] = A[M][K] B[N][K]^T."""
+    from hafnium_b200.batch import TILE_SHAPES, dgemm_nt
+
+    m, n, k = shape
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device=dev).manual_seed(0)
+    a = torch.randn((1, m, k), dtype=torch.float64, device=dev, generator=gen)
+    b = torch.randn((1, n, k), dtype=torch.float64, device=dev, generator=gen)
+    c = torch.empty((1, m, n), dtype=torch.float64, device=dev)
+    ref = a[0] @ b[0].T
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"gemm": [m, n, k]}
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(repeats):
+            fn()
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / repeats
+        return {"ms": ms, "tflops": 2.0 * m * n * k / ms / 1e9}
+
+    for tile, (bm, bn) in enumerate(TILE_SHAPES):
+        row = timed(lambda: dgemm_nt(a, b, c, tile=tile))
+        row["max_abs_diff"] = float((c[0] - ref).abs().max())
+        out[f"tile{tile}_{bm}x{bn}"] = row
+    out["cublas"] = timed(lambda: torch.matmul(a[0], b[0].T, out=c[0]))
+    print(json.dumps(out), flush=True)
 
 
 def main() -> None:
@@ -32,9 +68,15 @@ def main() -> None:
     ap.add_argument("--columns", type=int, default=0,
                     help="factor width of the K builds (default: the occupied orbitals), e.g. 320 to give a "
                          "smaller cluster the (H2O)64 tile shape")
+    ap.add_argument("--gemm", type=str, default="",
+                    help="M,N,K: time the FP64 DMMA GEMM tiles and cuBLAS on one product instead")
     args = ap.parse_args()
 
     import torch
+
+    if args.gemm:
+        gemm_case(torch, [int(x) for x in args.gemm.split(",")], max(1, args.repeats))
+        return
 
     from hafnium_b200 import _lib
     from hafnium_b200.molecule import water_cluster
