@@ -51,9 +51,19 @@ __host__ __device__ constexpr int smem_of() {
     return STAGES * (BM + BN) * (BK + 4) * (int)sizeof(double);
 }
 
+// CTAs per SM the register budget is sized for: up to 16 warps, as many as the
+// shared memory of the pipeline lets reside.
+template <int BM, int BN, int BK, int STAGES>
+__host__ __device__ constexpr int min_ctas_of() {
+    const int by_warps = 512 / threads_of<BM, BN>();
+    const int by_smem = (227 * 1024) / smem_of<BM, BN, BK, STAGES>();
+    const int m = by_warps < by_smem ? by_warps : by_smem;
+    return m < 1 ? 1 : m;
+}
+
 // VEC: operands 16-byte aligned with even row strides, copied two doubles at a time.
 template <int BM, int BN, int BK, int STAGES, bool VEC>
-__global__ void __launch_bounds__(threads_of<BM, BN>(), (512 / threads_of<BM, BN>()) < 1 ? 1 : 512 / threads_of<BM, BN>())
+__global__ void __launch_bounds__(threads_of<BM, BN>(), (min_ctas_of<BM, BN, BK, STAGES>()))
     k_dgemm_nt(GemmArgs g) {
     constexpr int THREADS = threads_of<BM, BN>();
     constexpr int LD = BK + 4;

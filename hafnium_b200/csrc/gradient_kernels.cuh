@@ -211,9 +211,7 @@ __device__ __forceinline__ void cta_sum12(double* v, double* red) {
     }
 }
 
-// Threads per CTA of the three-centre derivative kernel: with the pair data of
-// the larger classes at 50-90 KB of shared memory, two CTAs fit an SM, so the
-// CTA is made wide to keep 16 warps resident.
+// Threads per CTA of the pair-data kernel (one CTA per shell pair).
 constexpr int kGradThreads = 256;
 
 // The pair data of grad_pair_prologue, built once per shell pair into global
@@ -240,14 +238,37 @@ __global__ void __launch_bounds__(kGradThreads) k_grad_pair_data(const PairTask*
     if (threadIdx.x == 0) npps[blockIdx.x] = npp;
 }
 
-// One CTA per orbital shell pair of class (LA <= LB) and group of slabs of
-// auxiliary shells of class LP from this block's list (slab blockIdx.y, then
-// every gridDim.y-th); one thread per (auxiliary shell, m_P) of a slab.
-// Accumulates, for the Coulomb (slot 0..2) and exchange (slot 3..5) weights,
-// the auxiliary-centre derivative into gaux[aux shell][6] and the two orbital
+// Shapes of one class of the three-centre derivative kernel. As in the (P|mu nu)
+// kernel, the threads of an auxiliary shell (one per m_P, all in one warp) share
+// each primitive triple's R table (order l_a + l_b + l_P + 1): per round TPR of
+// them evaluate one triple's table each into a row of shared memory, and after
+// a warp barrier every thread contracts all TPR rows with the nonzero entries of
+// its own Cartesian-to-spherical row. The pair data stays in global memory
+// (read-only, the same address across the CTA), which leaves shared memory to
+// the tables.
+constexpr int kGradCenterThreads = 128;
+constexpr int kGradRTableBytes = 40 * 1024;
+template <int LA, int LB, int LP>
+struct GradCenterShape {
+    static constexpr int L = LA + LB + LP + 1;
+    static constexpr int NCP = ncart(LP), NSP = nsph(LP);
+    static constexpr int SPW = 32 / NSP;                           // auxiliary shells per warp
+    static constexpr int SPB = (kGradCenterThreads / 32) * SPW;    // ... per CTA
+    static constexpr int NH = ntet(LA + LB), NH1 = ntet(LA + LB + 1);
+    static constexpr int NR = ntet(L);
+    static constexpr int RS = (NR + 1) | 1;  // the table and its prefactor, odd: rows in different banks
+    static constexpr int FIT = kGradRTableBytes / (SPB * RS * 8);
+    static constexpr int TPR = FIT < 1 ? 1 : (FIT > NSP ? NSP : FIT);
+    static constexpr int R_DOUBLES = SPB * TPR * RS;
+};
+
+// One CTA per orbital shell pair of class (LA <= LB) and slab of SPB auxiliary
+// shells of class LP from this block's list; thread (slot, m_P) accumulates,
+// for the Coulomb (slot 0..2) and exchange (slot 3..5) weights, the
+// auxiliary-centre derivative into gaux[aux shell][6] and the two orbital
 // centres' derivatives into gorb[orbital shell][6].
 template <int LA, int LB, int LP>
-__global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTask* __restrict__ tasks,
+__global__ void __launch_bounds__(kGradCenterThreads) k_three_center_grad(const PairTask* __restrict__ tasks,
                                                            const DevShell* __restrict__ orb,
                                                            const DevShell* __restrict__ aux,
                                                            const double* __restrict__ exps,
@@ -259,47 +280,74 @@ __global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTa
                                                            const int* __restrict__ npps,
                                                            double* __restrict__ gorb, double* __restrict__ gaux) {
     using PL = GradPairLayout<LA, LB>;
-    constexpr int L = LA + LB + LP + 1;
-    constexpr int LAB = LA + LB;
-    constexpr int NCP = ncart(LP), NSP = nsph(LP);
-    constexpr int SPB = kGradThreads / NSP;
-    extern __shared__ double smem[];
-    __shared__ double red[kGradThreads / 32 * 12];
+    using SH = GradCenterShape<LA, LB, LP>;
+    constexpr int L = SH::L, NCP = SH::NCP, NSP = SH::NSP, SPW = SH::SPW, NH = SH::NH, NH1 = SH::NH1;
+    constexpr int TPR = SH::TPR, RS = SH::RS, NR = SH::NR;
+    extern __shared__ double sR[];           // the round's R tables
+    __shared__ int s_idx1[NCP * NH1];        // tet(h + c), h of order <= l_a + l_b + 1
+    __shared__ int s_idx3[NCP * NH * 3];     // tet(h + c + e_d), h of order <= l_a + l_b
+    __shared__ int s_nzc[NSP * NCP];         // per m_P: the Cartesian components with a nonzero weight
+    __shared__ double s_nzw[NSP * NCP];      // ... and the weights
+    __shared__ int s_nnz[NSP];
+    __shared__ int s_tp[SH::SPB * TPR];      // primitive pair of each table of the round, -1 past the end
+    __shared__ double red[kGradCenterThreads / 32 * 12];
     const PairTask task = tasks[blockIdx.x];
     const int ia_shell = task.swap ? task.second : task.first;
     const int ib_shell = task.swap ? task.first : task.second;
-    const DevShell A = orb[ia_shell];
-    const DevShell B = orb[ib_shell];
     const int npp = npps[blockIdx.x];
-    if (npp == 0) return;  // nothing survives screening
-    {
-        const double* src = pdata + offsets[blockIdx.x];
-        const int total = npp * PL::STRIDE;
-        for (int k = threadIdx.x; k < total; k += blockDim.x) smem[k] = src[k];
+    if (npp == 0) return;  // the same for the whole CTA: nothing survives screening
+    const double* __restrict__ pd = pdata + offsets[blockIdx.x];
+
+    for (int e = threadIdx.x; e < NCP * NH1; e += blockDim.x) {
+        const int c = e / NH1, h = e - c * NH1;
+        s_idx1[e] = tet(c_tet_t[h] + c_cart[LP][c][0], c_tet_u[h] + c_cart[LP][c][1], c_tet_v[h] + c_cart[LP][c][2]);
+    }
+    for (int e = threadIdx.x; e < NCP * NH * 3; e += blockDim.x) {
+        const int c = e / (NH * 3), r = e - c * NH * 3, h = r / 3, d = r - h * 3;
+        s_idx3[e] = tet(c_tet_t[h] + c_cart[LP][c][0] + (d == 0), c_tet_u[h] + c_cart[LP][c][1] + (d == 1),
+                        c_tet_v[h] + c_cart[LP][c][2] + (d == 2));
+    }
+    if (threadIdx.x < NSP) {
+        int k = 0;
+        for (int c = 0; c < NCP; ++c) {
+            const double w = c_c2s[c2s_offset(LP) + threadIdx.x * NCP + c];
+            if (w != 0.0) {
+                s_nzc[threadIdx.x * NCP + k] = c;
+                s_nzw[threadIdx.x * NCP + k] = w;
+                ++k;
+            }
+        }
+        s_nnz[threadIdx.x] = k;
     }
     __syncthreads();
 
-    const int slot = threadIdx.x / NSP, mp = threadIdx.x % NSP;
-    const int nslabs = (nalist + SPB - 1) / SPB;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wslot = lane / NSP, mp = lane - wslot * NSP;
+    const int slot = warp * SPW + wslot;
+    const int ia = blockIdx.y * SH::SPB + slot;
+    const bool active = wslot < SPW && ia < nalist;
     const double fac = task.first == task.second ? 1.0 : 2.0;
-    // per-thread sums over the slabs for the two orbital centres:
-    // A_J[3] A_K[3] B_J[3] B_K[3] (J parts with the factor c_P applied)
+    // per-thread sums for the two orbital centres: A_J[3] A_K[3] B_J[3] B_K[3]
+    // (J parts with the factor c_P applied)
     double v[12];
 #pragma unroll
     for (int k = 0; k < 12; ++k) v[k] = 0.0;
-    // this CTA's pair data stays in shared memory while it walks over slabs
-    for (int slab = blockIdx.y; slab < nslabs; slab += gridDim.y) {
-        const int ia = slab * SPB + slot;
-        if (slot >= SPB || ia >= nalist) continue;
-        // acc: Q_J[3] Q_K[3] A_J[3] A_K[3] (J parts without the factor c_P)
-        double acc[12];
+    // acc: Q_J[3] Q_K[3] A_J[3] A_K[3] (J parts without the factor c_P)
+    double acc[12];
 #pragma unroll
-        for (int k = 0; k < 12; ++k) acc[k] = 0.0;
-        const int pshell = alist[ia];
-        const DevShell P = aux[pshell];
+    for (int k = 0; k < 12; ++k) acc[k] = 0.0;
+    DevShell P{};
+    int pshell = 0, ntrip = 0;
+    double cP = 0.0;
+    double gk[PL::KK][PL::NSAB];
+    if (active) {
+        pshell = alist[ia];
+        P = aux[pshell];
+        ntrip = P.nprim * npp;
         const int pf = P.fn + mp;
-        const double cP = g.cfit[pf];
-        double gk[PL::KK][PL::NSAB];
+        cP = g.cfit[pf];
+        const DevShell A = orb[ia_shell];
+        const DevShell B = orb[ib_shell];
 #pragma unroll
         for (int ka = 0; ka < PL::KA; ++ka)
 #pragma unroll
@@ -315,20 +363,70 @@ __global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTa
                         }
                         gk[ka * PL::KB + kb][ma * PL::NSB + mb] = val;
                     }
-        double crow[NCP];
+    } else {
 #pragma unroll
-        for (int c = 0; c < NCP; ++c) crow[c] = c_c2s[c2s_offset(LP) + mp * NCP + c];
-        for (int i = 0; i < P.nprim; ++i) {
-            const double q = exps[P.prim + i];
-            double cq = coefs[P.coef + i] * pow(2.0 * q, -(double)LP);
-            if (LP & 1) cq = -cq;
-            for (int pp = 0; pp < npp; ++pp) {
-                const double* s = smem + pp * PL::STRIDE;
+        for (int k = 0; k < PL::KK; ++k)
+#pragma unroll
+            for (int m = 0; m < PL::NSAB; ++m) gk[k][m] = 0.0;
+    }
+    // rounds of this warp: its slowest shell's triples over TPR
+    const int rounds = __reduce_max_sync(0xffffffffu, (ntrip + TPR - 1) / TPR);
+    const int nnz = s_nnz[active ? mp : 0];
+    const int* __restrict__ nzc = s_nzc + (active ? mp : 0) * NCP;
+    const double* __restrict__ nzw = s_nzw + (active ? mp : 0) * NCP;
+
+    // this thread's triple t = r TPR + mp as (auxiliary primitive i, primitive pair pp),
+    // advanced by TPR per round; the auxiliary primitive's factors are kept while i stays
+    int ti = mp / npp, tpp = mp - (mp / npp) * npp;
+    int ci = -1;
+    double q = 0.0, cq = 0.0;
+    for (int r = 0; r < rounds; ++r) {
+        if (active && mp < TPR) {
+            int pp = -1;
+            if (ti < P.nprim) {
+                pp = tpp;
+                if (ti != ci) {
+                    ci = ti;
+                    q = exps[P.prim + ti];
+                    // c_P (2q)^-l_P (-1)^l_P
+                    const double h2q = 0.5 / q;
+                    cq = coefs[P.coef + ti];
+#pragma unroll
+                    for (int k = 0; k < LP; ++k) cq *= h2q;
+                    if (LP & 1) cq = -cq;
+                }
+                const double* s = pd + (int64_t)pp * PL::STRIDE;
                 const double p = s[0];
-                const double alpha = p * q / (p + q);
-                double R[ntet(L)];
-                hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, R);
-                const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * cq;
+                const double inv_pq = 1.0 / (p + q);
+                const double alpha = p * q * inv_pq;
+                double* row = sR + (slot * TPR + mp) * RS;
+                if constexpr (L <= 4) {
+                    double Rr[NR];
+                    hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, Rr);
+#pragma unroll
+                    for (int e = 0; e < NR; ++e) row[e] = Rr[e];
+                } else {
+                    hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, row);
+                }
+                // 2 pi^(5/2) / (p q sqrt(p + q)) c_P (2q)^-l_P (-1)^l_P
+                row[NR] = kTwoPi52 * sqrt(inv_pq) / (p * q) * cq;
+                tpp += TPR;
+                while (tpp >= npp) {
+                    tpp -= npp;
+                    ++ti;
+                }
+            }
+            s_tp[slot * TPR + mp] = pp;
+        }
+        __syncwarp();
+        if (active) {
+#pragma unroll 1
+            for (int j = 0; j < TPR; ++j) {
+                const int pj = s_tp[slot * TPR + j];
+                if (pj < 0) break;
+                const double* row = sR + (slot * TPR + j) * RS;
+                const double pref = row[NR];
+                const double* s = pd + (int64_t)pj * PL::STRIDE;
                 // exchange weight of this primitive pair: w[m] = sum_k cc[k] gk[k][m]
                 double w[PL::NSAB];
 #pragma unroll
@@ -342,21 +440,21 @@ __global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTa
                 const double* ea = s + PL::OFF_EA;
                 const double* ej = s + PL::OFF_EJ;
                 const double* eja = s + PL::OFF_EJA;
-                // auxiliary centre: -sum_c crow[c] R[h + c + e_d], formed as it is used
+                // auxiliary centre: -sum_c w_c R[h + c + e_d], formed as it is used
 #pragma unroll 1
-                for (int h = 0; h < PL::NH; ++h) {
-                    const int tu = c_tet_t[h], uu = c_tet_u[h], vu = c_tet_v[h];
+                for (int h = 0; h < NH; ++h) {
                     double gx = 0.0, gy = 0.0, gz = 0.0;
 #pragma unroll 1
-                    for (int c = 0; c < NCP; ++c) {
-                        const int t0 = tu + c_cart[LP][c][0], u0 = uu + c_cart[LP][c][1], v0 = vu + c_cart[LP][c][2];
-                        gx += crow[c] * R[tet(t0 + 1, u0, v0)];
-                        gy += crow[c] * R[tet(t0, u0 + 1, v0)];
-                        gz += crow[c] * R[tet(t0, u0, v0 + 1)];
+                    for (int k = 0; k < nnz; ++k) {
+                        const int* ix = s_idx3 + (nzc[k] * NH + h) * 3;
+                        const double wc = nzw[k];
+                        gx += wc * row[ix[0]];
+                        gy += wc * row[ix[1]];
+                        gz += wc * row[ix[2]];
                     }
                     double wk = 0.0;
 #pragma unroll
-                    for (int m = 0; m < PL::NSAB; ++m) wk += w[m] * et[m * PL::NH + h];
+                    for (int m = 0; m < PL::NSAB; ++m) wk += w[m] * et[m * NH + h];
                     const double wj = pref * ej[h];
                     wk *= pref;
                     acc[0] -= wj * gx;
@@ -366,26 +464,27 @@ __global__ void __launch_bounds__(kGradThreads) k_three_center_grad(const PairTa
                     acc[4] -= wk * gy;
                     acc[5] -= wk * gz;
                 }
-                // centre of the first orbital function: sum_c crow[c] R[h + c], h up to LAB + 1
+                // centre of the first orbital function: sum_c w_c R[h + c], h up to LAB + 1
 #pragma unroll 1
-                for (int h = 0; h < PL::NH1; ++h) {
-                    const int tu = c_tet_t[h], uu = c_tet_u[h], vu = c_tet_v[h];
+                for (int h = 0; h < NH1; ++h) {
                     double g1 = 0.0;
 #pragma unroll 1
-                    for (int c = 0; c < NCP; ++c)
-                        g1 += crow[c] * R[tet(tu + c_cart[LP][c][0], uu + c_cart[LP][c][1], vu + c_cart[LP][c][2])];
+                    for (int k = 0; k < nnz; ++k) g1 += nzw[k] * row[s_idx1[nzc[k] * NH1 + h]];
                     g1 *= pref;
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         double wk = 0.0;
 #pragma unroll
-                        for (int m = 0; m < PL::NSAB; ++m) wk += w[m] * ea[(d * PL::NSAB + m) * PL::NH1 + h];
-                        acc[6 + d] += eja[d * PL::NH1 + h] * g1;
+                        for (int m = 0; m < PL::NSAB; ++m) wk += w[m] * ea[(d * PL::NSAB + m) * NH1 + h];
+                        acc[6 + d] += eja[d * NH1 + h] * g1;
                         acc[9 + d] += wk * g1;
                     }
                 }
             }
         }
+        __syncwarp();
+    }
+    if (active) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             atomicAdd(gaux + (int64_t)pshell * 6 + d, fac * cP * acc[d]);
@@ -412,23 +511,19 @@ static cudaError_t three_center_grad_one(const PairTask* tasks, int ntasks, int 
                                          const int* alist, int nalist, const double* btable, GradWeights g,
                                          GradPairData pd, double* gorb, double* gaux, cudaStream_t stream) {
     if (ntasks == 0 || nalist == 0) return cudaSuccess;
-    constexpr int SPB = kGradThreads / nsph(LP);
-    const size_t smem = sizeof(double) * (size_t)max_npp * GradPairLayout<LA, LB>::STRIDE;
-    if (smem > 200 * 1024) return cudaErrorInvalidValue;
-    // the attribute covers the dynamic part; the static part (pair list, reduction)
-    // counts against the 48 KB default too
-    if (smem > 40 * 1024) {
+    using SH = GradCenterShape<LA, LB, LP>;
+    (void)max_npp;  // the pair data is read from global memory
+    const size_t smem = sizeof(double) * (size_t)SH::R_DOUBLES;
+    // the attribute covers the dynamic part; the static tables count against
+    // the 48 KB default too
+    if (smem > 32 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_three_center_grad<LA, LB, LP>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    // one slab per CTA: walking several slabs with one CTA (to build the pair
-    // data once) measured slower, the CTAs' costs being too uneven
-    const int nslabs = (nalist + SPB - 1) / SPB;
-    dim3 grid(ntasks, nslabs);
-    k_three_center_grad<LA, LB, LP><<<grid, kGradThreads, smem, stream>>>(tasks, orb, aux, exps, coefs, alist, nalist,
-                                                                         btable, g, pd.offsets, pd.data, pd.npps,
-                                                                         gorb, gaux);
+    dim3 grid(ntasks, (nalist + SH::SPB - 1) / SH::SPB);
+    k_three_center_grad<LA, LB, LP><<<grid, kGradCenterThreads, smem, stream>>>(
+        tasks, orb, aux, exps, coefs, alist, nalist, btable, g, pd.offsets, pd.data, pd.npps, gorb, gaux);
     return cudaGetLastError();
 }
 
