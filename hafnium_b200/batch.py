@@ -297,7 +297,7 @@ BATCH_FIXED_BYTES = 2 << 30  # the K chunk buffer of one batch
 def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-universal-jkfit", *, device: int = 0,
                 options: BatchOptions | None = None, tuner: TileTuner | None = None,
                 memory_fraction: float = 0.6, max_batch: int = 256, keep_densities: bool = False,
-                setup_threads: int = 32, retry_failed: bool = True) -> BatchResult:
+                setup_threads: int = 16, retry_failed: bool = True) -> BatchResult:
     """Converge every molecule's restricted DF-RHF; energies (and, with
     ``keep_densities``, the converged per-spin densities) in input order."""
     torch = _torch()

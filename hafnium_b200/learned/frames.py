@@ -84,24 +84,39 @@ def atom_frames(positions: np.ndarray):
     n = len(pos)
     if n < 3:
         return None
-    frames = []
-    for i in range(n):
-        d = np.linalg.norm(pos - pos[i], axis=1)
-        order = sorted((j for j in range(n) if j != i), key=lambda j: (round(float(d[j]), 6), j))
-        x = (pos[order[0]] - pos[i]) / d[order[0]]
-        frame = None
-        for j in order[1:]:
-            v = pos[j] - pos[i]
-            v = v - (v @ x) * x
-            norm = np.linalg.norm(v)
-            if norm > 0.1 * d[j]:  # more than about 6 degrees off the x axis
-                y = v / norm
-                frame = np.stack([x, y, np.cross(x, y)], axis=1)
-                break
-        if frame is None:
-            return None
-        frames.append(frame)
-    return frames
+    rows = np.arange(n)
+    diff = pos[None, :, :] - pos[:, None, :]  # [i, j] = r_j - r_i
+    dist = np.linalg.norm(diff, axis=2)
+    key = np.round(dist, 6)
+    np.fill_diagonal(key, np.inf)  # the atom itself sorts last
+    # neighbours nearest first, equal distances (to 1e-6 bohr) in atom order
+    order = np.lexsort((np.broadcast_to(rows, (n, n)), key), axis=-1)
+    first = order[:, 0]
+    x = diff[rows, first] / dist[rows, first][:, None]
+    cand = order[:, 1:n - 1]
+    v = diff[rows[:, None], cand]
+    v = v - np.einsum("ijk,ik->ij", v, x)[:, :, None] * x[:, None, :]
+    norm = np.linalg.norm(v, axis=2)
+    off_line = norm > 0.1 * dist[rows[:, None], cand]  # more than about 6 degrees off the x axis
+    if not np.all(off_line.any(axis=1)):
+        return None
+    k = off_line.argmax(axis=1)
+    y = v[rows, k] / norm[rows, k][:, None]
+    return list(np.stack([x, y, np.cross(x, y)], axis=2))
+
+
+def harmonic_rotations(frames, l: int) -> np.ndarray:
+    """``harmonic_rotation`` of many frames at once: [frame, 2l+1, 2l+1]."""
+    frames = np.asarray(frames, dtype=np.float64)
+    if l == 0:
+        return np.ones((len(frames), 1, 1))
+    t = solid_harmonics(l)
+    rng = np.random.default_rng(1234)
+    pts = rng.normal(size=(64, 3))
+    glob = _monomials(pts, l) @ t.T
+    rotated = np.einsum("pk,fkj->fpj", pts, frames).reshape(-1, 3)  # pts @ r for every frame
+    local = (_monomials(rotated, l) @ t.T).reshape(len(frames), 64, -1)
+    return np.einsum("mp,fpn->fmn", np.linalg.pinv(glob), local)
 
 
 def shell_layout(table, atom_index: int):
@@ -112,15 +127,25 @@ def shell_layout(table, atom_index: int):
 
 def ao_rotation(r: np.ndarray, layout) -> np.ndarray:
     """Block-diagonal U over the shells of ``layout`` (list of (l, n_contractions))."""
-    blocks = []
-    for l, k in layout:
-        u = harmonic_rotation(r, l)
-        blocks.extend([u] * k)
-    n = sum(b.shape[0] for b in blocks)
-    out = np.zeros((n, n))
-    at = 0
-    for b in blocks:
-        m = b.shape[0]
-        out[at:at + m, at:at + m] = b
-        at += m
+    return ao_rotations([r], [layout])[0]
+
+
+def ao_rotations(frames, layouts):
+    """``ao_rotation`` of every atom (frame and shell layout), with the rotation
+    of each angular momentum formed for all atoms at once."""
+    lmax = max((l for layout in layouts for l, _ in layout), default=0)
+    per_l = [harmonic_rotations(frames, l) for l in range(lmax + 1)]
+    out = []
+    for a, layout in enumerate(layouts):
+        blocks = []
+        for l, k in layout:
+            blocks.extend([per_l[l][a]] * k)
+        n = sum(b.shape[0] for b in blocks)
+        u = np.zeros((n, n))
+        at = 0
+        for b in blocks:
+            m = b.shape[0]
+            u[at:at + m, at:at + m] = b
+            at += m
+        out.append(u)
     return out

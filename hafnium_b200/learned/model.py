@@ -34,7 +34,7 @@ import pathlib
 
 import numpy as np
 
-from hafnium_b200.learned.frames import ao_rotation, atom_frames, shell_layout
+from hafnium_b200.learned.frames import ao_rotations, atom_frames, shell_layout
 
 R_CUT = 10.0  # bohr, atom-atom
 N_RBF = 16
@@ -73,8 +73,7 @@ def build_graph(molecule, table=None) -> dict | None:
     n = len(pos)
     rot = np.zeros((n, NA_AO, NA_AO))
     nfun = np.zeros(n, dtype=np.int64)
-    for a in range(n):
-        u = ao_rotation(frames[a], shell_layout(table, a))
+    for a, u in enumerate(ao_rotations(frames, [shell_layout(table, a) for a in range(n)])):
         if u.shape[0] > NA_AO:
             return None
         nfun[a] = u.shape[0]
@@ -378,10 +377,40 @@ def load_weights(path: pathlib.Path = WEIGHTS):
     return arrays, mean_diag, meta
 
 
-def predict_density(molecule, weights=None, device: int = 0):
-    """The network's per-spin density of a molecule in cc-pVDZ, or None (fall
-    back to SAD): no weights, an element the network was not trained on, or an
-    atom without a frame."""
+def assemble_density(graph: dict, d_blocks, o_blocks, mean_diag: np.ndarray, device):
+    """``blocks_to_density`` on the device: the network's blocks (torch tensors)
+    to the global per-spin density, FP64, as a torch tensor on ``device``."""
+    import torch
+
+    n = graph["n_nodes"]
+    f64 = dict(dtype=torch.float64, device=device)
+    elem = torch.as_tensor(graph["elem"], dtype=torch.long, device=device)
+    iu0 = torch.as_tensor(_IU[0], dtype=torch.long, device=device)
+    iu1 = torch.as_tensor(_IU[1], dtype=torch.long, device=device)
+    diag = torch.zeros((n, NA_AO, NA_AO), **f64)
+    diag[:, iu0, iu1] = d_blocks.to(torch.float64) + torch.as_tensor(mean_diag, **f64)[elem]
+    diag = diag + torch.triu(diag, 1).transpose(1, 2)
+    # dl[i][j] = the (i, j) block in the frames of atoms i and j
+    dl = torch.zeros((n, n, NA_AO, NA_AO), **f64)
+    idx = torch.arange(n, device=device)
+    dl[idx, idx] = diag
+    src = torch.as_tensor(graph["src"], dtype=torch.long, device=device)
+    dst = torch.as_tensor(graph["dst"], dtype=torch.long, device=device)
+    o = o_blocks.to(torch.float64).reshape(-1, NA_AO, NA_AO)
+    dl.index_put_((src, dst), 0.5 * o, accumulate=True)
+    dl.index_put_((dst, src), 0.5 * o.transpose(1, 2), accumulate=True)
+    rot = torch.as_tensor(graph["rot"], **f64)
+    dp = torch.einsum("iab,ijbc,jdc->ijad", rot, dl, rot)
+    atom, local = _padded_index(graph)
+    atom = torch.as_tensor(atom, dtype=torch.long, device=device)
+    local = torch.as_tensor(local, dtype=torch.long, device=device)
+    return dp[atom[:, None], atom[None, :], local[:, None], local[None, :]]
+
+
+def predict_density(molecule, weights=None, device: int = 0, table=None):
+    """The network's per-spin density of a molecule in cc-pVDZ (a torch FP64
+    tensor on the device), or None (fall back to SAD): no weights, an element
+    the network was not trained on, or an atom without a frame."""
     loaded = load_weights() if weights is None else weights
     if loaded is None:
         return None
@@ -389,11 +418,9 @@ def predict_density(molecule, weights=None, device: int = 0):
     trained = set(meta.get("elements", ()))
     if any(s.capitalize() not in trained for s in molecule.symbols):
         return None
-    graph = build_graph(molecule)
+    graph = build_graph(molecule, table)
     if graph is None:
         return None
     net = DeviceNet(params, device=device)
     out, _ = net.forward(net.upload_graph(graph))
-    d = out["d"].double().cpu().numpy()
-    o = out["o"].double().cpu().numpy()
-    return blocks_to_density(graph, d, o, mean_diag)
+    return assemble_density(graph, out["d"], out["o"], mean_diag, net.dev)

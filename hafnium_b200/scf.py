@@ -345,7 +345,7 @@ def learned_density_guess(molecule, ham: DeviceHamiltonian, *, weights=None, bas
     from hafnium_b200.learned.model import predict_density
 
     predicted = predict_density(molecule, weights, device=device) if basis == "cc-pvdz" else None
-    if predicted is None or not np.all(np.isfinite(predicted)):
+    if predicted is None or not bool(_torch().isfinite(predicted).all()):
         return atomic_density_guess(molecule, basis, device=device)
     return project_occupied(ham, predicted)
 

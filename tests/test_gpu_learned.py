@@ -47,3 +47,20 @@ def test_trained_network_beats_the_sad_guess():
     r_ml = solve_rhf(ham, guess=learned_density_guess(mol, ham, weights=weights))
     assert abs(r_ml.energy - r_sad.energy) <= 1e-8
     assert r_ml.n_iterations < r_sad.n_iterations
+
+
+def test_device_assembly_matches_the_host_blocks():
+    """The predicted blocks become the same global density on the device as on the host."""
+    import torch
+
+    from hafnium_b200.molecule import water_cluster
+
+    g = M.build_graph(water_cluster(6, 11))
+    rng = np.random.default_rng(8)
+    d = rng.normal(size=(g["n_nodes"], M.DIAG))
+    o = rng.normal(size=(len(g["src"]), M.OFF))
+    mean = rng.normal(size=(len(M.ELEMENTS), M.DIAG))
+    want = M.blocks_to_density(g, d, o, mean)
+    dev = torch.device("cuda", 0)
+    got = M.assemble_density(g, torch.as_tensor(d, device=dev), torch.as_tensor(o, device=dev), mean, dev)
+    np.testing.assert_allclose(got.cpu().numpy(), want, atol=1e-13)
