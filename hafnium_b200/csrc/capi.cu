@@ -8,6 +8,7 @@
 #include <future>
 #include <mutex>
 #include <thread>
+#include <unordered_set>
 #include <string>
 #include <vector>
 
@@ -48,6 +49,7 @@ struct ScheduleState {
 
 struct hf_ctx {
     int device = 0;
+    std::unordered_set<void*> pooled;  // blocks from the stream-ordered pool (freed with cudaFreeAsync)
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     std::string err;
@@ -116,15 +118,19 @@ bool holds_all_rows(const hf_ctx* c) { return c->row0 == 0 && fitted_rows(c) == 
                         std::string(#call) + ": " + cudaGetErrorString(_e));                  \
     } while (0)
 
-// Device memory that a context keeps. Blocks below kRetainMinBytes (shell
-// tables, the metric, small scratch) come from the device's stream-ordered
-// pool (cudaMallocAsync on the context's stream, then that stream is waited
-// for, so the block can be used anywhere at once): unlike cudaMalloc and
-// cudaFree, which may synchronise the whole device, the pool serves them
-// without a device-wide synchronisation, which matters when many contexts are
-// built at once (the batched SCF's clusters). Larger blocks are cudaMalloc'd
-// (and retained, below). cudaFree releases both kinds; every caller frees a
-// block only after the work that used it has completed.
+// Device memory that a context keeps. Blocks below kPoolMaxBytes (shell
+// tables, the metric, small scratch) come from the device's stream-ordered pool
+// (cudaMallocAsync on the context's stream, then that stream is waited for, so
+// the block can be used anywhere at once) and go back to it with cudaFreeAsync
+// on that stream: unlike cudaMalloc and cudaFree, which may synchronise the
+// whole device, neither waits for the work of other streams, which matters when
+// many contexts are built and destroyed at once (the batched SCF's clusters,
+// built on several host threads). Larger blocks are cudaMalloc'd (and
+// retained, below) and freed with cudaFree: served from the pool, blocks of
+// gigabytes were mapped afresh whenever a synchronisation trimmed the pool to
+// its release threshold (a batched setup of 128 clusters took 11 s instead of
+// 1.6 s). Every caller frees a block only after the work that used it on other
+// streams has completed.
 constexpr size_t kPoolMaxBytes = (size_t)256 << 20;
 int alloc(hf_ctx* ctx, void** p, size_t bytes) {
     ctx->stats.device_allocations++;
@@ -133,7 +139,9 @@ int alloc(hf_ctx* ctx, void** p, size_t bytes) {
     if (size < kPoolMaxBytes && ctx->stream) {
         e = cudaMallocAsync(p, size, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-        if (e != cudaSuccess) {
+        if (e == cudaSuccess) {
+            ctx->pooled.insert(*p);
+        } else {
             if (*p) cudaFree(*p);
             *p = nullptr;
             cudaGetLastError();
@@ -149,9 +157,18 @@ int alloc(hf_ctx* ctx, void** p, size_t bytes) {
     return HF_OK;
 }
 
+// Free a block of alloc(): stream-ordered for pool blocks, cudaFree otherwise.
+void free_block(hf_ctx* ctx, void* q) {
+    if (!q) return;
+    if (ctx->pooled.erase(q) && ctx->stream)
+        cudaFreeAsync(q, ctx->stream);
+    else
+        cudaFree(q);
+}
+
 template <class T>
-void release(T*& p) {
-    if (p) cudaFree((void*)p);
+void release(hf_ctx* ctx, T*& p) {
+    free_block(ctx, (void*)p);
     p = nullptr;
 }
 
@@ -159,8 +176,8 @@ void release(T*& p) {
 void schedule_release(hf_ctx* ctx) {
     ScheduleState& st = ctx->sched;
     for (double** q : {&st.prev, &st.anchor_d, &st.anchor_k, &st.anchor_ft, &st.dens, &st.ft, &st.overlap, &st.scalar})
-        release(*q);
-    for (auto& q : st.work) release(q);
+        release(ctx, *q);
+    for (auto& q : st.work) release(ctx, q);
     st = ScheduleState{};
 }
 
@@ -203,7 +220,7 @@ const double* shared_boys_table(int device) {
 // synchronises the device, is avoided. At most kRetainBlocks blocks are kept
 // per device; a failed allocation empties the cache and retries;
 // hf_release_retained frees it on request.
-constexpr size_t kRetainMinBytes = (size_t)256 << 20;
+constexpr size_t kRetainMinBytes = kPoolMaxBytes;  // smaller blocks come from the pool
 constexpr int kRetainBlocks = 8;
 constexpr int kRetainDevices = 64;
 struct Retained {
@@ -262,7 +279,7 @@ void big_release(hf_ctx* ctx, T*& p, size_t& have) {
     const size_t bytes = have;
     have = 0;
     if (bytes < kRetainMinBytes || ctx->device < 0 || ctx->device >= kRetainDevices) {
-        cudaFree(q);
+        free_block(ctx, q);
         return;
     }
     // the block may still be read by work queued on this context's stream
@@ -625,11 +642,11 @@ int hf_ctx_create(int device, hf_ctx** out) {
 }
 
 static void free_shells(hf_ctx* ctx) {
-    release(ctx->d_orb);
-    release(ctx->d_aux);
-    release(ctx->d_exps);
-    release(ctx->d_coefs);
-    for (auto& p : ctx->d_aux_by_l) release(p);
+    release(ctx, ctx->d_orb);
+    release(ctx, ctx->d_aux);
+    release(ctx, ctx->d_exps);
+    release(ctx, ctx->d_coefs);
+    for (auto& p : ctx->d_aux_by_l) release(ctx, p);
 }
 
 int hf_ctx_destroy(hf_ctx* ctx) {
@@ -637,7 +654,7 @@ int hf_ctx_destroy(hf_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_shells(ctx);
-    release(ctx->d_metric);
+    release(ctx, ctx->d_metric);
     big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
     big_release(ctx, ctx->d_work, ctx->work_bytes);
     big_release(ctx, ctx->d_io, ctx->io_bytes);
@@ -647,8 +664,8 @@ int hf_ctx_destroy(hf_ctx* ctx) {
     big_release(ctx, ctx->d_tcwork, ctx->tcwork_bytes);
     big_release(ctx, ctx->d_ctc, ctx->ctc_bytes);
     schedule_release(ctx);
-    release(ctx->d_info);
-    release(ctx->d_scalar);
+    release(ctx, ctx->d_info);
+    release(ctx, ctx->d_scalar);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -709,7 +726,7 @@ int hf_shells_upload(hf_ctx* ctx, const hf_shell_table* orbt, const hf_shell_tab
     if (auxt && (s = check_table(ctx, auxt, "auxiliary", kMaxAuxL, true)) != HF_OK) return s;
     free_shells(ctx);
     big_release(ctx, ctx->d_B, ctx->b_alloc_bytes);
-    release(ctx->d_metric);
+    release(ctx, ctx->d_metric);
     big_release(ctx, ctx->d_bf16_b, ctx->bf16_alloc_bytes);
     ctx->built = false;
     ctx->row0 = 0;
@@ -1509,7 +1526,7 @@ int hf_three_center(hf_ctx* ctx, double* out) {
     const size_t ns = ctx->orb.size(), task_cap = ns * (ns + 1) / 2 + 16;
     if (alloc(ctx, (void**)&T, sizeof(double) * (size_t)ncols * N) ||
         alloc(ctx, (void**)&d_tasks, sizeof(PairTask) * task_cap)) {
-        release(T);
+        release(ctx, T);
         return HF_ERR_OOM;
     }
     HF_CU(cudaMemsetAsync(T, 0, sizeof(double) * (size_t)ncols * N, ctx->stream));
@@ -1519,8 +1536,8 @@ int hf_three_center(hf_ctx* ctx, double* out) {
         h.resize((size_t)ncols * N);
         cudaMemcpy(h.data(), T, sizeof(double) * h.size(), cudaMemcpyDeviceToHost);
     }
-    release(T);
-    release(d_tasks);
+    release(ctx, T);
+    release(ctx, d_tasks);
     if (s != HF_OK) return s;
     for (int mu = 0; mu < n; ++mu)
         for (int nu = 0; nu < n; ++nu) {
@@ -1627,7 +1644,7 @@ int hf_four_center(hf_ctx* ctx, double* out, int on_device) {
     ++ctx->stats.kernel_launches;
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess && !on_device) e = cudaMemcpy(out, tmp, bytes, cudaMemcpyDeviceToHost);
-    release(tmp);
+    release(ctx, tmp);
     if (e != cudaSuccess) return fail(ctx, HF_ERR_CUDA, std::string("four-centre: ") + cudaGetErrorString(e));
     return HF_OK;
 }

@@ -377,24 +377,28 @@ __device__ int pair_prologue(const DevShell& A, const DevShell& B, const double*
 }
 
 // Shapes of one (P|mu nu) class. The threads of an auxiliary shell (one per
-// m_P) share each primitive triple's R table: per round, TPR of them each
-// evaluate the Boys function and R table of one triple into shared memory, and
-// after a barrier every thread contracts all TPR tables with its own m_P row of
-// the Cartesian-to-spherical matrix. TPR is NSP unless the tables would pass
-// kRTableBytes (the high classes, whose tables hold up to 165 entries).
+// m_P, all in one warp) share each primitive triple's R table: per round, TPR
+// of them each evaluate the Boys function and R table of one triple into
+// shared memory, and after a warp barrier every thread contracts all TPR tables
+// with its own m_P row of the Cartesian-to-spherical matrix. TPR is NSP unless
+// the tables would pass kRTableBytes (the high classes, whose tables hold up to
+// 165 entries). For l_P = 0 each shell has one thread, which keeps its table in
+// registers.
 constexpr int kRTableBytes = 48 * 1024;
 template <int LA, int LB, int LP>
 struct ThreeCenterShape {
     static constexpr int L = LA + LB + LP;
-    static constexpr int NCP = ncart(LP), NSP = nsph(LP), SPB = 128 / NSP;
+    static constexpr int NCP = ncart(LP), NSP = nsph(LP);
+    static constexpr int SPW = 32 / NSP;  // auxiliary shells per warp
+    static constexpr int SPB = 4 * SPW;   // ... per 128-thread CTA
     static constexpr int NH = ntet(LA + LB);
     static constexpr int NR = ntet(L);
     // the table and its prefactor, padded to an odd count of doubles so that
     // rows of consecutive threads fall in different banks
     static constexpr int RS = (NR + 1) | 1;
     static constexpr int FIT = kRTableBytes / (SPB * RS * 8);
-    static constexpr int TPR = FIT < 1 ? 1 : (FIT > NSP ? NSP : FIT);
-    static constexpr int R_DOUBLES = SPB * TPR * RS;
+    static constexpr int TPR = NSP == 1 ? 1 : (FIT < 1 ? 1 : (FIT > NSP ? NSP : FIT));
+    static constexpr int R_DOUBLES = NSP == 1 ? 0 : SPB * TPR * RS;
 };
 
 // One CTA per orbital shell pair of class (LA <= LB) and a slab of SPB auxiliary
@@ -413,7 +417,7 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
                                                       int r_offset, double* __restrict__ T) {
     using PL = PairLayout<LA, LB>;
     using SH = ThreeCenterShape<LA, LB, LP>;
-    constexpr int L = SH::L, NCP = SH::NCP, NSP = SH::NSP, SPB = SH::SPB, NH = SH::NH, TPR = SH::TPR;
+    constexpr int L = SH::L, NCP = SH::NCP, NSP = SH::NSP, SPW = SH::SPW, NH = SH::NH, TPR = SH::TPR;
     constexpr int RS = SH::RS, NR = SH::NR;
     extern __shared__ double smem[];
     __shared__ int s_pos[2 * kMaxPrimPairs + 1];
@@ -421,8 +425,7 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
     __shared__ int s_nzc[NSP * NCP];     // per m_P: the Cartesian components with a nonzero weight
     __shared__ double s_nzw[NSP * NCP];  // ... and the weights
     __shared__ int s_nnz[NSP];
-    __shared__ int s_tp[SPB * TPR];      // primitive pair of each table of the round, -1 past the end
-    __shared__ int s_rounds;
+    __shared__ int s_tp[SH::SPB * TPR];  // primitive pair of each table of the round, -1 past the end
     double* sR = smem + r_offset;
 
     for (int e = threadIdx.x; e < NCP * NH; e += blockDim.x) {
@@ -441,7 +444,6 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
         }
         s_nnz[threadIdx.x] = k;
     }
-    if (threadIdx.x == 0) s_rounds = 0;
 
     const PairTask task = tasks[blockIdx.x];
     const DevShell A = orb[task.swap ? task.second : task.first];
@@ -449,19 +451,20 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
     const int npp = pair_prologue<LA, LB>(A, B, exps, coefs, smem, s_pos);  // ends with a barrier
     if (npp == 0) return;  // the same for the whole CTA; the chunk was zeroed
 
-    const int slot = threadIdx.x / NSP, mp = threadIdx.x - slot * NSP;
-    const int ia = blockIdx.y * SPB + slot;
-    const bool active = slot < SPB && ia < nalist;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wslot = lane / NSP, mp = lane - wslot * NSP;
+    const int slot = warp * SPW + wslot;
+    const int ia = blockIdx.y * SH::SPB + slot;
+    const bool active = wslot < SPW && ia < nalist;
     DevShell P{};
     int ntrip = 0;
     if (active) {
         P = aux[alist[ia]];
         ntrip = P.nprim * npp;
-        if (mp == 0) atomicMax(&s_rounds, (ntrip + TPR - 1) / TPR);
     }
-    __syncthreads();
-    const int rounds = s_rounds;
-    const int nnz = s_nnz[mp < NSP ? mp : 0];
+    // rounds of this warp: its slowest shell's triples over TPR
+    const int rounds = __reduce_max_sync(0xffffffffu, (ntrip + TPR - 1) / TPR);
+    const int nnz = s_nnz[active ? mp : 0];
 
     double acc[PL::KK][PL::NSAB];
 #pragma unroll
@@ -469,72 +472,107 @@ __global__ void __launch_bounds__(128) k_three_center(const PairTask* __restrict
 #pragma unroll
         for (int m = 0; m < PL::NSAB; ++m) acc[k][m] = 0.0;
 
+    // this thread's triple t = r TPR + mp as (auxiliary primitive i, primitive pair pp),
+    // advanced by TPR per round; the auxiliary primitive's factors are kept while i stays
+    int ti = mp / npp, tpp = mp - (mp / npp) * npp;
+    int ci = -1;
+    double q = 0.0, cq = 0.0;
     for (int r = 0; r < rounds; ++r) {
-        if (active && mp < TPR) {
-            const int t = r * TPR + mp;
-            int pp = -1;
-            if (t < ntrip) {
-                const int i = t / npp;
-                pp = t - i * npp;
-                const double q = exps[P.prim + i];
+        int pp = -1;
+        double R[NSP == 1 ? NR : 1];
+        if (active && mp < TPR && ti < P.nprim) {
+            pp = tpp;
+            if (ti != ci) {
+                ci = ti;
+                q = exps[P.prim + ti];
                 const double inv_q = 1.0 / q;
                 // c_P (2q)^-l_P (-1)^l_P 2 pi^(5/2) / q
-                double cq = coefs[P.coef + i] * kTwoPi52 * inv_q;
+                cq = coefs[P.coef + ti] * kTwoPi52 * inv_q;
                 const double h2q = 0.5 * inv_q;
 #pragma unroll
                 for (int k = 0; k < LP; ++k) cq *= h2q;
                 if (LP & 1) cq = -cq;
-                const double* s = smem + pp * PL::STRIDE;
-                const double p = s[0];
-                // one division per primitive triple: 1/(p+q) gives both the reduced
-                // exponent and the prefactor 2 pi^(5/2) / (p q sqrt(p+q))
-                const double inv_pq = 1.0 / (p + q);
-                const double alpha = p * q * inv_pq;
+            }
+            const double* s = smem + pp * PL::STRIDE;
+            const double p = s[0];
+            // one division per primitive triple: 1/(p+q) gives both the reduced
+            // exponent and the prefactor 2 pi^(5/2) / (p q sqrt(p+q))
+            const double inv_pq = 1.0 / (p + q);
+            const double alpha = p * q * inv_pq;
+            const double pref = s[4] * sqrt(inv_pq) * cq;
+            if constexpr (NSP == 1) {
+                hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, R);
+                const double scale = pref * c_c2s[c2s_offset(LP)];  // the single weight of l_P = 0
+#pragma unroll
+                for (int e = 0; e < NR; ++e) R[e] *= scale;
+            } else {
                 double* row = sR + (slot * TPR + mp) * RS;
                 if constexpr (L <= 4) {
-                    double R[NR];
-                    hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, R);
+                    double Rr[NR];
+                    hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, Rr);
 #pragma unroll
-                    for (int e = 0; e < NR; ++e) row[e] = R[e];
+                    for (int e = 0; e < NR; ++e) row[e] = Rr[e];
                 } else {
                     hermite_r<L>(alpha, s[1] - P.x, s[2] - P.y, s[3] - P.z, btable, row);
                 }
-                row[NR] = s[4] * sqrt(inv_pq) * cq;
+                row[NR] = pref;
             }
-            s_tp[slot * TPR + mp] = pp;
+            tpp += TPR;
+            while (tpp >= npp) {
+                tpp -= npp;
+                ++ti;
+            }
         }
-        if constexpr (NSP > 1) __syncthreads();
-        if (active) {
-#pragma unroll 1
-            for (int j = 0; j < TPR; ++j) {
-                const int pp = s_tp[slot * TPR + j];
-                if (pp < 0) break;
-                const double* row = sR + (slot * TPR + j) * RS;
-                double G[NH];
-#pragma unroll
-                for (int h = 0; h < NH; ++h) G[h] = 0.0;
-#pragma unroll 1
-                for (int k = 0; k < nnz; ++k) {
-                    const int* ix = s_idx + s_nzc[mp * NCP + k] * NH;
-                    const double w = s_nzw[mp * NCP + k];
-#pragma unroll
-                    for (int h = 0; h < NH; ++h) G[h] += w * row[ix[h]];
-                }
-                const double pref = row[NR];
+        if constexpr (NSP == 1) {
+            // l_P = 0: one thread per shell, the table (weight and prefactor
+            // applied) in registers
+            if (pp >= 0) {
                 const double* s = smem + pp * PL::STRIDE;
                 const double* et = s + PL::ET;
 #pragma unroll
                 for (int m = 0; m < PL::NSAB; ++m) {
                     double val = 0.0;
 #pragma unroll
-                    for (int h = 0; h < NH; ++h) val += et[m * NH + h] * G[h];
-                    val *= pref;
+                    for (int h = 0; h < NH; ++h) val += et[m * NH + h] * R[h];
 #pragma unroll
                     for (int k = 0; k < PL::KK; ++k) acc[k][m] += s[PL::CC + k] * val;
                 }
             }
+        } else {
+            if (active && mp < TPR) s_tp[slot * TPR + mp] = pp;
+            __syncwarp();
+            if (active) {
+#pragma unroll 1
+                for (int j = 0; j < TPR; ++j) {
+                    const int pj = s_tp[slot * TPR + j];
+                    if (pj < 0) break;
+                    const double* row = sR + (slot * TPR + j) * RS;
+                    double G[NH];
+#pragma unroll
+                    for (int h = 0; h < NH; ++h) G[h] = 0.0;
+#pragma unroll 1
+                    for (int k = 0; k < nnz; ++k) {
+                        const int* ix = s_idx + s_nzc[mp * NCP + k] * NH;
+                        const double w = s_nzw[mp * NCP + k];
+#pragma unroll
+                        for (int h = 0; h < NH; ++h) G[h] += w * row[ix[h]];
+                    }
+                    const double pref = row[NR];
+                    const double* s = smem + pj * PL::STRIDE;
+                    const double* et = s + PL::ET;
+#pragma unroll
+                    for (int m = 0; m < PL::NSAB; ++m) {
+                        double val = 0.0;
+#pragma unroll
+                        for (int h = 0; h < NH; ++h) val += et[m * NH + h] * G[h];
+                        val *= pref;
+#pragma unroll
+                        for (int k = 0; k < PL::KK; ++k) acc[k][m] += s[PL::CC + k] * val;
+                    }
+                }
+            }
+            __syncwarp();
         }
-        if constexpr (NSP > 1) __syncthreads();
     }
     if (!active) return;
 
@@ -590,7 +628,7 @@ static cudaError_t three_center_one(const PairTask* tasks, int ntasks, int max_n
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    dim3 grid(ntasks, (nalist + SH::SPB - 1) / SH::SPB);
+    dim3 grid(ntasks, (nalist + SH::SPB - 1) / SH::SPB);  // 4 warps of SPW shells
     k_three_center<LA, LB, LP><<<grid, 128, smem, stream>>>(tasks, orb, aux, exps, coefs, alist, nalist, btable,
                                                             chunk, r_offset, T);
     return cudaGetLastError();

@@ -105,8 +105,9 @@ int hf_set_stream(hf_ctx* ctx, void* stream);
  * areas, when at least 256 MiB, are not freed when a context is destroyed or
  * rebuilt: up to eight per device are kept and handed to the next context
  * whose request fits, so a run over many geometries of one size maps them
- * once. A failed allocation empties the cache first. This frees the blocks
- * kept for `device` now. No reference counterpart (the reference holds host
+ * once (smaller blocks come from the device's stream-ordered pool and go back
+ * to it without a device-wide synchronisation). A failed allocation empties
+ * the cache first. This frees the blocks kept for `device` now. No reference counterpart (the reference holds host
  * arrays only). */
 int hf_release_retained(int device);
 

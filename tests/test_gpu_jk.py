@@ -89,9 +89,10 @@ def test_shape_mismatch_raises(system):
 
 
 def test_a_rebuilt_context_takes_the_retained_fitted_tensor_block():
-    """The fitted tensor of (H2O)16 (1.2 GB) is kept when its context closes and
-    handed to the next context of that size, so the second build makes one
-    device allocation fewer and gives the same J."""
+    """The fitted tensor of (H2O)16 (1.2 GB, above the stream-ordered pool's
+    256 MiB) is kept when its context closes and handed to the next context of
+    that size, so the second build makes one device allocation fewer and gives
+    the same J."""
     import torch
 
     from hafnium_b200 import _lib
