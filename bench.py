@@ -102,12 +102,21 @@ class ClockSampler:
         self.proc = None
 
     def start(self) -> None:
+        """Start sampling and return once the first sample is written, so that
+        nvidia-smi's own start-up (NVML initialisation) is over before the timed
+        region begins (at most 5 s)."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
         except Exception:  # noqa: BLE001
             self.proc = None
+            return
+        deadline = time.time() + 5.0
+        while time.time() < deadline and self.proc.poll() is None:
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -272,9 +281,13 @@ def run_b200(args) -> None:
             one_scf(torch, mol, dev, guess_kind=guess_kind, protocol=True)
     if world > 1:
         dist.barrier()
+    import gc
+
+    gc.collect()  # the warm-up's garbage, not the first timed step's
     torch.cuda.synchronize(dev)
     sampler = ClockSampler(local)
     sampler.start()
+
     def timed_region(**kw):
         """K whole SCFs as one timed region (CUDA events, synchronised on both sides,
         a barrier before under torchrun), each step also timed on its own."""
