@@ -1407,7 +1407,8 @@ int hf_density_factor(hf_ctx* ctx, const double* D, double* F, int64_t max_rank,
     const size_t nn = (size_t)n * n;
     const int64_t cap = std::min<int64_t>(max_rank, n);
     Carver cv;
-    const size_t oD = cv.take(nn), oL = cv.take((size_t)cap * n);
+    const size_t oD = cv.take(nn), oL = cv.take((size_t)cap * n),
+                 oW = cv.take(pivoted_cholesky_work_doubles((int)n));
     int st = ensure_scratch(ctx, &ctx->d_stage, &ctx->stage_bytes, sizeof(double) * cv.used);
     if (st != HF_OK) return st;
     double* sD = ctx->d_stage + oD;
@@ -1419,7 +1420,7 @@ int hf_density_factor(hf_ctx* ctx, const double* D, double* F, int64_t max_rank,
     }
     time_begin(ctx);
     HF_CU(cudaMemsetAsync(ctx->d_info, 0, 2 * sizeof(int), ctx->stream));
-    HF_CU(pivoted_cholesky(dD, 0, (int)n, 1e-14, (int)cap, Lc, 0, ctx->d_info, 1, nullptr, ctx->stream));
+    HF_CU(pivoted_cholesky_blocked(dD, (int)n, 1e-14, (int)cap, Lc, ctx->d_info, ctx->d_stage + oW, ctx->stream));
     ++ctx->stats.kernel_launches;
     int res[2] = {0, 0};
     HF_CU(cudaMemcpyAsync(res, ctx->d_info, sizeof(res), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1444,7 +1445,7 @@ int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_d
     const int64_t opad_max = std::max<int64_t>(64, round_up(n, 64));
     Carver cv;
     const size_t oD = cv.take(nn), oL = cv.take(nn), oK = cv.take(nn), oCt = cv.take(opad_max * npad),
-                 osg = cv.take(opad_max);
+                 osg = cv.take(opad_max), oW = cv.take(pivoted_cholesky_work_doubles((int)n));
     int st = ensure_scratch(ctx, &ctx->d_stage, &ctx->stage_bytes, sizeof(double) * cv.used);
     if (st != HF_OK) return st;
     double* buf = ctx->d_stage;
@@ -1458,7 +1459,7 @@ int hf_exchange(hf_ctx* ctx, const double* D, double* K, int precision, int on_d
     }
     time_begin(ctx);
     cudaMemsetAsync(ctx->d_info, 0, 2 * sizeof(int), ctx->stream);
-    HF_CU(pivoted_cholesky(dD, 0, (int)n, 1e-14, (int)n, Lc, 0, ctx->d_info, 1, nullptr, ctx->stream));
+    HF_CU(pivoted_cholesky_blocked(dD, (int)n, 1e-14, (int)n, Lc, ctx->d_info, buf + oW, ctx->stream));
     int res[2] = {0, 0};
     cudaMemcpyAsync(res, ctx->d_info, sizeof(res), cudaMemcpyDeviceToHost, ctx->stream);
     cudaError_t e = cudaStreamSynchronize(ctx->stream);

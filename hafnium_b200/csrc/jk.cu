@@ -178,11 +178,6 @@ static_assert(XBM % 64 == 0 && 64 % XBK == 0, "a k slice stays inside one packed
 
 __device__ __forceinline__ uint32_t xsmem(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
-__device__ __forceinline__ void xcp8(double* dst, const double* src, const double* base, bool valid) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(xsmem(dst)), "l"(valid ? src : base),
-                 "r"(valid ? 8 : 0));
-}
-
 // 16-byte asynchronous copy (both addresses 16-byte aligned); an invalid piece
 // copies nothing and zero-fills.
 __device__ __forceinline__ void xcp16(double* dst, const double* src, const double* base, bool valid) {
@@ -457,6 +452,149 @@ __global__ void __launch_bounds__(1024) k_pivoted_cholesky(const double* __restr
     }
 }
 
+// Blocked pivoted Cholesky of one matrix: the pivots and the factor of
+// k_pivoted_cholesky, with the rows that pivots already taken subtract kept in
+// a working copy W = D - sum L L^T that a DMMA product updates once per panel
+// of kPivotPanel pivots. Within a panel each pivot's column needs W's row and
+// at most kPivotPanel - 1 corrections instead of one per earlier pivot, so the
+// sequential part no longer rereads the whole factor from L2 at every pivot.
+constexpr int kPivotPanel = 32;
+struct PivotState {
+    double dmax0;  // the largest initial diagonal entry
+    int k;         // pivots taken
+    int stop;      // 1 once the remaining diagonal falls below tol dmax0 or k reaches maxr
+    int active;    // the trailing update of this panel has work (DMMA batch flag)
+    int pad;
+};
+
+__device__ __forceinline__ void block_argmax(double best, int bi, double* rv, int* ri, double& out_best,
+                                             int& out_i) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) {
+            best = ob;
+            bi = oi;
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        rv[threadIdx.x >> 5] = best;
+        ri[threadIdx.x >> 5] = bi;
+    }
+    __syncthreads();
+    double b = -1.0;
+    int p = -1;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w)
+        if (rv[w] > b || (rv[w] == b && ri[w] >= 0 && (p < 0 || ri[w] < p))) {
+            b = rv[w];
+            p = ri[w];
+        }
+    out_best = b;
+    out_i = p;
+}
+
+__global__ void __launch_bounds__(1024) k_pc_init(const double* __restrict__ D, int n, double* __restrict__ d,
+                                                  unsigned char* __restrict__ used, PivotState* st) {
+    __shared__ double rv[32];
+    __shared__ int ri[32];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        d[i] = D[(int64_t)i * n + i];
+        used[i] = 0;
+        m = fmax(m, fabs(d[i]));
+    }
+    double b;
+    int unused_i;
+    block_argmax(m, (int)threadIdx.x, rv, ri, b, unused_i);
+    if (threadIdx.x == 0) {
+        st->dmax0 = b;
+        st->k = 0;
+        st->stop = n > 0 ? 0 : 1;
+        st->active = 0;
+    }
+}
+
+__global__ void __launch_bounds__(512) k_pc_panel(const double* __restrict__ W, int n, double tol, int maxr,
+                                                   double* __restrict__ Lc, double* __restrict__ Lp,
+                                                   double* __restrict__ d, unsigned char* __restrict__ used,
+                                                   PivotState* st) {
+    __shared__ double rv[32];
+    __shared__ int ri[32];
+    __shared__ double s_piv;
+    __shared__ int s_p, s_stop;
+    const int tid = threadIdx.x;
+    const int k0 = st->k;
+    const double dmax0 = st->dmax0;
+    if (st->stop) {
+        if (tid == 0) st->active = 0;
+        return;
+    }
+    const int b = min(kPivotPanel, maxr - k0);
+    int done = 0;
+    for (int j = 0; j < b; ++j) {
+        double best = -1.0;
+        int bi = -1;
+        for (int i = tid; i < n; i += blockDim.x)
+            if (!used[i] && d[i] > best) {
+                best = d[i];
+                bi = i;
+            }
+        double bb;
+        int p;
+        block_argmax(best, bi, rv, ri, bb, p);
+        if (tid == 0) {
+            s_stop = (p < 0 || !(bb > tol * dmax0)) ? 1 : 0;
+            s_p = p;
+            s_piv = s_stop ? 0.0 : sqrt(bb);
+        }
+        __syncthreads();
+        if (s_stop) break;
+        const int pv = s_p;
+        const double piv = s_piv;
+        // each thread owns rows i = tid + m blockDim.x: it alone writes their column
+        // entries, diagonal and used flag, and alone reads d and used for them in
+        // the next pivot's search, so the two barriers of the search suffice
+        for (int i = tid; i < n; i += blockDim.x) {
+            double l = 0.0;
+            if (i == pv) {
+                l = piv;
+                used[i] = 1;
+            } else if (!used[i]) {
+                double sum = W[(int64_t)pv * n + i];
+                for (int jj = 0; jj < j; ++jj) sum -= Lp[i * kPivotPanel + jj] * Lp[pv * kPivotPanel + jj];
+                l = sum / piv;
+                d[i] -= l * l;
+            }
+            Lc[(int64_t)(k0 + j) * n + i] = l;
+            Lp[i * kPivotPanel + j] = l;
+        }
+        ++done;
+    }
+    __syncthreads();
+    // columns of the panel past its last pivot add nothing to the trailing update
+    for (int e = tid; e < n * kPivotPanel; e += blockDim.x)
+        if (e % kPivotPanel >= done) Lp[e] = 0.0;
+    if (tid == 0) {
+        st->k = k0 + done;
+        st->stop = (done < b || k0 + done >= maxr) ? 1 : 0;
+        st->active = done > 0 ? 1 : 0;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_pc_finish(int n, double tol, const double* __restrict__ d,
+                                                    const unsigned char* __restrict__ used,
+                                                    const PivotState* st, int* __restrict__ out) {
+    // indefinite if a remaining diagonal entry is clearly negative
+    int bad = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (!used[i] && d[i] < -1e3 * tol * st->dmax0) bad = 1;
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) {
+        out[0] = st->k;
+        out[1] = bad;
+    }
+}
+
 // Ct[i][mu] = Lc[i][mu] for i < rank and mu < n (rank = info[2 c]), else 0;
 // sign[i] = 1 when sign is given (single cluster).
 __global__ void k_factor_pad(const double* __restrict__ Lc, int64_t strideL, int64_t n, const int* __restrict__ info,
@@ -626,6 +764,48 @@ cudaError_t pivoted_cholesky(const double* D, int64_t strideD, int n, double tol
     cudaError_t e = jk_configure();
     if (e != cudaSuccess) return e;
     k_pivoted_cholesky<<<count, 1024, smem, stream>>>(D, strideD, n, tol, maxr, Lc, strideL, info, active);
+    return cudaGetLastError();
+}
+
+size_t pivoted_cholesky_work_doubles(int n) {
+    return (size_t)n * n + (size_t)n * kPivotPanel + n + (n + 7) / 8 + 4;
+}
+
+cudaError_t pivoted_cholesky_blocked(const double* D, int n, double tol, int maxr, double* Lc, int* info,
+                                     double* work, cudaStream_t stream) {
+    if (n < 1 || maxr < 1) return cudaErrorInvalidValue;
+    cudaError_t e = jk_configure();
+    if (e != cudaSuccess) return e;
+    double* W = work;
+    double* Lp = W + (size_t)n * n;
+    double* d = Lp + (size_t)n * kPivotPanel;
+    unsigned char* used = reinterpret_cast<unsigned char*>(d + n);
+    PivotState* st = reinterpret_cast<PivotState*>(d + n + (n + 7) / 8);
+    e = cudaMemcpyAsync(W, D, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, stream);
+    if (e != cudaSuccess) return e;
+    k_pc_init<<<1, 1024, 0, stream>>>(D, n, d, used, st);
+    const int panels = (maxr + kPivotPanel - 1) / kPivotPanel;
+    for (int pnl = 0; pnl < panels; ++pnl) {
+        k_pc_panel<<<1, 512, 0, stream>>>(W, n, tol, maxr, Lc, Lp, d, used, st);
+        if (pnl + 1 == panels) break;  // no pivot follows the last panel
+        // W -= Lp Lp^T (skipped, CTA by CTA, once the factorisation has stopped)
+        GemmArgs g{};
+        g.M = g.N = n;
+        g.K = kPivotPanel;
+        g.A = g.B = Lp;
+        g.lda = g.ldb = kPivotPanel;
+        g.C = W;
+        g.ldc = n;
+        g.alpha = -1.0;
+        g.beta = 1.0;
+        g.kmode = 0;
+        g.epi = 0;
+        g.tile = 5;
+        g.active = &st->active;
+        e = dgemm_nt(g, 1, stream);
+        if (e != cudaSuccess) return e;
+    }
+    k_pc_finish<<<1, 1024, 0, stream>>>(n, tol, d, used, st, info);
     return cudaGetLastError();
 }
 

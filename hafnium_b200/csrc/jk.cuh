@@ -62,6 +62,14 @@ int64_t syrk_partial_doubles(int64_t npad, int count);
 cudaError_t pivoted_cholesky(const double* D, int64_t strideD, int n, double tol, int maxr, double* Lc,
                              int64_t strideL, int* info, int count, const int* active, cudaStream_t stream);
 
+// The same factorisation of one matrix, blocked: a working copy of D in `work`
+// (pivoted_cholesky_work_doubles(n) doubles, device) is updated by a DMMA
+// product once per panel of 32 pivots; the pivots and the factor are those of
+// pivoted_cholesky up to rounding. info[0] = rank, info[1] = 1 when indefinite.
+size_t pivoted_cholesky_work_doubles(int n);
+cudaError_t pivoted_cholesky_blocked(const double* D, int n, double tol, int maxr, double* Lc, int* info,
+                                     double* work, cudaStream_t stream);
+
 // Ct[i][mu] = Lc[i][mu] (i < info[2c], mu < n), zero padded to [opad][npad] per
 // cluster; sign[i] = 1 when sign is given.
 cudaError_t factor_pad(const double* Lc, int64_t strideL, int64_t n, const int* info, double* Ct, int64_t strideCt,
