@@ -19,7 +19,11 @@ namespace hf {
 namespace {
 constexpr int NB = 64;
 
-// Factor the nb x nb diagonal block at (k0, k0) in place (lower), unblocked.
+// Factor the nb x nb diagonal block at (k0, k0) in place (lower), unblocked, by
+// 256 threads (a 16 x 16 grid over the trailing triangle). Per column every
+// thread takes the pivot's square root itself, so a column needs two barriers:
+// after its scaling and after the trailing update (during which thread 0 stores
+// the pivot, which no thread reads then).
 __global__ void __launch_bounds__(256) k_potrf_diag(double* A, int64_t lda, int k0, int nb, int* info,
                                                     double* piv_min) {
     __shared__ double a[NB][NB + 1];
@@ -30,23 +34,20 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double* A, int64_t lda, int 
     }
     __syncthreads();
     for (int j = 0; j < nb; ++j) {
+        const double d = a[j][j];
+        const bool bad = !(d > 0.0);
+        const double r = bad ? 1.0 : sqrt(d);
+        for (int i = j + 1 + tid; i < nb; i += blockDim.x) a[i][j] /= r;
+        __syncthreads();
         if (tid == 0) {
-            const double d = a[j][j];
-            if (!(d > 0.0)) {
-                atomicExch(info, k0 + j + 1);
-                a[j][j] = 1.0;
-            } else {
-                a[j][j] = sqrt(d);
-                if (a[j][j] < *piv_min) *piv_min = a[j][j];
-            }
+            if (bad) atomicExch(info, k0 + j + 1);
+            else if (r < *piv_min) *piv_min = r;
+            a[j][j] = r;
         }
-        __syncthreads();
-        for (int i = j + 1 + tid; i < nb; i += blockDim.x) a[i][j] /= a[j][j];
-        __syncthreads();
-        const int rem = nb - j - 1;
-        for (int e = tid; e < rem * rem; e += blockDim.x) {
-            const int i = j + 1 + e / rem, l = j + 1 + e % rem;
-            if (l <= i) a[i][l] -= a[i][j] * a[l][j];
+        // trailing update of the lower triangle, threads as a 16 x 16 grid over (i, l)
+        for (int i = j + 1 + (tid >> 4); i < nb; i += 16) {
+            const double aij = a[i][j];
+            for (int l = j + 1 + (tid & 15); l <= i; l += 16) a[i][l] -= aij * a[l][j];
         }
         __syncthreads();
     }
@@ -56,12 +57,16 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double* A, int64_t lda, int 
     }
 }
 
-// Rows below the diagonal block: L_ik = A_ik L_kk^{-T}, one thread per row.
+// Rows below the diagonal block: L_ik = A_ik L_kk^{-T}, one thread per row, by
+// forward substitution in right-looking order: once x[q] is known it is
+// subtracted from every later entry, so the 64 entries' updates are independent
+// of one another (the same operations, in the same order per entry, as summing
+// each entry's terms before its division).
 __global__ void __launch_bounds__(128) k_trsm_panel(double* A, int64_t lda, int k0, int nb, int n) {
     __shared__ double l[NB][NB + 1];
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-        const int i = e / nb, j = e % nb;
-        l[i][j] = A[(int64_t)(k0 + i) * lda + k0 + j];
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+        const int i = e / NB, j = e % NB;
+        l[i][j] = (i < nb && j < nb) ? A[(int64_t)(k0 + i) * lda + k0 + j] : 0.0;
     }
     __syncthreads();
     const int row = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
@@ -69,12 +74,13 @@ __global__ void __launch_bounds__(128) k_trsm_panel(double* A, int64_t lda, int 
     double* r = A + (int64_t)row * lda + k0;
     double x[NB];
 #pragma unroll
-    for (int j = 0; j < NB; ++j) {
-        if (j < nb) {
-            double s = r[j];
+    for (int j = 0; j < NB; ++j) x[j] = (j < nb) ? r[j] : 0.0;
 #pragma unroll
-            for (int q = 0; q < j; ++q) s -= x[q] * l[j][q];
-            x[j] = s / l[j][j];
+    for (int q = 0; q < NB; ++q) {
+        if (q < nb) {
+            x[q] = x[q] / l[q][q];
+#pragma unroll
+            for (int j = q + 1; j < NB; ++j) x[j] -= x[q] * l[j][q];
         }
     }
 #pragma unroll
@@ -89,10 +95,13 @@ __global__ void k_zero_upper(double* A, int64_t lda, int n) {
     if (j > i) A[(int64_t)i * lda + j] = 0.0;
 }
 
-// Inverse of the lower-triangular diagonal block at (k0, k0); one thread per
-// column, forward substitution. Writes Linv (row-major) and LinvT.
-__global__ void __launch_bounds__(64) k_trtri_diag(const double* L, int64_t ld, int k0, int nb, double* Linv,
+// Inverse of the lower-triangular diagonal blocks (k0, k0), k0 = 64 blockIdx.x,
+// all at once (they are independent): one CTA per block, one thread per column,
+// forward substitution. Writes Linv (row-major) and LinvT.
+__global__ void __launch_bounds__(64) k_trtri_diag(const double* L, int64_t ld, int n, double* Linv,
                                                    double* LinvT) {
+    const int k0 = blockIdx.x * NB;
+    const int nb = (n - k0 < NB) ? n - k0 : NB;
     __shared__ double l[NB][NB + 1];
     for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
         const int i = e / nb, j = e % nb;
@@ -171,10 +180,7 @@ cudaError_t triangular_inverse(const double* L, int n, int64_t ld, double* Linv,
                                cudaStream_t stream) {
     cudaMemsetAsync(Linv, 0, sizeof(double) * (size_t)n * ld, stream);
     cudaMemsetAsync(LinvT, 0, sizeof(double) * (size_t)n * ld, stream);
-    for (int k0 = 0; k0 < n; k0 += NB) {
-        const int nb = (n - k0 < NB) ? n - k0 : NB;
-        k_trtri_diag<<<1, 64, 0, stream>>>(L, ld, k0, nb, Linv, LinvT);
-    }
+    k_trtri_diag<<<(n + NB - 1) / NB, 64, 0, stream>>>(L, ld, n, Linv, LinvT);
     for (int k0 = NB; k0 < n; k0 += NB) {
         const int nb = (n - k0 < NB) ? n - k0 : NB;
         // Wt[c][m] = sum_{k in [c, k0)} L[k0 + m][k] Linv[k][c]   (c < k0)
