@@ -67,6 +67,28 @@ class Shell:
 
 
 @functools.lru_cache(maxsize=None)
+def _element_block(name: str, z: int):
+    """One atom's part of a ShellTable for element z in basis ``name``: angular
+    momenta, primitives per shell, exponents, normalised coefficients (each
+    shell's contractions one after another) and contractions per shell; None
+    when the basis has no functions for z. Computed once per basis and element."""
+    shells = element_shells(name).get(z)
+    if not shells:
+        return None
+    ls, nprim, exps, coefs, ks = [], [], [], [], []
+    for shell in shells:
+        rows = shell.primitive_coefficients()
+        ls.append(shell.l)
+        nprim.append(len(shell.exponents))
+        exps.extend(shell.exponents)
+        for row in rows:
+            coefs.extend(row)
+        ks.append(len(rows))
+    return (np.asarray(ls, dtype=np.int64), np.asarray(nprim, dtype=np.int64), np.asarray(exps, dtype=np.float64),
+            np.asarray(coefs, dtype=np.float64), np.asarray(ks, dtype=np.int64))
+
+
+@functools.lru_cache(maxsize=None)
 def element_shells(name: str) -> dict[int, tuple[Shell, ...]]:
     """Shells per atomic number of a shipped basis set (library.py:47-72 splitting)."""
     path = DATA / f"{name.lower()}.json"
@@ -119,34 +141,32 @@ class ShellTable:
 
     @classmethod
     def build(cls, name: str, symbols, positions) -> "ShellTable":
-        """Lay out basis ``name`` on atoms ``symbols`` at ``positions`` (Bohr)."""
+        """Lay out basis ``name`` on atoms ``symbols`` at ``positions`` (Bohr): each
+        atom's shells, exponents and normalised coefficients in the order of the
+        element's shells, atoms in order."""
         from hafnium_b200.molecule import atomic_number
 
-        by_z = element_shells(name)
         positions = np.asarray(positions, dtype=np.float64)
-        ls, centers, offsets, exps, coefs, ks, atoms = [], [], [0], [], [], [], []
-        for index, symbol in enumerate(symbols):
+        parts = []
+        for symbol in symbols:
             z = atomic_number(symbol)
-            if z not in by_z or not by_z[z]:
+            block = _element_block(name, z)
+            if block is None:
                 raise InputError(f"basis set {name!r} has no functions for {symbol}")
-            for shell in by_z[z]:
-                rows = shell.primitive_coefficients()
-                ls.append(shell.l)
-                centers.append(positions[index])
-                exps.extend(shell.exponents)
-                offsets.append(len(exps))
-                for row in rows:
-                    coefs.extend(row)
-                ks.append(len(rows))
-                atoms.append(index)
+            parts.append(block)
+        if not parts:
+            none = np.zeros(0, dtype=np.int64)
+            return cls(none, np.zeros((0, 3)), np.zeros(1, dtype=np.int64), np.zeros(0), np.zeros(0), none, none)
+        nsh = np.array([len(b[0]) for b in parts])
+        nprim = np.concatenate([b[1] for b in parts])
         return cls(
-            np.asarray(ls, dtype=np.int64),
-            np.asarray(centers, dtype=np.float64).reshape(-1, 3),
-            np.asarray(offsets, dtype=np.int64),
-            np.asarray(exps, dtype=np.float64),
-            np.asarray(coefs, dtype=np.float64),
-            np.asarray(ks, dtype=np.int64),
-            np.asarray(atoms, dtype=np.int64),
+            np.concatenate([b[0] for b in parts]),
+            np.repeat(positions[: len(parts)], nsh, axis=0).reshape(-1, 3),
+            np.concatenate([[0], np.cumsum(nprim)]).astype(np.int64),
+            np.concatenate([b[2] for b in parts]),
+            np.concatenate([b[3] for b in parts]),
+            np.concatenate([b[4] for b in parts]),
+            np.repeat(np.arange(len(parts), dtype=np.int64), nsh),
         )
 
     @classmethod
