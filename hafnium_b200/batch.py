@@ -320,7 +320,8 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
     iterations = np.zeros(len(molecules), dtype=np.int32)
     states = ["not_run"] * len(molecules)
     densities = [None] * len(molecules) if keep_densities else None
-    timings = {"setup_s": 0.0, "run_s": 0.0, "waves": 0, "tiles": {}}
+    timings = {"tables_s": time.perf_counter() - t_start, "setup_s": 0.0, "run_s": 0.0, "results_s": 0.0,
+               "waves": 0, "tiles": {}}
     # waves: groups in order of size, split to fit the memory budget
     pending = []
     for key in sorted(shapes):
@@ -386,6 +387,7 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
             for c in ctxs:
                 c.close()
         del keep, batches
+        t3 = time.perf_counter()
         if retry_failed:
             # a cluster the batch could not converge (no gap for purification, or
             # the iteration limit) goes through the per-cluster driver instead
@@ -415,6 +417,7 @@ def solve_batch(molecules, basis: str = "cc-pvdz", auxiliary: str = "def2-univer
                     del ham
         timings["setup_s"] += t1 - t0
         timings["run_s"] += t2 - t1
+        timings["results_s"] += t3 - t2
         timings["waves"] += 1
     pool.shutdown()
     return BatchResult(energies, iterations, states, time.perf_counter() - t_start, timings, densities)
