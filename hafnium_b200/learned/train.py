@@ -1,13 +1,14 @@
 """Train the learned initial density on converged densities from this SCF.
 
-    python -m hafnium_b200.learned.train --clusters 2000 --epochs 60 --out weights.npz
+    python -m hafnium_b200.learned.train [--clusters 16000] [--epochs 100] [--lr 3e-4] [--out weights.npz]
+
+(the defaults are the recipe of the shipped weights, weights_ccpvdz_atoms.npz)
 
 1. Seeded water clusters (H2O)n, n uniform in [2, 12], are converged together
    by the batched device DF-RHF (SAD guess, FP64, the reference's default
-   tolerances).
-   Their per-spin densities, expressed in the frames of their atoms (the
-   shell-pair blocks of every atom and every atom pair within the cutoff), are
-   the targets.
+   tolerances). Their per-spin densities, expressed in the frames of their
+   atoms (the shell-pair blocks of every atom and every atom pair within the
+   cutoff), are the targets.
 2. The network (hafnium_b200.learned.model) is trained with Adam on the device,
    forward and backward running on the hfnn kernels, several clusters per step.
 3. Held-out (H2O)16-24 clusters are converged from the SAD guess and from the
@@ -165,10 +166,10 @@ def evaluate(weights, sizes, seed0: int, device: int = 0, per_size: int = 3):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--clusters", type=int, default=2000)
-    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--clusters", type=int, default=16000)
+    ap.add_argument("--epochs", type=int, default=100)
     ap.add_argument("--batch", type=int, default=16)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr", type=float, default=3e-4)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--eval", type=str, default="16,20,24")
     ap.add_argument("--out", type=str, default=str(M.WEIGHTS))
