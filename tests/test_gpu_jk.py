@@ -183,3 +183,30 @@ def test_sharded_builder_over_a_one_rank_nccl_group():
     finally:
         if created:
             dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("rank", [1, 20, 33, 70])
+def test_density_factor_reproduces_a_semidefinite_density(system, rank):
+    """hf_density_factor (the blocked pivoted Cholesky: panels of 32 pivots) finds the
+    density's rank and a factor with F F^T = D, across panel boundaries; a rank limit
+    stops it early, and an indefinite density is refused."""
+    import torch
+
+    from hafnium_b200.errors import InputError
+
+    two_body, _ = system
+    n = two_body.n_ao
+    r = max(1, min(rank, n - 4))
+    rng = np.random.default_rng(rank)
+    c = rng.normal(size=(n, r)) / np.sqrt(n)
+    d = c @ c.T
+    dt = torch.as_tensor(d, device="cuda")
+    f = two_body.context.density_factor_device(dt, n)
+    # the rank, up to pivots on rounding residues just above the 1e-14 cut
+    assert f.shape[0] == n and r <= f.shape[1] <= r + 2
+    np.testing.assert_allclose((f @ f.T).cpu().numpy(), d, atol=1e-12 * np.abs(d).max(), rtol=0)
+    limit = max(1, r // 2)
+    assert two_body.context.density_factor_device(dt, limit).shape[1] == limit
+    bad = d - 3.0 * np.abs(d).max() * np.outer(np.eye(n)[0], np.eye(n)[0])
+    with pytest.raises(InputError, match="semidefinite"):
+        two_body.context.density_factor_device(torch.as_tensor(bad, device="cuda"), n)
