@@ -52,6 +52,41 @@ def test_contractions_have_unit_norm():
                 assert total == pytest.approx(1.0, abs=1e-12)
 
 
+@pytest.mark.parametrize("basis", ["cc-pvdz", "def2-universal-jkfit", "sto-3g", "def2-svp"])
+def test_shell_table_lays_out_each_atom_shell_by_shell(basis):
+    """ShellTable.build (each element's block computed once) equals the table laid out
+    shell by shell and atom by atom, as shell_table.py:84-116 does, for molecules of
+    several elements; an element the basis lacks is refused."""
+    from hafnium_b200.errors import InputError
+    from hafnium_b200.molecule import Molecule, atomic_number
+
+    rng = np.random.default_rng(5)
+    mols = [water_cluster(3, 1), Molecule(("N", "H", "H", "H", "C", "O"), rng.normal(size=(6, 3)) * 2.0)]
+    for mol in mols:
+        ls, centers, offsets, exps, coefs, ks, atoms = [], [], [0], [], [], [], []
+        for index, symbol in enumerate(mol.symbols):
+            for shell in element_shells(basis)[atomic_number(symbol)]:
+                rows = shell.primitive_coefficients()
+                ls.append(shell.l)
+                centers.append(mol.positions[index])
+                exps.extend(shell.exponents)
+                offsets.append(len(exps))
+                for row in rows:
+                    coefs.extend(row)
+                ks.append(len(rows))
+                atoms.append(index)
+        t = ShellTable.build(basis, mol.symbols, mol.positions)
+        np.testing.assert_array_equal(t.angular_momenta, ls)
+        np.testing.assert_array_equal(t.centers, np.asarray(centers).reshape(-1, 3))
+        np.testing.assert_array_equal(t.primitive_offsets, offsets)
+        np.testing.assert_array_equal(t.exponents, exps)
+        np.testing.assert_array_equal(t.coefficients, coefs)
+        np.testing.assert_array_equal(t.n_contractions, ks)
+        np.testing.assert_array_equal(t.shell_atoms, atoms)
+    with pytest.raises(InputError):
+        ShellTable.build(basis, ("O", "Xe"), np.zeros((2, 3)))
+
+
 def test_diis_and_filling_match_the_oracle():
     rng = np.random.default_rng(0)
     a = rng.normal(size=(5, 5))
