@@ -677,7 +677,18 @@ const char* hf_last_error(const hf_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 
 int hf_set_stream(hf_ctx* ctx, void* stream) {
     if (!ctx) return HF_ERR_ARG;
-    ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+    cudaStream_t next = stream ? (cudaStream_t)stream : ctx->own;
+    if (ctx->stream && next != ctx->stream) {
+        // the context's pool blocks go back with cudaFreeAsync on its current stream, so
+        // the work queued on the old stream finishes before the switch (unless that
+        // stream is being captured, where the caller orders the work)
+        cudaSetDevice(ctx->device);
+        cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(ctx->stream, &capture) == cudaSuccess && capture == cudaStreamCaptureStatusNone)
+            cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+    }
+    ctx->stream = next;
     return HF_OK;
 }
 

@@ -98,7 +98,10 @@ typedef struct hf_stats {
 int hf_ctx_create(int device, hf_ctx** out);
 int hf_ctx_destroy(hf_ctx* ctx);
 const char* hf_last_error(const hf_ctx* ctx);
-/* Launch on this stream (cudaStream_t) from now on; NULL = the context's own. */
+/* Launch on this stream (cudaStream_t) from now on; NULL = the context's own.
+ * Waits for the work queued on the previous stream first (unless that stream
+ * is being captured), since the context's blocks are released in the order of
+ * its current stream. */
 int hf_set_stream(hf_ctx* ctx, void* stream);
 
 /* The device blocks of fitted tensors, their BF16 copies and the J/K scratch
