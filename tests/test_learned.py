@@ -166,3 +166,25 @@ def test_untrained_elements_and_linear_molecules_fall_back():
     linear = Molecule(("O", "H", "H"), np.array([[0.0, 0, 0], [0, 0, 1.8], [0, 0, -1.8]]))
     assert M.build_graph(linear) is None
     assert M.predict_density(linear, weights) is None
+
+
+def test_batched_rotations_and_the_torch_assembly_match_their_plain_forms():
+    """harmonic_rotations (all frames at once) equals harmonic_rotation frame by frame, and
+    assemble_density (torch, here on the CPU) equals blocks_to_density (NumPy)."""
+    import torch
+
+    from hafnium_b200.learned.frames import harmonic_rotations
+
+    rng = np.random.default_rng(9)
+    frames = [random_rotation(rng) for _ in range(5)]
+    for l in range(3):
+        batched = harmonic_rotations(frames, l)
+        for f, u in zip(frames, batched):
+            np.testing.assert_allclose(u, harmonic_rotation(f, l), atol=1e-13)
+    g = M.build_graph(water_cluster(4, 6))
+    d = rng.normal(size=(g["n_nodes"], M.DIAG))
+    o = rng.normal(size=(len(g["src"]), M.OFF))
+    mean = rng.normal(size=(len(M.ELEMENTS), M.DIAG))
+    want = M.blocks_to_density(g, d, o, mean)
+    got = M.assemble_density(g, torch.as_tensor(d), torch.as_tensor(o), mean, torch.device("cpu"))
+    np.testing.assert_allclose(got.numpy(), want, atol=1e-13)
